@@ -1,0 +1,1134 @@
+// B200 engine for the per-batch GPU path of continuous subgraph matching.
+//
+// Device data layout (HBM):
+//   pool   u32 words holding every sorted neighbour run; runs start on 16-byte
+//          boundaries; allocation is a bump pointer, updated runs are written
+//          out of place and dead space is reclaimed by compaction.
+//   rec    uint4 per (direction d, compressed vertex u), row-major [d][dvcap]:
+//          x = run offset (words), y = run length, z = delta offset, w = delta length.
+//          One 16-byte load resolves both the old list and this batch's delta
+//          list of (d, u) (the two halves the reference keeps in index_gpu and
+//          update_index, graph_gpu.h:41-49).
+//   dval   this batch's delta values, sorted by (d, u, v), not deduplicated
+//          (calig_helper_gamma.cu:569-573).
+//
+// Per batch (calig_helper_gamma.cu:485-597 + graph_gpu.cu:1261-1480):
+//   1. edits = previous delta (deferred merge-back) + ins (add) + del (remove),
+//      packed to (d,u,v,op) and radix-sorted; one warp per touched (d,u) writes
+//      (old run U adds) \ removes.  One pass over each touched run per batch,
+//      where the reference makes three (merge ins, remove del, merge delta).
+//   2. delta keys packed + sorted -> dval and rec.z/.w for touched (d,u).
+//   3. persistent warp DFS seeded from the delta edges of every query edge
+//      (all query edges in one launch; the edge index ei travels with the seed).
+//   4. rec.z/.w of touched (d,u) cleared; this batch's delta becomes the
+//      pending merge-back of the next batch.
+#include <cuda_runtime.h>
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "cgbdsm.h"
+#include "query.h"
+
+using cgb::EdgePlan;
+using cgb::kMaxBN;
+using cgb::kMaxDir;
+using cgb::kMaxQE;
+using cgb::kMaxQV;
+
+namespace {
+
+constexpr uint32_t kFull = 0xffffffffu;
+constexpr int kDfsWarps = 8;  // warps per DFS block
+
+__constant__ EdgePlan c_plan[kMaxQE];
+
+// ---------------------------------------------------------------------------
+// key packing
+// ---------------------------------------------------------------------------
+struct PackInfo {
+    uint32_t B;      // bits per vertex id
+    uint32_t nd;     // directions
+    uint32_t dv;     // compressed vertex count
+};
+
+__device__ __forceinline__ bool decode_ext(uint64_t k, const PackInfo& pi, uint32_t& d, uint32_t& u,
+                                           uint32_t& v) {
+    d = (uint32_t)(k >> 59);
+    u = (uint32_t)((k >> 32) & 0x07FFFFFFu);
+    v = (uint32_t)k;
+    return d < pi.nd && u < pi.dv && v < pi.dv;
+}
+
+__device__ __forceinline__ uint64_t pack_duv(uint32_t d, uint32_t u, uint32_t v, uint32_t B) {
+    return ((uint64_t)d << (2 * B)) | ((uint64_t)u << B) | (uint64_t)v;
+}
+
+// Edits: ((d,u,v) << 1) | op, op 0 = add, 1 = remove.  Invalid keys raise err
+// bit 1 and are turned into a no-op remove of (0,0,0) ... which is harmless
+// only if it does not exist; instead they are mapped past the end (all ones)
+// and ignored by the merge.
+__global__ void k_pack_edits(const uint64_t* __restrict__ in, uint64_t n, uint32_t op, PackInfo pi,
+                             uint64_t* __restrict__ out, unsigned int* err) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (; i < n; i += stride) {
+        uint32_t d, u, v;
+        if (decode_ext(in[i], pi, d, u, v)) {
+            out[i] = (pack_duv(d, u, v, pi.B) << 1) | op;
+        } else {
+            out[i] = ~0ull;
+            atomicOr(err, 1u);
+        }
+    }
+}
+
+__global__ void k_pack_delta(const uint64_t* __restrict__ in, uint64_t n, PackInfo pi,
+                             uint64_t* __restrict__ out, unsigned int* err) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (; i < n; i += stride) {
+        uint32_t d, u, v;
+        if (decode_ext(in[i], pi, d, u, v)) {
+            out[i] = pack_duv(d, u, v, pi.B);
+        } else {
+            out[i] = ~0ull;
+            atomicOr(err, 2u);
+        }
+    }
+}
+
+// du = (d << B) | u of a sorted packed array (shift = B or B+1 for edits);
+// invalid (all-ones) entries map to 0xffffffff.
+__global__ void k_extract_du(const uint64_t* __restrict__ in, uint64_t n, uint32_t shift,
+                             uint32_t* __restrict__ du) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (; i < n; i += stride) {
+        uint64_t k = in[i];
+        du[i] = (k == ~0ull) ? 0xffffffffu : (uint32_t)(k >> shift);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// fused edit merge: one warp per touched (d, u)
+// ---------------------------------------------------------------------------
+struct MergeArgs {
+    uint4* rec;
+    uint32_t dvcap;
+    uint32_t* pool;
+    unsigned long long* pool_top;
+    unsigned long long pool_cap;
+    long long* live_words;       // sum of round4(len) over runs
+    const uint64_t* edits;       // sorted ((d,u,v)<<1|op)
+    const uint32_t* run_du;
+    const uint32_t* run_len;
+    const uint32_t* run_off;
+    const int* num_runs;
+    uint32_t B;
+    unsigned int* err;
+};
+
+__device__ __forceinline__ uint32_t round4(uint32_t x) { return (x + 3u) & ~3u; }
+
+// Merge-path split for diagonal k of X (base values) and Y (edits, value = e>>1 & vmask):
+// X wins ties, so for equal values the base element precedes add, add precedes remove.
+__device__ __forceinline__ uint32_t merge_split(const uint32_t* X, uint32_t xl, const uint64_t* Y,
+                                                uint32_t yl, uint32_t k, uint64_t vmask) {
+    uint32_t lo = k > yl ? k - yl : 0;
+    uint32_t hi = k < xl ? k : xl;
+    while (lo < hi) {
+        uint32_t mid = (lo + hi) >> 1;
+        uint32_t yv = (uint32_t)((Y[k - 1 - mid] >> 1) & vmask);
+        if (X[mid] <= yv) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
+__global__ void k_merge_runs(MergeArgs a) {
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+    const int nruns = *a.num_runs;
+    const uint64_t vmask = (1ull << a.B) - 1ull;
+    for (uint32_t r = gw; r < (uint32_t)nruns; r += nw) {
+        const uint32_t du = a.run_du[r];
+        if (du == 0xffffffffu) continue;  // invalid keys
+        const uint32_t d = du >> a.B, u = du & (uint32_t)vmask;
+        const uint64_t* Y = a.edits + a.run_off[r];
+        const uint32_t yl = a.run_len[r];
+        uint4* recp = a.rec + (size_t)d * a.dvcap + u;
+        const uint4 old = *recp;
+        const uint32_t* X = a.pool + old.x;
+        const uint32_t xl = old.y;
+        const uint32_t bound = xl + yl;
+        unsigned long long off = 0;
+        if (lane == 0) {
+            off = atomicAdd(a.pool_top, (unsigned long long)round4(bound));
+            if (off + round4(bound) > a.pool_cap) {
+                atomicOr(a.err, 4u);
+                off = ~0ull;
+            }
+        }
+        off = __shfl_sync(kFull, off, 0);
+        if (off == ~0ull) continue;  // pool exhausted: run left unchanged, error raised
+        uint32_t* C = a.pool + off;
+        const uint32_t total = xl + yl;
+        uint32_t outn = 0;
+        for (uint32_t k0 = 0; k0 < total; k0 += 32) {
+            const uint32_t k = k0 + lane;
+            bool emit = false;
+            uint32_t val = 0;
+            if (k < total) {
+                uint32_t i = merge_split(X, xl, Y, yl, k, vmask);
+                uint32_t j = k - i;
+                // element k
+                bool fromX = (i < xl) && (j >= yl || X[i] <= (uint32_t)((Y[j] >> 1) & vmask));
+                uint32_t op = 0;
+                if (fromX) { val = X[i]; ++i; }
+                else { val = (uint32_t)((Y[j] >> 1) & vmask); op = (uint32_t)(Y[j] & 1ull); ++j; }
+                // element k + 1: last of its value group?
+                bool last = true;
+                if (k + 1 < total) {
+                    uint32_t nv = (i < xl && (j >= yl || X[i] <= (uint32_t)((Y[j] >> 1) & vmask)))
+                                      ? X[i] : (uint32_t)((Y[j] >> 1) & vmask);
+                    last = (nv != val);
+                }
+                emit = last && op == 0;
+            }
+            const uint32_t bal = __ballot_sync(kFull, emit);
+            if (emit) C[outn + __popc(bal & ((1u << lane) - 1u))] = val;
+            outn += __popc(bal);
+        }
+        if (lane == 0) {
+            *recp = make_uint4((uint32_t)off, outn, old.z, old.w);
+            long long dl = (long long)round4(outn) - (long long)round4(xl);
+            if (dl) atomicAdd((unsigned long long*)a.live_words, (unsigned long long)dl);
+            // unused tail of the allocation is dead space until compaction
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// delta lists
+// ---------------------------------------------------------------------------
+__global__ void k_delta_values(const uint64_t* __restrict__ keys, uint64_t n, uint64_t vmask,
+                               uint32_t* __restrict__ dval) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (; i < n; i += stride) dval[i] = (uint32_t)(keys[i] & vmask);
+}
+
+__global__ void k_delta_recs(uint4* rec, uint32_t dvcap, const uint32_t* run_du, const uint32_t* run_len,
+                             const uint32_t* run_off, const int* num_runs, uint32_t B, int clear) {
+    const int n = *num_runs;
+    const uint32_t umask = (1u << B) - 1u;
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+        uint32_t du = run_du[r];
+        if (du == 0xffffffffu) continue;
+        uint4* p = rec + (size_t)(du >> B) * dvcap + (du & umask);
+        uint4 v = *p;
+        if (clear) { v.z = 0; v.w = 0; }
+        else { v.z = run_off[r]; v.w = run_len[r]; }
+        *p = v;
+    }
+}
+
+// Seed ranges: delta entries of direction seed_dir(ei) form one contiguous
+// range of the sorted packed delta array.
+__global__ void k_seed_ranges(const uint64_t* __restrict__ dkeys, uint64_t n, uint32_t B, uint32_t qe,
+                              const uint8_t* qe_dirs /*[qe][2]*/, const uint8_t* edge_ok, int have_ok,
+                              uint32_t* seed_lo, uint32_t* seed_pre) {
+    __shared__ uint32_t cnt[kMaxQE];
+    const uint32_t t = threadIdx.x;
+    auto lower = [&](uint64_t key) {
+        uint64_t lo = 0, hi = n;
+        while (lo < hi) {
+            uint64_t mid = (lo + hi) >> 1;
+            if (dkeys[mid] < key) lo = mid + 1; else hi = mid;
+        }
+        return (uint32_t)lo;
+    };
+    if (t < qe) {
+        uint32_t s = c_plan[t].seed_dir;
+        uint32_t lo = lower((uint64_t)s << (2 * B));
+        uint32_t hi = lower((uint64_t)(s + 1) << (2 * B));
+        uint32_t d0 = qe_dirs[2 * t], d1 = qe_dirs[2 * t + 1];
+        uint32_t c0 = lower((uint64_t)(d0 + 1) << (2 * B)) - lower((uint64_t)d0 << (2 * B));
+        uint32_t c1 = lower((uint64_t)(d1 + 1) << (2 * B)) - lower((uint64_t)d1 << (2 * B));
+        bool ok = have_ok ? (edge_ok[t] != 0) : (c0 > 0 && c1 > 0);
+        seed_lo[t] = lo;
+        cnt[t] = ok ? hi - lo : 0;
+    }
+    __syncthreads();
+    if (t == 0) {
+        uint32_t acc = 0;
+        for (uint32_t e = 0; e < qe; ++e) { seed_pre[e] = acc; acc += cnt[e]; }
+        seed_pre[qe] = acc;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// persistent warp DFS (count only)
+// ---------------------------------------------------------------------------
+struct DfsArgs {
+    const uint4* rec;
+    uint32_t dvcap;
+    const uint32_t* pool;
+    const uint32_t* dval;
+    const uint64_t* dkeys;
+    uint32_t B;
+    uint32_t qe;
+    const uint32_t* seed_lo;
+    const uint32_t* seed_pre;
+    unsigned long long* counts;  // [qe]
+    unsigned int* work_next;
+};
+
+__device__ __forceinline__ bool list_contains(const uint32_t* __restrict__ pool, const uint32_t* __restrict__ dval,
+                                              const uint4& r, uint32_t x) {
+    // main part
+    {
+        const uint32_t* p = pool + r.x;
+        uint32_t lo = 0, n = r.y;
+        while (n > 0) {
+            uint32_t half = n >> 1;
+            if (__ldg(p + lo + half) < x) { lo += half + 1; n -= half + 1; }
+            else n = half;
+        }
+        if (lo < r.y && __ldg(p + lo) == x) return true;
+    }
+    if (r.w) {
+        const uint32_t* p = dval + r.z;
+        uint32_t lo = 0, n = r.w;
+        while (n > 0) {
+            uint32_t half = n >> 1;
+            if (__ldg(p + lo + half) < x) { lo += half + 1; n -= half + 1; }
+            else n = half;
+        }
+        if (lo < r.w && __ldg(p + lo) == x) return true;
+    }
+    return false;
+}
+
+__global__ void __launch_bounds__(kDfsWarps * 32) k_dfs_count(DfsArgs a) {
+    __shared__ uint32_t s_cand[kDfsWarps][kMaxQV][32];
+    __shared__ uint4 s_bn[kDfsWarps][kMaxBN];
+    __shared__ uint32_t s_m[kDfsWarps][kMaxQV];
+    __shared__ uint32_t s_pre[kMaxQE + 1];
+    __shared__ uint32_t s_lo[kMaxQE];
+
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t w = threadIdx.x >> 5;
+    if (threadIdx.x <= a.qe) s_pre[threadIdx.x] = a.seed_pre[threadIdx.x];
+    if (threadIdx.x < a.qe) s_lo[threadIdx.x] = a.seed_lo[threadIdx.x];
+    __syncthreads();
+    const uint32_t total = s_pre[a.qe];
+    const uint64_t vmask = (1ull << a.B) - 1ull;
+    uint32_t* m = s_m[w];
+    uint4* bn = s_bn[w];
+
+    // per-depth state held by lane == depth
+    uint32_t st_ncand = 0, st_pos = 0, st_next = 0, st_len = 0, st_gen = 0;
+    unsigned long long cnt = 0;
+    int cur_ei = -1;
+
+    for (;;) {
+        uint32_t item = 0;
+        if (lane == 0) item = atomicAdd(a.work_next, 1u);
+        item = __shfl_sync(kFull, item, 0);
+        if (item >= total) break;
+        int ei = 0;
+        while (ei + 1 < (int)a.qe && s_pre[ei + 1] <= item) ++ei;
+        if (ei != cur_ei) {
+            if (cur_ei >= 0 && lane == 0 && cnt) atomicAdd(a.counts + cur_ei, cnt);
+            cnt = 0;
+            cur_ei = ei;
+        }
+        const EdgePlan& P = c_plan[ei];
+        const uint64_t key = a.dkeys[s_lo[ei] + (item - s_pre[ei])];
+        if (lane == 0) {
+            m[0] = (uint32_t)((key >> a.B) & vmask);
+            m[1] = (uint32_t)(key & vmask);
+        }
+        const uint32_t n = P.n;
+        if (n == 2) { cnt += 1; __syncwarp(); continue; }
+        __syncwarp();
+
+        // set up depth j: resolve BN records, choose the shortest list as generator
+        auto setup = [&](uint32_t j) {
+            const uint32_t o0 = P.bn_off[j], o1 = P.bn_off[j + 1];
+            const uint32_t nb = o1 - o0;
+            uint32_t len = 0xffffffffu;
+            if (lane < nb) {
+                const uint32_t k = o0 + lane;
+                uint4 r = a.rec[(size_t)P.bn_dir[k] * a.dvcap + m[P.bn_pos[k]]];
+                if (!P.bn_dvis[k]) r.w = 0;
+                bn[k] = r;
+                len = r.y + r.w;
+            }
+            // argmin (len, lane)
+            uint32_t best = len, bl = lane;
+            for (int o = 16; o > 0; o >>= 1) {
+                uint32_t ol = __shfl_xor_sync(kFull, best, o);
+                uint32_t oi = __shfl_xor_sync(kFull, bl, o);
+                if (ol < best || (ol == best && oi < bl)) { best = ol; bl = oi; }
+            }
+            if (lane == j) { st_ncand = 0; st_pos = 0; st_next = 0; st_len = best; st_gen = bl; }
+            __syncwarp();
+        };
+
+        setup(2);
+        uint32_t j = 2;
+        while (j >= 2) {
+            const uint32_t ncand = __shfl_sync(kFull, st_ncand, j);
+            const uint32_t pos = __shfl_sync(kFull, st_pos, j);
+            if (pos < ncand) {
+                if (lane == j) st_pos = pos + 1;
+                if (lane == 0) m[j] = s_cand[w][j][pos];
+                __syncwarp();
+                ++j;
+                setup(j);
+                continue;
+            }
+            const uint32_t gnext = __shfl_sync(kFull, st_next, j);
+            const uint32_t glen = __shfl_sync(kFull, st_len, j);
+            if (gnext < glen) {
+                const uint32_t g = __shfl_sync(kFull, st_gen, j);
+                const uint32_t o0 = P.bn_off[j], o1 = P.bn_off[j + 1];
+                const uint4 gr = bn[o0 + g];
+                const uint32_t idx = gnext + lane;
+                bool ok = idx < glen;
+                uint32_t c = 0;
+                if (ok) {
+                    c = idx < gr.y ? __ldg(a.pool + gr.x + idx) : __ldg(a.dval + gr.z + (idx - gr.y));
+                    for (uint32_t t = 0; t < j; ++t) ok &= (c != m[t]);
+                    for (uint32_t k = o0; k < o1 && ok; ++k) {
+                        if (k == o0 + g) continue;
+                        ok = list_contains(a.pool, a.dval, bn[k], c);
+                    }
+                }
+                const uint32_t bal = __ballot_sync(kFull, ok);
+                if (j == n - 1) {
+                    cnt += __popc(bal);
+                } else {
+                    if (ok) s_cand[w][j][__popc(bal & ((1u << lane) - 1u))] = c;
+                    if (lane == j) { st_ncand = __popc(bal); st_pos = 0; }
+                }
+                if (lane == j) st_next = gnext + 32;
+                __syncwarp();
+                continue;
+            }
+            --j;
+        }
+    }
+    if (cur_ei >= 0 && lane == 0 && cnt) atomicAdd(a.counts + cur_ei, cnt);
+}
+
+// ---------------------------------------------------------------------------
+// maintenance kernels
+// ---------------------------------------------------------------------------
+__global__ void k_rec_sizes(const uint4* rec, uint32_t dvcap, uint32_t dv, uint32_t nd, uint32_t* out_round4,
+                            uint32_t* out_len) {
+    uint64_t total = (uint64_t)nd * dv;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        uint32_t d = (uint32_t)(i / dv), u = (uint32_t)(i % dv);
+        uint32_t len = rec[(size_t)d * dvcap + u].y;
+        if (out_round4) out_round4[i] = round4(len);
+        if (out_len) out_len[i] = len;
+    }
+}
+
+// Copies every run to its compacted offset (warp per (d,u)).
+__global__ void k_compact(uint4* rec, uint32_t dvcap, uint32_t dv, uint32_t nd, const uint32_t* src,
+                          uint32_t* dst, const unsigned long long* new_off) {
+    const uint32_t lane = threadIdx.x & 31;
+    uint64_t total = (uint64_t)nd * dv;
+    for (uint64_t i = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < total;
+         i += ((uint64_t)gridDim.x * blockDim.x) >> 5) {
+        uint32_t d = (uint32_t)(i / dv), u = (uint32_t)(i % dv);
+        uint4* p = rec + (size_t)d * dvcap + u;
+        uint4 r = *p;
+        uint64_t no = new_off[i];
+        for (uint32_t k = lane; k < r.y; k += 32) dst[no + k] = src[r.x + k];
+        if (lane == 0) { r.x = (uint32_t)no; *p = r; }
+    }
+}
+
+__global__ void k_dump(const uint4* rec, uint32_t dvcap, uint32_t dv, uint32_t nd, const uint32_t* pool,
+                       const unsigned long long* off, uint64_t* out) {
+    const uint32_t lane = threadIdx.x & 31;
+    uint64_t total = (uint64_t)nd * dv;
+    for (uint64_t i = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < total;
+         i += ((uint64_t)gridDim.x * blockDim.x) >> 5) {
+        uint32_t d = (uint32_t)(i / dv), u = (uint32_t)(i % dv);
+        uint4 r = rec[(size_t)d * dvcap + u];
+        uint64_t o = off[i];
+        for (uint32_t k = lane; k < r.y; k += 32)
+            out[o + k] = ((uint64_t)d << 59) | ((uint64_t)u << 32) | pool[r.x + k];
+    }
+}
+
+__global__ void k_copy_rows(const uint4* src, uint32_t src_cap, uint4* dst, uint32_t dst_cap, uint32_t nd,
+                            uint32_t dv) {
+    uint64_t total = (uint64_t)nd * dv;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        uint32_t d = (uint32_t)(i / dv), u = (uint32_t)(i % dv);
+        dst[(size_t)d * dst_cap + u] = src[(size_t)d * src_cap + u];
+    }
+}
+
+__global__ void k_u32_to_u64(const uint32_t* in, unsigned long long* out, uint64_t n) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (uint64_t)gridDim.x * blockDim.x)
+        out[i] = in[i];
+}
+
+inline uint32_t bits_for(uint32_t dv) {
+    uint32_t b = 1;
+    while ((1ull << b) < (uint64_t)dv) ++b;
+    return b;
+}
+
+}  // namespace
+
+// ===========================================================================
+// host side
+// ===========================================================================
+struct cgb_handle {
+    cgb_config cfg{};
+    int device = 0;
+    int num_sms = 148;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    std::string err;
+    uint64_t launches = 0;
+
+    // query
+    bool have_query = false;
+    cgb::QueryMeta q;
+    EdgePlan plans[kMaxQE];
+    uint8_t* d_qe_dirs = nullptr;  // [qe][2]
+    uint8_t* d_edge_ok = nullptr;  // [kMaxQE]
+
+    // index
+    bool have_index = false;
+    uint32_t nd = 0, dv = 0, dvcap = 0;
+    uint4* rec = nullptr;
+    uint32_t* pool = nullptr;
+    uint32_t* pool_alt = nullptr;
+    unsigned long long pool_cap = 0;
+    // device scalars: [0] pool_top, [1] live_words, [2] err, [3] work_next
+    unsigned long long* d_scal = nullptr;
+    unsigned long long* h_scal = nullptr;  // pinned mirror (4 scalars + counts)
+    unsigned long long h_pool_top = 0;
+    long long h_live = 0;
+
+    // per-batch buffers (grown on demand)
+    uint64_t* d_keys_in = nullptr; size_t keys_in_cap = 0;       // uploaded ext keys (ins|del|delta)
+    uint64_t* d_pending = nullptr; size_t pending_cap = 0; uint64_t n_pending = 0;  // ext delta keys
+    uint64_t* d_edits = nullptr; uint64_t* d_edits_alt = nullptr; size_t edits_cap = 0;
+    uint32_t* d_du = nullptr; uint32_t* d_run_du = nullptr; uint32_t* d_run_len = nullptr;
+    uint32_t* d_run_off = nullptr; size_t runs_cap = 0;
+    int* d_num_runs = nullptr;
+    uint64_t* d_dkeys = nullptr; uint64_t* d_dkeys_alt = nullptr; size_t dkeys_cap = 0;
+    uint32_t* d_dval = nullptr;
+    uint32_t* d_ddu = nullptr;
+    uint32_t* d_drun_du = nullptr; uint32_t* d_drun_len = nullptr; uint32_t* d_drun_off = nullptr;
+    size_t druns_cap = 0;
+    uint32_t* d_seed = nullptr;  // [0..kMaxQE) lo, [kMaxQE..2kMaxQE+1) pre
+    unsigned long long* d_counts = nullptr;  // [kMaxQE]
+    void* d_temp = nullptr; size_t temp_cap = 0;
+
+    uint64_t last_counts[kMaxQE] = {0};
+    float last_t[4] = {0, 0, 0, 0};
+    cudaEvent_t ev[5] = {};
+};
+
+namespace {
+
+cgb_status fail(cgb_handle* h, cgb_status s, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    if (h) h->err = buf;
+    return s;
+}
+
+#define CK(call)                                                                                 \
+    do {                                                                                         \
+        cudaError_t e_ = (call);                                                                 \
+        if (e_ != cudaSuccess) {                                                                 \
+            return fail(h, e_ == cudaErrorMemoryAllocation ? CGB_ERR_OOM : CGB_ERR_CUDA,         \
+                        "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
+        }                                                                                        \
+    } while (0)
+
+#define LAUNCHED() (h->launches++)
+
+template <typename T>
+cgb_status grow(cgb_handle* h, T*& p, size_t& cap, size_t need) {
+    if (need <= cap && p) return CGB_OK;
+    size_t nc = std::max<size_t>(need + need / 2, 1024);
+    if (p) CK(cudaFree(p));
+    p = nullptr;
+    CK(cudaMalloc(&p, nc * sizeof(T)));
+    cap = nc;
+    return CGB_OK;
+}
+
+cgb_status grow_temp(cgb_handle* h, size_t need) {
+    if (need <= h->temp_cap && h->d_temp) return CGB_OK;
+    size_t nc = std::max<size_t>(need + need / 2, 1 << 20);
+    if (h->d_temp) CK(cudaFree(h->d_temp));
+    h->d_temp = nullptr;
+    CK(cudaMalloc(&h->d_temp, nc));
+    h->temp_cap = nc;
+    return CGB_OK;
+}
+
+inline int grid_for(const cgb_handle* h, uint64_t n, int block = 256) {
+    uint64_t g = (n + block - 1) / block;
+    uint64_t cap = (uint64_t)h->num_sms * 8;
+    if (g > cap) g = cap;
+    if (g < 1) g = 1;
+    return (int)g;
+}
+
+cgb_status ensure_dvcap(cgb_handle* h, uint32_t dv) {
+    if (dv <= h->dvcap && h->rec) return CGB_OK;
+    uint32_t nc = std::max<uint32_t>(dv + dv / 4 + 1024, h->dvcap * 2);
+    uint4* nr = nullptr;
+    CK(cudaMalloc(&nr, (size_t)h->nd * nc * sizeof(uint4)));
+    CK(cudaMemsetAsync(nr, 0, (size_t)h->nd * nc * sizeof(uint4), h->stream));
+    if (h->rec) {
+        k_copy_rows<<<grid_for(h, (uint64_t)h->nd * h->dv), 256, 0, h->stream>>>(h->rec, h->dvcap, nr, nc, h->nd,
+                                                                                   h->dv);
+        LAUNCHED();
+        CK(cudaGetLastError());
+        CK(cudaStreamSynchronize(h->stream));
+        CK(cudaFree(h->rec));
+    }
+    h->rec = nr;
+    h->dvcap = nc;
+    return CGB_OK;
+}
+
+// Compacts the pool into pool_alt (allocating or growing it to new_cap words)
+// and swaps.  Synchronous.
+cgb_status compact_pool(cgb_handle* h, unsigned long long new_cap) {
+    const uint64_t n = (uint64_t)h->nd * h->dv;
+    if (new_cap < h->pool_cap) new_cap = h->pool_cap;
+    uint32_t* dst = nullptr;
+    if (h->pool_alt && new_cap == h->pool_cap) {
+        dst = h->pool_alt;
+    } else {
+        if (h->pool_alt) CK(cudaFree(h->pool_alt));
+        h->pool_alt = nullptr;
+        CK(cudaMalloc(&dst, new_cap * sizeof(uint32_t)));
+    }
+    unsigned long long live = 0;
+    if (n > 0) {
+        uint32_t* sizes = nullptr;
+        unsigned long long* offs = nullptr;
+        CK(cudaMalloc(&sizes, n * sizeof(uint32_t)));
+        CK(cudaMalloc(&offs, (n + 1) * sizeof(unsigned long long)));
+        k_rec_sizes<<<grid_for(h, n), 256, 0, h->stream>>>(h->rec, h->dvcap, h->dv, h->nd, sizes, nullptr);
+        LAUNCHED();
+        k_u32_to_u64<<<grid_for(h, n), 256, 0, h->stream>>>(sizes, offs, n);
+        LAUNCHED();
+        size_t tb = 0;
+        CK(cub::DeviceScan::ExclusiveSum(nullptr, tb, offs, offs, (int64_t)n + 1, h->stream));
+        // offs has n valid entries; scanning n+1 needs a defined last element
+        CK(cudaMemsetAsync(offs + n, 0, sizeof(unsigned long long), h->stream));
+        if (grow_temp(h, tb) != CGB_OK) return CGB_ERR_OOM;
+        CK(cub::DeviceScan::ExclusiveSum(h->d_temp, tb, offs, offs, (int64_t)n + 1, h->stream));
+        LAUNCHED();
+        k_compact<<<grid_for(h, n * 32), 256, 0, h->stream>>>(h->rec, h->dvcap, h->dv, h->nd, h->pool, dst, offs);
+        LAUNCHED();
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(&live, offs + n, sizeof(live), cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        CK(cudaFree(sizes));
+        CK(cudaFree(offs));
+    }
+    uint32_t* old = h->pool;
+    h->pool = dst;
+    if (new_cap == h->pool_cap) {
+        h->pool_alt = old;
+    } else {
+        CK(cudaFree(old));
+        h->pool_alt = nullptr;
+        h->pool_cap = new_cap;
+    }
+    h->h_pool_top = live;
+    h->h_live = (long long)live;
+    unsigned long long sc[2] = {live, live};
+    CK(cudaMemcpyAsync(h->d_scal, sc, sizeof(sc), cudaMemcpyHostToDevice, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return CGB_OK;
+}
+
+// Ensures the pool can absorb a merge of n_edits edits in the worst case.
+cgb_status reserve_pool(cgb_handle* h, uint64_t n_edits) {
+    const unsigned long long need = (unsigned long long)std::max<long long>(h->h_live, 0) + 4ull * n_edits + 64;
+    if (h->h_pool_top + need <= h->pool_cap) return CGB_OK;
+    unsigned long long cap = h->pool_cap;
+    while ((unsigned long long)std::max<long long>(h->h_live, 0) + need > cap * 3 / 4) cap = cap * 2;
+    return compact_pool(h, cap);
+}
+
+// Sorts packed keys in place (alt buffer used as ping-pong); returns sorted pointer.
+cgb_status radix_sort(cgb_handle* h, uint64_t*& keys, uint64_t*& alt, uint64_t n, int end_bit) {
+    if (n == 0) return CGB_OK;
+    cub::DoubleBuffer<uint64_t> db(keys, alt);
+    size_t tb = 0;
+    CK(cub::DeviceRadixSort::SortKeys(nullptr, tb, db, (int64_t)n, 0, end_bit, h->stream));
+    if (grow_temp(h, tb) != CGB_OK) return CGB_ERR_OOM;
+    CK(cub::DeviceRadixSort::SortKeys(h->d_temp, tb, db, (int64_t)n, 0, end_bit, h->stream));
+    LAUNCHED();
+    if (db.Current() != keys) std::swap(keys, alt);
+    return CGB_OK;
+}
+
+// Run-length segments of du over n sorted entries; offsets by exclusive scan.
+cgb_status segment(cgb_handle* h, const uint32_t* du, uint64_t n, uint32_t* run_du, uint32_t* run_len,
+                   uint32_t* run_off, int* num_runs) {
+    size_t tb = 0;
+    CK(cub::DeviceRunLengthEncode::Encode(nullptr, tb, du, run_du, run_len, num_runs, (int64_t)n, h->stream));
+    size_t tb2 = 0;
+    CK(cub::DeviceScan::ExclusiveSum(nullptr, tb2, run_len, run_off, (int64_t)n, h->stream));
+    if (grow_temp(h, std::max(tb, tb2)) != CGB_OK) return CGB_ERR_OOM;
+    CK(cub::DeviceRunLengthEncode::Encode(h->d_temp, tb, du, run_du, run_len, num_runs, (int64_t)n, h->stream));
+    LAUNCHED();
+    // scanning n entries (runs beyond num_runs hold garbage but are never read)
+    CK(cub::DeviceScan::ExclusiveSum(h->d_temp, tb2, run_len, run_off, (int64_t)n, h->stream));
+    LAUNCHED();
+    return CGB_OK;
+}
+
+// Grow-only per-batch buffers (reallocated only when a batch is larger than any before).
+cgb_status ensure_edit_buffers(cgb_handle* h, uint64_t n) {
+    if (n <= h->edits_cap && h->d_edits) return CGB_OK;
+    size_t nc = std::max<size_t>(n + n / 2, 1 << 16);
+    CK(cudaStreamSynchronize(h->stream));
+    void* olds[] = {h->d_edits, h->d_edits_alt, h->d_du, h->d_run_du, h->d_run_len, h->d_run_off};
+    for (void* p : olds) if (p) CK(cudaFree(p));
+    CK(cudaMalloc(&h->d_edits, nc * sizeof(uint64_t)));
+    CK(cudaMalloc(&h->d_edits_alt, nc * sizeof(uint64_t)));
+    CK(cudaMalloc(&h->d_du, nc * sizeof(uint32_t)));
+    CK(cudaMalloc(&h->d_run_du, nc * sizeof(uint32_t)));
+    CK(cudaMalloc(&h->d_run_len, nc * sizeof(uint32_t)));
+    CK(cudaMalloc(&h->d_run_off, nc * sizeof(uint32_t)));
+    h->edits_cap = nc;
+    h->runs_cap = nc;
+    return CGB_OK;
+}
+
+cgb_status ensure_delta_buffers(cgb_handle* h, uint64_t n) {
+    if (n <= h->dkeys_cap && h->d_dkeys) return CGB_OK;
+    size_t nc = std::max<size_t>(n + n / 2, 1 << 16);
+    CK(cudaStreamSynchronize(h->stream));
+    void* olds[] = {h->d_dkeys, h->d_dkeys_alt, h->d_dval, h->d_ddu, h->d_drun_du, h->d_drun_len, h->d_drun_off};
+    for (void* p : olds) if (p) CK(cudaFree(p));
+    CK(cudaMalloc(&h->d_dkeys, nc * sizeof(uint64_t)));
+    CK(cudaMalloc(&h->d_dkeys_alt, nc * sizeof(uint64_t)));
+    CK(cudaMalloc(&h->d_dval, nc * sizeof(uint32_t)));
+    CK(cudaMalloc(&h->d_ddu, nc * sizeof(uint32_t)));
+    CK(cudaMalloc(&h->d_drun_du, nc * sizeof(uint32_t)));
+    CK(cudaMalloc(&h->d_drun_len, nc * sizeof(uint32_t)));
+    CK(cudaMalloc(&h->d_drun_off, nc * sizeof(uint32_t)));
+    h->dkeys_cap = nc;
+    h->druns_cap = nc;
+    return CGB_OK;
+}
+
+// Applies edits = adds0 (ext keys, device) + adds1 + removes to the index.
+cgb_status apply_edits(cgb_handle* h, const uint64_t* adds0, uint64_t n0, const uint64_t* adds1, uint64_t n1,
+                       const uint64_t* rems, uint64_t n2) {
+    const uint64_t n = n0 + n1 + n2;
+    if (n == 0) return CGB_OK;
+    cgb_status s;
+    if ((s = reserve_pool(h, n)) != CGB_OK) return s;
+    if ((s = ensure_edit_buffers(h, n)) != CGB_OK) return s;
+    PackInfo pi{bits_for(h->dv), h->nd, h->dv};
+    unsigned int* d_err = (unsigned int*)(h->d_scal + 2);
+    if (n0) { k_pack_edits<<<grid_for(h, n0), 256, 0, h->stream>>>(adds0, n0, 0, pi, h->d_edits, d_err); LAUNCHED(); }
+    if (n1) { k_pack_edits<<<grid_for(h, n1), 256, 0, h->stream>>>(adds1, n1, 0, pi, h->d_edits + n0, d_err); LAUNCHED(); }
+    if (n2) { k_pack_edits<<<grid_for(h, n2), 256, 0, h->stream>>>(rems, n2, 1, pi, h->d_edits + n0 + n1, d_err); LAUNCHED(); }
+    CK(cudaGetLastError());
+    // valid keys use 2B+6 bits; one more bit makes the all-ones invalid marker sort last
+    if ((s = radix_sort(h, h->d_edits, h->d_edits_alt, n, 2 * (int)pi.B + 7)) != CGB_OK) return s;
+    k_extract_du<<<grid_for(h, n), 256, 0, h->stream>>>(h->d_edits, n, pi.B + 1, h->d_du);
+    LAUNCHED();
+    if ((s = segment(h, h->d_du, n, h->d_run_du, h->d_run_len, h->d_run_off, h->d_num_runs)) != CGB_OK) return s;
+    MergeArgs ma;
+    ma.rec = h->rec;
+    ma.dvcap = h->dvcap;
+    ma.pool = h->pool;
+    ma.pool_top = h->d_scal + 0;
+    ma.pool_cap = h->pool_cap;
+    ma.live_words = (long long*)(h->d_scal + 1);
+    ma.edits = h->d_edits;
+    ma.run_du = h->d_run_du;
+    ma.run_len = h->d_run_len;
+    ma.run_off = h->d_run_off;
+    ma.num_runs = h->d_num_runs;
+    ma.B = pi.B;
+    ma.err = d_err;
+    const int mg = std::max(1, std::min<int>((int)((n * 32 + 255) / 256), h->num_sms * 16));
+    k_merge_runs<<<mg, 256, 0, h->stream>>>(ma);
+    LAUNCHED();
+    CK(cudaGetLastError());
+    return CGB_OK;
+}
+
+cgb_status sync_scalars(cgb_handle* h) {
+    CK(cudaMemcpyAsync(h->h_scal, h->d_scal, 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(h->h_scal + 4, h->d_counts, kMaxQE * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                       h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    h->h_pool_top = h->h_scal[0];
+    h->h_live = (long long)h->h_scal[1];
+    return CGB_OK;
+}
+
+cgb_status flush_pending(cgb_handle* h) {
+    if (h->n_pending == 0) return CGB_OK;
+    cgb_status s = apply_edits(h, h->d_pending, h->n_pending, nullptr, 0, nullptr, 0);
+    if (s != CGB_OK) return s;
+    h->n_pending = 0;
+    return sync_scalars(h);
+}
+
+}  // namespace
+
+extern "C" {
+
+void cgb_default_config(cgb_config* cfg) {
+    if (!cfg) return;
+    std::memset(cfg, 0, sizeof(*cfg));
+}
+
+cgb_status cgb_create(const cgb_config* cfg, cgb_handle** out) {
+    if (!out) return CGB_ERR_ARG;
+    *out = nullptr;
+    cgb_handle* h = new cgb_handle();
+    if (cfg) h->cfg = *cfg; else cgb_default_config(&h->cfg);
+    h->device = h->cfg.device;
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev == 0) {
+        cgb_status s = fail(h, CGB_ERR_CUDA, "no CUDA device: %s", cudaGetErrorString(e));
+        *out = h;
+        return s;
+    }
+    if (h->device < 0 || h->device >= ndev) { *out = h; return fail(h, CGB_ERR_ARG, "bad device %d", h->device); }
+#define CKC(call) do { cudaError_t e_ = (call); if (e_ != cudaSuccess) { *out = h; return fail(h, CGB_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(e_)); } } while (0)
+    CKC(cudaSetDevice(h->device));
+    CKC(cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, h->device));
+    CKC(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+    h->own_stream = true;
+    CKC(cudaMalloc(&h->d_scal, 4 * sizeof(unsigned long long)));
+    CKC(cudaMemset(h->d_scal, 0, 4 * sizeof(unsigned long long)));
+    CKC(cudaMallocHost(&h->h_scal, (4 + kMaxQE) * sizeof(unsigned long long)));
+    CKC(cudaMalloc(&h->d_num_runs, 2 * sizeof(int)));
+    CKC(cudaMalloc(&h->d_seed, (3 * kMaxQE + 2) * sizeof(uint32_t)));
+    CKC(cudaMalloc(&h->d_counts, kMaxQE * sizeof(unsigned long long)));
+    CKC(cudaMalloc(&h->d_qe_dirs, 2 * kMaxQE));
+    CKC(cudaMalloc(&h->d_edge_ok, kMaxQE));
+    for (auto& ev : h->ev) CKC(cudaEventCreate(&ev));
+#undef CKC
+    *out = h;
+    return CGB_OK;
+}
+
+void cgb_destroy(cgb_handle* h) {
+    if (!h) return;
+    cudaSetDevice(h->device);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    void* ptrs[] = {h->rec, h->pool, h->pool_alt, h->d_scal, h->d_keys_in, h->d_pending, h->d_edits,
+                    h->d_edits_alt, h->d_du, h->d_run_du, h->d_run_len, h->d_run_off, h->d_num_runs,
+                    h->d_dkeys, h->d_dkeys_alt, h->d_dval, h->d_ddu, h->d_drun_du, h->d_drun_len, h->d_drun_off,
+                    h->d_seed, h->d_counts, h->d_temp, h->d_qe_dirs, h->d_edge_ok};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    if (h->h_scal) cudaFreeHost(h->h_scal);
+    for (auto& ev : h->ev)
+        if (ev) cudaEventDestroy(ev);
+    if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+}
+
+const char* cgb_last_error(const cgb_handle* h) { return h ? h->err.c_str() : "null handle"; }
+
+cgb_status cgb_load_query(cgb_handle* h, uint32_t qv, uint32_t qe, const uint32_t* edges) {
+    if (!h || !edges) return CGB_ERR_ARG;
+    if (h->have_index) return fail(h, CGB_ERR_STATE, "query must be loaded before the index");
+    std::string e = cgb::build_query_meta(qv, qe, edges, h->q);
+    if (!e.empty()) return fail(h, CGB_ERR_ARG, "%s", e.c_str());
+    h->nd = h->q.nd;
+    uint8_t dirs[2 * kMaxQE];
+    for (uint32_t i = 0; i < h->q.qe; ++i) { dirs[2 * i] = h->q.qe_dir[i][0]; dirs[2 * i + 1] = h->q.qe_dir[i][1]; }
+    CK(cudaSetDevice(h->device));
+    CK(cudaMemcpy(h->d_qe_dirs, dirs, 2 * h->q.qe, cudaMemcpyHostToDevice));
+    h->have_query = true;
+    return CGB_OK;
+}
+
+cgb_status cgb_load_query_file(cgb_handle* h, const char* path) {
+    if (!h || !path) return CGB_ERR_ARG;
+    std::vector<uint32_t> labels, edges;
+    uint32_t qv = 0;
+    std::string e = cgb::parse_query_file(path, labels, edges, qv);
+    if (!e.empty()) return fail(h, CGB_ERR_IO, "%s", e.c_str());
+    return cgb_load_query(h, qv, (uint32_t)(edges.size() / 2), edges.data());
+}
+
+uint32_t cgb_query_dir(const cgb_handle* h, uint32_t a, uint32_t b) {
+    if (!h || !h->have_query || a >= h->q.qv || b >= h->q.qv) return 255;
+    return h->q.eidx[a * kMaxQV + b];
+}
+
+cgb_status cgb_build_index(cgb_handle* h, const uint64_t* keys, uint64_t n, uint32_t dv_count) {
+    if (!h) return CGB_ERR_ARG;
+    if (!h->have_query) return fail(h, CGB_ERR_STATE, "load a query first");
+    if (h->have_index) return fail(h, CGB_ERR_STATE, "index already built");
+    if (dv_count > CGB_MAX_VID) return fail(h, CGB_ERR_LIMIT, "dv_count %u exceeds 2^27-1", dv_count);
+    if (n && !keys) return CGB_ERR_ARG;
+    CK(cudaSetDevice(h->device));
+    // planner statistics (calig_helper_gamma.cu:304-311): entries and
+    // non-empty vertices per direction -> mean run length
+    std::vector<uint64_t> card(h->nd, 0), nodes(h->nd, 0);
+    {
+        std::vector<uint8_t> seen((size_t)h->nd * std::max<uint32_t>(dv_count, 1), 0);
+        for (uint64_t i = 0; i < n; ++i) {
+            uint32_t d = (uint32_t)(keys[i] >> 59), u = (uint32_t)((keys[i] >> 32) & 0x07FFFFFFu);
+            uint32_t v = (uint32_t)keys[i];
+            if (d >= h->nd || u >= dv_count || v >= dv_count)
+                return fail(h, CGB_ERR_ARG, "key %llu out of range (dir %u u %u v %u, dv %u)",
+                            (unsigned long long)i, d, u, v, dv_count);
+            card[d]++;
+            uint8_t& s = seen[(size_t)d * dv_count + u];
+            if (!s) { s = 1; nodes[d]++; }
+        }
+    }
+    float avg[kMaxDir] = {0};
+    for (uint32_t d = 0; d < h->nd; ++d) avg[d] = nodes[d] ? (float)card[d] / (float)nodes[d] : 0.f;
+    cgb::plan_edges(h->q, avg, h->plans);
+    CK(cudaMemcpyToSymbol(c_plan, h->plans, sizeof(EdgePlan) * kMaxQE));
+
+    h->dv = dv_count;
+    cgb_status s;
+    if ((s = ensure_dvcap(h, std::max<uint32_t>(dv_count, 1))) != CGB_OK) return s;
+    unsigned long long cap = h->cfg.pool_words;
+    if (cap == 0) cap = std::max<unsigned long long>(4ull * n + (16ull << 20), 64ull << 20);
+    CK(cudaMalloc(&h->pool, cap * sizeof(uint32_t)));
+    h->pool_cap = cap;
+    h->h_pool_top = 0;
+    h->h_live = 0;
+    CK(cudaMemsetAsync(h->d_scal, 0, 4 * sizeof(unsigned long long), h->stream));
+    if ((s = grow(h, h->d_keys_in, h->keys_in_cap, std::max<uint64_t>(n, 1))) != CGB_OK) return s;
+    if (n) CK(cudaMemcpyAsync(h->d_keys_in, keys, n * sizeof(uint64_t), cudaMemcpyHostToDevice, h->stream));
+    if ((s = apply_edits(h, h->d_keys_in, n, nullptr, 0, nullptr, 0)) != CGB_OK) return s;
+    if ((s = sync_scalars(h)) != CGB_OK) return s;
+    if (h->h_scal[2]) return fail(h, CGB_ERR_ARG, "invalid keys (error bits %llu)", h->h_scal[2]);
+    h->have_index = true;
+    return CGB_OK;
+}
+
+cgb_status cgb_apply_batch_device(cgb_handle* h, uint32_t dv_count, const uint64_t* ins, uint64_t n_ins,
+                                  const uint64_t* del, uint64_t n_del, const uint64_t* delta, uint64_t n_delta,
+                                  const uint8_t* edge_ok, void* stream, uint64_t* out_count) {
+    if (!h || !out_count) return CGB_ERR_ARG;
+    *out_count = 0;
+    if (!h->have_index) return fail(h, CGB_ERR_STATE, "build the index first");
+    if (dv_count < h->dv) return fail(h, CGB_ERR_ARG, "dv_count must not decrease (%u < %u)", dv_count, h->dv);
+    if (dv_count > CGB_MAX_VID) return fail(h, CGB_ERR_LIMIT, "dv_count exceeds 2^27-1");
+    if ((n_ins && !ins) || (n_del && !del) || (n_delta && !delta)) return CGB_ERR_ARG;
+    if (n_delta > 0xffffffffull) return fail(h, CGB_ERR_LIMIT, "delta batch too large");
+    CK(cudaSetDevice(h->device));
+    cudaStream_t user = (cudaStream_t)stream;
+    if (user && user != h->stream) {
+        // order this batch after the caller's prior work on `user`
+        CK(cudaEventRecord(h->ev[4], user));
+        CK(cudaStreamWaitEvent(h->stream, h->ev[4], 0));
+    }
+    cgb_status s;
+    if ((s = ensure_dvcap(h, dv_count)) != CGB_OK) return s;
+    h->dv = dv_count;
+    const uint32_t B = bits_for(dv_count);
+    PackInfo pi{B, h->nd, dv_count};
+    unsigned int* d_err = (unsigned int*)(h->d_scal + 2);
+    CK(cudaMemsetAsync(h->d_scal + 2, 0, 2 * sizeof(unsigned long long), h->stream));
+    CK(cudaMemsetAsync(h->d_counts, 0, kMaxQE * sizeof(unsigned long long), h->stream));
+    CK(cudaEventRecord(h->ev[0], h->stream));
+
+    // 1. index update: pending delta (add) + ins (add) + del (remove)
+    if ((s = apply_edits(h, h->d_pending, h->n_pending, ins, n_ins, del, n_del)) != CGB_OK) return s;
+    h->n_pending = 0;
+    CK(cudaEventRecord(h->ev[1], h->stream));
+
+    // 2. delta lists
+    const bool match = n_delta > 0;
+    if (match) {
+        if ((s = ensure_delta_buffers(h, n_delta)) != CGB_OK) return s;
+        uint32_t* du = h->d_ddu;
+        k_pack_delta<<<grid_for(h, n_delta), 256, 0, h->stream>>>(delta, n_delta, pi, h->d_dkeys, d_err);
+        LAUNCHED();
+        if ((s = radix_sort(h, h->d_dkeys, h->d_dkeys_alt, n_delta, 2 * (int)B + 6)) != CGB_OK) return s;
+        k_delta_values<<<grid_for(h, n_delta), 256, 0, h->stream>>>(h->d_dkeys, n_delta, (1ull << B) - 1, h->d_dval);
+        LAUNCHED();
+        k_extract_du<<<grid_for(h, n_delta), 256, 0, h->stream>>>(h->d_dkeys, n_delta, B, du);
+        LAUNCHED();
+        if ((s = segment(h, du, n_delta, h->d_drun_du, h->d_drun_len, h->d_drun_off, h->d_num_runs + 1)) != CGB_OK)
+            return s;
+        k_delta_recs<<<grid_for(h, n_delta), 256, 0, h->stream>>>(h->rec, h->dvcap, h->d_drun_du, h->d_drun_len,
+                                                                   h->d_drun_off, h->d_num_runs + 1, B, 0);
+        LAUNCHED();
+        if (edge_ok) CK(cudaMemcpyAsync(h->d_edge_ok, edge_ok, h->q.qe, cudaMemcpyHostToDevice, h->stream));
+        k_seed_ranges<<<1, 32, 0, h->stream>>>(h->d_dkeys, n_delta, B, h->q.qe, h->d_qe_dirs, h->d_edge_ok,
+                                               edge_ok ? 1 : 0, h->d_seed, h->d_seed + kMaxQE);
+        LAUNCHED();
+        CK(cudaGetLastError());
+        CK(cudaEventRecord(h->ev[2], h->stream));
+
+        // 3. matching
+        DfsArgs da;
+        da.rec = h->rec;
+        da.dvcap = h->dvcap;
+        da.pool = h->pool;
+        da.dval = h->d_dval;
+        da.dkeys = h->d_dkeys;
+        da.B = B;
+        da.qe = h->q.qe;
+        da.seed_lo = h->d_seed;
+        da.seed_pre = h->d_seed + kMaxQE;
+        da.counts = h->d_counts;
+        da.work_next = (unsigned int*)(h->d_scal + 3);
+        int bps = h->cfg.dfs_blocks_per_sm ? (int)h->cfg.dfs_blocks_per_sm : 8;
+        k_dfs_count<<<h->num_sms * bps, kDfsWarps * 32, 0, h->stream>>>(da);
+        LAUNCHED();
+        CK(cudaGetLastError());
+        CK(cudaEventRecord(h->ev[3], h->stream));
+
+        // 4. clear delta records; this delta becomes the pending merge-back
+        k_delta_recs<<<grid_for(h, n_delta), 256, 0, h->stream>>>(h->rec, h->dvcap, h->d_drun_du, h->d_drun_len,
+                                                                   h->d_drun_off, h->d_num_runs + 1, B, 1);
+        LAUNCHED();
+        if ((s = grow(h, h->d_pending, h->pending_cap, n_delta)) != CGB_OK) return s;
+        CK(cudaMemcpyAsync(h->d_pending, delta, n_delta * sizeof(uint64_t), cudaMemcpyDeviceToDevice, h->stream));
+        h->n_pending = n_delta;
+    } else {
+        CK(cudaEventRecord(h->ev[2], h->stream));
+        CK(cudaEventRecord(h->ev[3], h->stream));
+    }
+    if ((s = sync_scalars(h)) != CGB_OK) return s;
+    float t01 = 0, t12 = 0, t23 = 0, t03 = 0;
+    cudaEventElapsedTime(&t01, h->ev[0], h->ev[1]);
+    cudaEventElapsedTime(&t12, h->ev[1], h->ev[2]);
+    cudaEventElapsedTime(&t23, h->ev[2], h->ev[3]);
+    cudaEventElapsedTime(&t03, h->ev[0], h->ev[3]);
+    h->last_t[0] = t01; h->last_t[1] = t12; h->last_t[2] = t23; h->last_t[3] = t03;
+    if (h->h_scal[2]) {
+        h->n_pending = 0;
+        return fail(h, (h->h_scal[2] & 4u) ? CGB_ERR_OOM : CGB_ERR_ARG,
+                    "batch rejected: error bits %llu (1/2 = key out of range, 4 = pool exhausted)", h->h_scal[2]);
+    }
+    uint64_t total = 0;
+    for (uint32_t e = 0; e < h->q.qe; ++e) { h->last_counts[e] = h->h_scal[4 + e]; total += h->h_scal[4 + e]; }
+    *out_count = total;
+    if (h->cfg.flags & CGB_FLAG_NO_MERGE_BACK_DEFER) {
+        if ((s = flush_pending(h)) != CGB_OK) return s;
+    }
+    return CGB_OK;
+}
+
+cgb_status cgb_apply_batch(cgb_handle* h, uint32_t dv_count, const uint64_t* ins, uint64_t n_ins,
+                           const uint64_t* del, uint64_t n_del, const uint64_t* delta, uint64_t n_delta,
+                           const uint8_t* edge_ok, uint64_t* out_count) {
+    if (!h || !out_count) return CGB_ERR_ARG;
+    if ((n_ins && !ins) || (n_del && !del) || (n_delta && !delta)) return CGB_ERR_ARG;
+    CK(cudaSetDevice(h->device));
+    const uint64_t n = n_ins + n_del + n_delta;
+    cgb_status s;
+    if ((s = grow(h, h->d_keys_in, h->keys_in_cap, std::max<uint64_t>(n, 1))) != CGB_OK) return s;
+    uint64_t* d = h->d_keys_in;
+    if (n_ins) CK(cudaMemcpyAsync(d, ins, n_ins * 8, cudaMemcpyHostToDevice, h->stream));
+    if (n_del) CK(cudaMemcpyAsync(d + n_ins, del, n_del * 8, cudaMemcpyHostToDevice, h->stream));
+    if (n_delta) CK(cudaMemcpyAsync(d + n_ins + n_del, delta, n_delta * 8, cudaMemcpyHostToDevice, h->stream));
+    return cgb_apply_batch_device(h, dv_count, d, n_ins, d + n_ins, n_del, d + n_ins + n_del, n_delta, edge_ok,
+                                  nullptr, out_count);
+}
+
+cgb_status cgb_last_edge_counts(const cgb_handle* h, uint64_t* out, uint32_t cap) {
+    if (!h || !out) return CGB_ERR_ARG;
+    for (uint32_t e = 0; e < cap && e < h->q.qe; ++e) out[e] = h->last_counts[e];
+    return CGB_OK;
+}
+
+cgb_status cgb_last_timings(const cgb_handle* h, float* t4) {
+    if (!h || !t4) return CGB_ERR_ARG;
+    for (int i = 0; i < 4; ++i) t4[i] = h->last_t[i];
+    return CGB_OK;
+}
+
+uint64_t cgb_kernel_launches(const cgb_handle* h) { return h ? h->launches : 0; }
+
+cgb_status cgb_read_index(cgb_handle* h, uint64_t* out, uint64_t cap, uint64_t* n_out) {
+    if (!h || !n_out) return CGB_ERR_ARG;
+    if (!h->have_index) return fail(h, CGB_ERR_STATE, "no index");
+    CK(cudaSetDevice(h->device));
+    cgb_status s;
+    if ((s = flush_pending(h)) != CGB_OK) return s;
+    const uint64_t n = (uint64_t)h->nd * h->dv;
+    uint32_t* lens = nullptr;
+    unsigned long long* offs = nullptr;
+    CK(cudaMalloc(&lens, std::max<uint64_t>(n, 1) * sizeof(uint32_t)));
+    CK(cudaMalloc(&offs, (n + 1) * sizeof(unsigned long long)));
+    CK(cudaMemsetAsync(offs, 0, (n + 1) * sizeof(unsigned long long), h->stream));
+    if (n) {
+        k_rec_sizes<<<grid_for(h, n), 256, 0, h->stream>>>(h->rec, h->dvcap, h->dv, h->nd, nullptr, lens);
+        LAUNCHED();
+        k_u32_to_u64<<<grid_for(h, n), 256, 0, h->stream>>>(lens, offs, n);
+        LAUNCHED();
+    }
+    size_t tb = 0;
+    CK(cub::DeviceScan::ExclusiveSum(nullptr, tb, offs, offs, (int64_t)n + 1, h->stream));
+    if ((s = grow_temp(h, tb)) != CGB_OK) return s;
+    CK(cub::DeviceScan::ExclusiveSum(h->d_temp, tb, offs, offs, (int64_t)n + 1, h->stream));
+    LAUNCHED();
+    unsigned long long total = 0;
+    CK(cudaMemcpyAsync(&total, offs + n, sizeof(total), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    *n_out = total;
+    if (out && cap >= total && total > 0) {
+        uint64_t* d_out = nullptr;
+        CK(cudaMalloc(&d_out, total * sizeof(uint64_t)));
+        k_dump<<<grid_for(h, n * 32), 256, 0, h->stream>>>(h->rec, h->dvcap, h->dv, h->nd, h->pool, offs, d_out);
+        LAUNCHED();
+        CK(cudaMemcpyAsync(out, d_out, total * sizeof(uint64_t), cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        CK(cudaFree(d_out));
+    } else if (out && cap < total) {
+        CK(cudaFree(lens));
+        CK(cudaFree(offs));
+        return fail(h, CGB_ERR_ARG, "output capacity %llu < %llu", (unsigned long long)cap, total);
+    }
+    CK(cudaFree(lens));
+    CK(cudaFree(offs));
+    return CGB_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,146 @@
+#include "query.h"
+
+#include <algorithm>
+#include <cstring>
+#include <fstream>
+#include <sstream>
+
+namespace cgb {
+
+std::string parse_query_file(const std::string& path, std::vector<uint32_t>& labels,
+                             std::vector<uint32_t>& edges, uint32_t& qv) {
+    // Text format of graph.cpp:57-114 / calig.cpp:111-164: 't' lines are
+    // skipped, "v id label", "e a b label".
+    std::ifstream in(path);
+    if (!in) return "cannot open query file " + path;
+    labels.clear();
+    edges.clear();
+    qv = 0;
+    std::string line;
+    while (std::getline(in, line)) {
+        std::istringstream ss(line);
+        char t;
+        if (!(ss >> t)) continue;
+        if (t == 'v') {
+            uint32_t id, lb;
+            if (!(ss >> id >> lb)) return "bad vertex line: " + line;
+            if (id >= labels.size()) labels.resize(id + 1, 0);
+            labels[id] = lb;
+            qv = std::max(qv, id + 1);
+        } else if (t == 'e') {
+            uint32_t a, b;
+            if (!(ss >> a >> b)) return "bad edge line: " + line;
+            edges.push_back(a);
+            edges.push_back(b);
+        }
+    }
+    return "";
+}
+
+std::string build_query_meta(uint32_t qv, uint32_t qe, const uint32_t* edges, QueryMeta& q) {
+    if (qv < 2 || qv > (uint32_t)kMaxQV) return "query must have 2..12 vertices";
+    if (qe == 0 || 2 * qe > (uint32_t)kMaxDir) return "query must have 1..16 edges (5-bit directed index)";
+    q = QueryMeta();
+    q.qv = qv;
+    q.nbrs.assign(qv, {});
+    for (uint32_t i = 0; i < qe; ++i) {
+        uint32_t a = edges[2 * i], b = edges[2 * i + 1];
+        if (a >= qv || b >= qv || a == b) return "bad query edge";
+        auto& na = q.nbrs[a];
+        if (std::find(na.begin(), na.end(), b) != na.end()) return "duplicate query edge";
+        na.push_back(b);
+        q.nbrs[b].push_back(a);
+    }
+    for (auto& n : q.nbrs) std::sort(n.begin(), n.end());
+    std::memset(q.eidx, 255, sizeof(q.eidx));
+    uint32_t pos = 0;
+    for (uint32_t u = 0; u < qv; ++u)
+        for (uint32_t w : q.nbrs[u]) {
+            q.eidx[u * kMaxQV + w] = (uint8_t)pos;
+            q.dir_src[pos] = (uint8_t)u;
+            q.dir_dst[pos] = (uint8_t)w;
+            ++pos;
+        }
+    q.nd = pos;
+    uint32_t e = 0;
+    for (uint32_t u = 0; u < qv; ++u)
+        for (uint32_t w : q.nbrs[u]) {
+            if (u > w) continue;
+            q.qe_u[e] = (uint8_t)u;
+            q.qe_v[e] = (uint8_t)w;
+            q.qe_dir[e][0] = q.eidx[u * kMaxQV + w];
+            q.qe_dir[e][1] = q.eidx[w * kMaxQV + u];
+            q.dir_to_edge[q.qe_dir[e][0]] = (uint8_t)e;
+            q.dir_to_edge[q.qe_dir[e][1]] = (uint8_t)e;
+            ++e;
+        }
+    q.qe = e;
+    return "";
+}
+
+// Per-edge vertex order: ei's endpoints first (the delta edge is the seed),
+// then greedily the unvisited vertex with the most visited neighbours, ties
+// broken by the smallest estimated candidate count (min avg run length over
+// its backward edges), then by vertex id.  The tie-breaking criteria restate
+// the reference's global-order rules 1 and 4 (plan.cpp:595-708); the start is
+// the delta edge instead of a global edge because matching is seeded from the
+// delta lists.
+void plan_edges(const QueryMeta& q, const float* avg_deg, EdgePlan* plans) {
+    for (uint32_t ei = 0; ei < q.qe; ++ei) {
+        EdgePlan& p = plans[ei];
+        std::memset(&p, 0, sizeof(p));
+        p.n = (uint8_t)q.qv;
+        uint32_t a = q.qe_u[ei], b = q.qe_v[ei];
+        // seed from the endpoint whose other edges are more selective
+        p.vs[0] = (uint8_t)a;
+        p.vs[1] = (uint8_t)b;
+        p.seed_dir = q.eidx[a * kMaxQV + b];
+        std::vector<int> pos(q.qv, -1);
+        pos[a] = 0;
+        pos[b] = 1;
+        for (uint32_t j = 2; j < q.qv; ++j) {
+            int best = -1, best_bn = -1;
+            float best_est = 0.f;
+            for (uint32_t u = 0; u < q.qv; ++u) {
+                if (pos[u] >= 0) continue;
+                int nbn = 0;
+                float est = 3.4e38f;
+                for (uint32_t w : q.nbrs[u])
+                    if (pos[w] >= 0) {
+                        ++nbn;
+                        est = std::min(est, avg_deg[q.eidx[w * kMaxQV + u]]);
+                    }
+                if (nbn == 0) continue;
+                if (nbn > best_bn || (nbn == best_bn && est < best_est)) {
+                    best = (int)u;
+                    best_bn = nbn;
+                    best_est = est;
+                }
+            }
+            if (best < 0) {  // disconnected query: take the smallest unvisited vertex
+                for (uint32_t u = 0; u < q.qv; ++u)
+                    if (pos[u] < 0) { best = (int)u; break; }
+            }
+            pos[best] = (int)j;
+            p.vs[j] = (uint8_t)best;
+        }
+        uint32_t k = 0;
+        for (uint32_t j = 0; j < q.qv; ++j) {
+            p.bn_off[j] = (uint8_t)k;
+            if (j < 2) continue;
+            uint32_t u = p.vs[j];
+            for (uint32_t t = 0; t < j; ++t) {
+                uint32_t w = p.vs[t];
+                uint8_t d = q.eidx[w * kMaxQV + u];
+                if (d == 255) continue;
+                p.bn_pos[k] = (uint8_t)t;
+                p.bn_dir[k] = d;
+                p.bn_dvis[k] = q.dir_to_edge[d] < ei ? 1 : 0;
+                ++k;
+            }
+        }
+        p.bn_off[q.qv] = (uint8_t)k;
+    }
+}
+
+}  // namespace cgb

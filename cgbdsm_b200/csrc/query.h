@@ -1,0 +1,50 @@
+// Query pattern metadata and per-edge matching plans (host side).
+#pragma once
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace cgb {
+
+constexpr int kMaxQV = 12;   // utils/config.h:5 (MAX_VCOUNT)
+constexpr int kMaxDir = 32;  // 5-bit directed index in the key (calig_helper_gamma.cu:228)
+constexpr int kMaxQE = 16;
+constexpr int kMaxBN = 48;
+
+// Query graph metadata, numbered exactly as the reference numbers it:
+//   dir index  graph.cpp:137-148  (vertex ascending, neighbour ascending)
+//   edge order graph.cpp:184-199  ((u, uu) with u < uu, u ascending then uu)
+struct QueryMeta {
+    uint32_t qv = 0, qe = 0, nd = 0;
+    std::vector<uint32_t> labels;                  // file labels (unused by the GPU path)
+    std::vector<std::vector<uint32_t>> nbrs;       // sorted neighbour lists
+    uint8_t eidx[kMaxQV * kMaxQV];                 // 255 = no edge
+    uint8_t qe_u[kMaxQE], qe_v[kMaxQE];            // undirected edges
+    uint8_t qe_dir[kMaxQE][2];                     // eidx(u,v), eidx(v,u)
+    uint8_t dir_to_edge[kMaxDir];
+    uint8_t dir_src[kMaxDir], dir_dst[kMaxDir];
+};
+
+// Matching plan of one query edge ei: vertex order starting at ei's endpoints,
+// and for every later position the backward neighbours (BN) whose lists
+// constrain it.  bn_dvis marks BN directions whose delta part is visible to
+// ei (dir_to_edge < ei; enumeration.cu:937, cpu_dfs.cpp:76-77).
+struct EdgePlan {
+    uint8_t n;
+    uint8_t seed_dir;
+    uint8_t vs[kMaxQV];
+    uint8_t bn_off[kMaxQV + 1];
+    uint8_t bn_pos[kMaxBN];
+    uint8_t bn_dir[kMaxBN];
+    uint8_t bn_dvis[kMaxBN];
+    uint8_t pad[3];
+};
+
+// Returns "" on success, else an error message.
+std::string build_query_meta(uint32_t qv, uint32_t qe, const uint32_t* edges, QueryMeta& q);
+std::string parse_query_file(const std::string& path, std::vector<uint32_t>& labels,
+                             std::vector<uint32_t>& edges, uint32_t& qv);
+// avg_deg[dir]: mean run length of direction dir in the initial index.
+void plan_edges(const QueryMeta& q, const float* avg_deg, EdgePlan* plans);
+
+}  // namespace cgb

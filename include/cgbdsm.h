@@ -1,0 +1,138 @@
+/*
+ * cgbdsm.h — C ABI of the B200 continuous-subgraph-matching engine.
+ *
+ * The engine owns, on one CUDA device, the per-batch GPU half of the
+ * reference's pipeline ("Stage 2", main_calig.cpp:281-384):
+ *
+ *   index update     TransferUpdateAll        calig_helper_gamma.cu:485-517
+ *   delta lists      TransferUpdateIndex      calig_helper_gamma.cu:569-597
+ *   matching         MatchingBitAll           graph_gpu.cu:1261-1480
+ *   delta merge-back BatchUpdateGlobalIndex   calig_helper_gamma.cu:539-567
+ *
+ * Inputs are the reference's 64-bit keys
+ *     key = (dir << 59) | (u << 32) | v
+ * with dir the directed query-edge index (graph.cpp:137-148, < 32), u and v
+ * compressed data-vertex ids (< 2^27, calig_helper_gamma.cu:77-105, 228-229).
+ *
+ * Conventions: every call returns a cgb_status; nothing calls exit().  A handle
+ * is used by one host thread at a time; distinct handles are independent.
+ * Host pointers are plain host memory unless a name says "device".
+ */
+#ifndef CGBDSM_H
+#define CGBDSM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    CGB_OK = 0,
+    CGB_ERR_ARG = 1,      /* invalid argument (sizes, ids, key fields)          */
+    CGB_ERR_CUDA = 2,     /* CUDA runtime error; cgb_last_error() has the text   */
+    CGB_ERR_OOM = 3,      /* device allocation failed                            */
+    CGB_ERR_LIMIT = 4,    /* a documented limit was exceeded                     */
+    CGB_ERR_STATE = 5,    /* call out of order (e.g. batch before index build)   */
+    CGB_ERR_TIMEOUT = 6,  /* a bounded device wait ran out                       */
+    CGB_ERR_IO = 7        /* file could not be read                              */
+} cgb_status;
+
+typedef struct cgb_handle cgb_handle;
+
+typedef struct {
+    int device;              /* CUDA device ordinal (reference: argv[4], main_calig.cpp:64) */
+    uint64_t pool_words;     /* neighbour-run pool capacity in u32 words; 0 = automatic     */
+    uint32_t dfs_blocks_per_sm; /* persistent DFS blocks per SM; 0 = automatic              */
+    uint32_t flags;          /* CGB_FLAG_* below                                           */
+} cgb_config;
+
+#define CGB_FLAG_NO_MERGE_BACK_DEFER 0x1u /* apply the delta merge-back eagerly after matching */
+
+/* Limits (reference: utils/config.h:5-6; key layout calig_helper_gamma.cu:228-229). */
+#define CGB_MAX_QV 12
+#define CGB_MAX_DIR 32
+#define CGB_MAX_VID ((1u << 27) - 1u)
+
+/* Fills *cfg with defaults (device 0, automatic sizes). */
+void cgb_default_config(cgb_config* cfg);
+
+/* Creates an engine on cfg->device.  Replaces GPUGraphLoader's constructor
+ * (graph_gpu.cu:58-102) and CaLiGHelperGamma's (calig_helper_gamma.cu:19-49). */
+cgb_status cgb_create(const cgb_config* cfg, cgb_handle** out);
+void cgb_destroy(cgb_handle* h);
+/* Text of the last error on this handle ("" if none).  Valid until the next call. */
+const char* cgb_last_error(const cgb_handle* h);
+
+/* Loads the query pattern: qv vertices (<= 12), qe undirected edges given as
+ * (a, b) pairs, a != b.  Directed indices follow graph.cpp:137-148 (CSR order:
+ * vertex ascending, neighbour ascending); undirected edge order graph.cpp:184-199.
+ * Replaces CPUGraphLoader::SetQueryMeta + GPUGraphLoader::LoadQuery
+ * (graph.cpp:123-209, graph_gpu.cu:156-172).  2*qe must be <= 32. */
+cgb_status cgb_load_query(cgb_handle* h, uint32_t qv, uint32_t qe, const uint32_t* edges);
+/* Same, from a query file in the reference text format (graph.cpp:43-121). */
+cgb_status cgb_load_query_file(cgb_handle* h, const char* path);
+/* Directed index of query edge (a -> b), or 255 if not an edge. */
+uint32_t cgb_query_dir(const cgb_handle* h, uint32_t a, uint32_t b);
+
+/* Builds the initial device index from keys (any order, no duplicates) over
+ * dv_count compressed vertices, and plans the matching orders from the index's
+ * per-direction cardinalities.  Replaces ConvertGlobalIndex
+ * (calig_helper_gamma.cu:238-360) + Plan::GenerateMatchingOrders_v2 + LoadPlan
+ * + AllocOnline (plan.cpp:31-54, graph_gpu.cu:174-209). */
+cgb_status cgb_build_index(cgb_handle* h, const uint64_t* keys, uint64_t n, uint32_t dv_count);
+
+/* One batch, host buffers (copied to the device inside the call):
+ *   ins    keys inserted into the index (LI-filtered by the producer);
+ *          duplicates allowed, deduplicated (calig_helper_gamma.cu:254-256)
+ *   del    keys removed from the index (calig_helper_gamma.cu:260-265)
+ *   delta  this batch's delta keys: matched with the delta visibility rule,
+ *          then merged into the index (calig_helper_gamma.cu:569-597, 539-567)
+ *   dv_count  compressed-vertex count after this batch's mapping update
+ *          (non-decreasing; calig_helper_gamma.cu:107-130)
+ *   edge_ok   optional (NULL = derived): per undirected query edge, non-zero if
+ *          both of its directions have delta keys (calig_helper_gamma.cu:436-444)
+ *   *out_count  positive matches of this batch (graph_gpu.cu:1261-1480):
+ *          sum over query edges ei with edge_ok of the embeddings that map ei to
+ *          a delta edge, edges e < ei to old-or-delta edges, edges e > ei to old
+ *          edges only (enumeration.cu:768, 797, 937).
+ * Order of effects, as in the reference: index := (index + ins) - del; match;
+ * index := index + delta.  An empty delta skips matching and the merge-back
+ * (main_calig.cpp:301-302) and yields *out_count = 0. */
+cgb_status cgb_apply_batch(cgb_handle* h, uint32_t dv_count,
+                           const uint64_t* ins, uint64_t n_ins,
+                           const uint64_t* del, uint64_t n_del,
+                           const uint64_t* delta, uint64_t n_delta,
+                           const uint8_t* edge_ok, uint64_t* out_count);
+
+/* Same batch with the three key arrays already in device memory (HBM) and the
+ * work enqueued on `stream` (a cudaStream_t; NULL = the handle's stream).
+ * The count is written to *out_count after the call returns (it synchronizes
+ * the stream once at the end). */
+cgb_status cgb_apply_batch_device(cgb_handle* h, uint32_t dv_count,
+                                  const uint64_t* ins_device, uint64_t n_ins,
+                                  const uint64_t* del_device, uint64_t n_del,
+                                  const uint64_t* delta_device, uint64_t n_delta,
+                                  const uint8_t* edge_ok, void* stream,
+                                  uint64_t* out_count);
+
+/* Per-query-edge counts of the last batch (qe entries). */
+cgb_status cgb_last_edge_counts(const cgb_handle* h, uint64_t* out, uint32_t cap);
+
+/* The current index (after any pending delta merge-back) as sorted keys.
+ * With out == NULL only *n is set.  Replaces reading RelationsGPU
+ * (graph_gpu.h:41-49) for parity checks. */
+cgb_status cgb_read_index(cgb_handle* h, uint64_t* out, uint64_t cap, uint64_t* n);
+
+/* Timing of the last batch on the device (CUDA events, milliseconds):
+ * t[0] index update, t[1] delta lists, t[2] matching, t[3] total. */
+cgb_status cgb_last_timings(const cgb_handle* h, float* t4);
+
+/* Number of kernels this engine has launched so far. */
+uint64_t cgb_kernel_launches(const cgb_handle* h);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CGBDSM_H */

@@ -1,0 +1,526 @@
+/*
+ * oracle.c — CPU restatement of the reference's per-batch GPU path.
+ *
+ * TEST INFRASTRUCTURE ONLY: tests/, the smoke check and bench.py's
+ * cpu_baseline leg use it as the checker.  The product never links it.
+ *
+ * Parity pin: tests/test_oracle_pin.py runs this restatement and the
+ * reference's own CPU path (oracle/_ref/libcgbref.so, built from the
+ * reference's unmodified calig.cpp / cpu_index_mirror.cpp / cpu_dfs.cpp) on
+ * the same seeded inputs and requires identical counts and index contents;
+ * tests/golden/ holds the vectors that pin it without the reference tree.
+ *
+ * What it restates (reference file:line):
+ *   index set semantics   cpu_index_mirror.cpp:132-229 (MergeInsert = sort,
+ *                         unique, set_union; MergeRemove = sort,
+ *                         set_difference), InitFromSortedEdges :98-130
+ *   delta lists           cpu_index_mirror.cpp:231-269 (RebuildUpdate: sorted,
+ *                         not deduplicated)
+ *   batch order           main_calig.cpp:294-349: ins, del, [match], delta
+ *                         merge-back; an empty delta skips both
+ *                         (main_calig.cpp:301-302)
+ *   query numbering       graph.cpp:137-148 (directed), :184-199 (undirected)
+ *   matching semantics    cpu_dfs.cpp:64-132: for edge ei, lists of ei's own
+ *                         directions are the delta lists only; other
+ *                         directions are the main list plus the delta list
+ *                         when dir_to_edge < ei; candidates from the first
+ *                         backward neighbour, membership in the others,
+ *                         injectivity against all matched vertices.
+ *   seeding               enumeration.cu:727-809 without masks: every vertex
+ *                         dv, every entry of the resolved list of the order's
+ *                         first edge.
+ * Two seeding modes are provided:
+ *   ORC_GLOBAL  the reference's: one global vertex order for every ei, seeds
+ *               over all dv (exactly cpu_dfs semantics given that order)
+ *   ORC_PER_EDGE  per-edge orders starting at ei's endpoints, seeds = delta
+ *               entries of ei; equal to ORC_GLOBAL whenever the index lists
+ *               are symmetric ((a->b) contains y at x iff (b->a) contains x
+ *               at y), which tests/ check as a property.
+ * Plus an independent brute-force embedding counter for the incremental
+ * identity  sum(batch counts) = |Emb(Q, G_after)| - |Emb(Q, G_before)|.
+ */
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define ORC_MAXQV 12
+#define ORC_MAXD 32
+#define ORC_MAXQE 16
+
+enum { ORC_GLOBAL = 0, ORC_PER_EDGE = 1 };
+
+typedef struct {
+    uint32_t* v;
+    uint32_t n, cap;
+} List;
+
+typedef struct {
+    uint32_t qv, qe, nd;
+    uint8_t eidx[ORC_MAXQV * ORC_MAXQV];
+    uint8_t qe_u[ORC_MAXQE], qe_v[ORC_MAXQE];
+    uint8_t dir_to_edge[ORC_MAXD];
+    uint32_t dv, dvcap;
+    List* main;   /* [nd * dvcap] */
+    List* delta;  /* [nd * dvcap] */
+    uint64_t* pending;  /* delta keys of the last matched batch (merged before the next) */
+    uint64_t n_pending;
+    uint64_t last_edge_counts[ORC_MAXQE];
+} Orc;
+
+static int cmp_u64(const void* a, const void* b) {
+    uint64_t x = *(const uint64_t*)a, y = *(const uint64_t*)b;
+    return x < y ? -1 : x > y;
+}
+static int cmp_u32(const void* a, const void* b) {
+    uint32_t x = *(const uint32_t*)a, y = *(const uint32_t*)b;
+    return x < y ? -1 : x > y;
+}
+
+static void list_reserve(List* l, uint32_t n) {
+    if (n <= l->cap) return;
+    uint32_t c = l->cap ? l->cap : 4;
+    while (c < n) c *= 2;
+    l->v = (uint32_t*)realloc(l->v, (size_t)c * 4);
+    l->cap = c;
+}
+
+static int list_has(const List* l, uint32_t x) {
+    uint32_t lo = 0, hi = l->n;
+    while (lo < hi) {
+        uint32_t m = (lo + hi) >> 1;
+        if (l->v[m] < x) lo = m + 1; else hi = m;
+    }
+    return lo < l->n && l->v[lo] == x;
+}
+
+static void grow_dv(Orc* o, uint32_t dv) {
+    if (dv <= o->dvcap) { if (dv > o->dv) o->dv = dv; return; }
+    uint32_t nc = o->dvcap ? o->dvcap : 64;
+    while (nc < dv) nc *= 2;
+    List* nm = (List*)calloc((size_t)o->nd * nc, sizeof(List));
+    List* ndl = (List*)calloc((size_t)o->nd * nc, sizeof(List));
+    for (uint32_t d = 0; d < o->nd; ++d)
+        for (uint32_t u = 0; u < o->dvcap; ++u) {
+            nm[(size_t)d * nc + u] = o->main[(size_t)d * o->dvcap + u];
+            ndl[(size_t)d * nc + u] = o->delta[(size_t)d * o->dvcap + u];
+        }
+    free(o->main);
+    free(o->delta);
+    o->main = nm;
+    o->delta = ndl;
+    o->dvcap = nc;
+    o->dv = dv;
+}
+
+#define KD(k) ((uint32_t)((k) >> 59))
+#define KU(k) ((uint32_t)(((k) >> 32) & 0x07FFFFFFu))
+#define KV(k) ((uint32_t)(k))
+
+/* Applies sorted keys to main lists: set union (is_insert) or set difference. */
+static void merge_sorted(Orc* o, const uint64_t* s, uint64_t n, int is_insert) {
+    uint64_t i = 0;
+    uint32_t* tmp = NULL;
+    size_t tcap = 0;
+    while (i < n) {
+        uint32_t d = KD(s[i]), u = KU(s[i]);
+        uint64_t j = i;
+        while (j < n && KD(s[j]) == d && KU(s[j]) == u) ++j;
+        List* l = &o->main[(size_t)d * o->dvcap + u];
+        size_t need = (size_t)l->n + (j - i);
+        if (need > tcap) { tcap = need * 2; tmp = (uint32_t*)realloc(tmp, tcap * 4); }
+        uint32_t a = 0, c = 0;
+        uint64_t b = i;
+        while (a < l->n || b < j) {
+            if (b >= j || (a < l->n && l->v[a] < KV(s[b]))) tmp[c++] = l->v[a++];
+            else if (a >= l->n || KV(s[b]) < l->v[a]) { if (is_insert) tmp[c++] = KV(s[b]); ++b; }
+            else { if (is_insert) tmp[c++] = l->v[a]; ++a; ++b; }
+        }
+        list_reserve(l, c);
+        memcpy(l->v, tmp, (size_t)c * 4);
+        l->n = c;
+        i = j;
+    }
+    free(tmp);
+}
+
+static uint64_t* sorted_copy(const uint64_t* k, uint64_t n, int unique, uint64_t* out_n) {
+    uint64_t* s = (uint64_t*)malloc((n ? n : 1) * 8);
+    memcpy(s, k, n * 8);
+    qsort(s, n, 8, cmp_u64);
+    if (unique && n) {
+        uint64_t w = 1;
+        for (uint64_t i = 1; i < n; ++i) if (s[i] != s[w - 1]) s[w++] = s[i];
+        n = w;
+    }
+    *out_n = n;
+    return s;
+}
+
+/* ------------------------------------------------------------------ API */
+
+void* orc_create(uint32_t qv, uint32_t qe, const uint32_t* edges) {
+    if (qv < 2 || qv > ORC_MAXQV || qe == 0 || 2 * qe > ORC_MAXD) return NULL;
+    Orc* o = (Orc*)calloc(1, sizeof(Orc));
+    o->qv = qv;
+    uint8_t adj[ORC_MAXQV][ORC_MAXQV];
+    memset(adj, 0, sizeof(adj));
+    for (uint32_t i = 0; i < qe; ++i) {
+        uint32_t a = edges[2 * i], b = edges[2 * i + 1];
+        if (a >= qv || b >= qv || a == b) { free(o); return NULL; }
+        adj[a][b] = adj[b][a] = 1;
+    }
+    memset(o->eidx, 255, sizeof(o->eidx));
+    uint32_t pos = 0;
+    for (uint32_t u = 0; u < qv; ++u)           /* graph.cpp:137-148 */
+        for (uint32_t w = 0; w < qv; ++w)
+            if (adj[u][w]) o->eidx[u * ORC_MAXQV + w] = (uint8_t)pos++;
+    o->nd = pos;
+    uint32_t e = 0;
+    for (uint32_t u = 0; u < qv; ++u)           /* graph.cpp:184-199 */
+        for (uint32_t w = u + 1; w < qv; ++w)
+            if (adj[u][w]) {
+                o->qe_u[e] = (uint8_t)u;
+                o->qe_v[e] = (uint8_t)w;
+                o->dir_to_edge[o->eidx[u * ORC_MAXQV + w]] = (uint8_t)e;
+                o->dir_to_edge[o->eidx[w * ORC_MAXQV + u]] = (uint8_t)e;
+                ++e;
+            }
+    o->qe = e;
+    return o;
+}
+
+void orc_destroy(void* h) {
+    Orc* o = (Orc*)h;
+    if (!o) return;
+    for (size_t i = 0; i < (size_t)o->nd * o->dvcap; ++i) { free(o->main[i].v); free(o->delta[i].v); }
+    free(o->main);
+    free(o->delta);
+    free(o->pending);
+    free(o);
+}
+
+uint32_t orc_num_dir(void* h) { return ((Orc*)h)->nd; }
+uint32_t orc_num_edges(void* h) { return ((Orc*)h)->qe; }
+uint32_t orc_dir(void* h, uint32_t a, uint32_t b) { return ((Orc*)h)->eidx[a * ORC_MAXQV + b]; }
+
+/* InitFromSortedEdges (cpu_index_mirror.cpp:98-130). */
+int orc_build(void* h, const uint64_t* keys, uint64_t n, uint32_t dv) {
+    Orc* o = (Orc*)h;
+    grow_dv(o, dv ? dv : 1);
+    o->dv = dv;
+    uint64_t m;
+    uint64_t* s = sorted_copy(keys, n, 0, &m);
+    for (uint64_t i = 0; i < m; ++i)
+        if (KD(s[i]) >= o->nd || KU(s[i]) >= dv || KV(s[i]) >= dv) { free(s); return -1; }
+    merge_sorted(o, s, m, 1);
+    free(s);
+    return 0;
+}
+
+/* ---- matching ---- */
+typedef struct {
+    const Orc* o;
+    uint32_t ei;
+    uint8_t vs[ORC_MAXQV];
+    uint8_t bn_off[ORC_MAXQV + 1];
+    uint8_t bn_pos[64], bn_dir[64];
+    int seed_dirs[2];
+    uint32_t m[ORC_MAXQV];
+} Run;
+
+/* cpu_dfs.cpp:67-78: (base, app) of directed edge d at vertex x under ei. */
+static void resolve(const Run* r, uint32_t d, uint32_t x, const List** base, const List** app) {
+    const Orc* o = r->o;
+    size_t i = (size_t)d * o->dvcap + x;
+    int seed = ((int)d == r->seed_dirs[0] || (int)d == r->seed_dirs[1]);
+    *base = seed ? &o->delta[i] : &o->main[i];
+    *app = (o->dir_to_edge[d] < r->ei) ? &o->delta[i] : NULL;
+}
+
+static uint64_t dfs(Run* r, uint32_t j) {
+    const Orc* o = r->o;
+    uint32_t b0 = r->bn_off[j], b1 = r->bn_off[j + 1];
+    const List *gb, *ga;
+    resolve(r, r->bn_dir[b0], r->m[r->bn_pos[b0]], &gb, &ga);
+    uint64_t cnt = 0;
+    for (int part = 0; part < 2; ++part) {
+        const List* L = part ? ga : gb;
+        if (!L) continue;
+        for (uint32_t t = 0; t < L->n; ++t) {
+            uint32_t c = L->v[t];
+            int ok = 1;
+            for (uint32_t k = 0; k < j && ok; ++k) ok = (r->m[k] != c);
+            for (uint32_t k = b0 + 1; k < b1 && ok; ++k) {
+                const List *xb, *xa;
+                resolve(r, r->bn_dir[k], r->m[r->bn_pos[k]], &xb, &xa);
+                ok = list_has(xb, c) || (xa && list_has(xa, c));
+            }
+            if (!ok) continue;
+            if (j + 1 == o->qv) ++cnt;
+            else { r->m[j] = c; cnt += dfs(r, j + 1); }
+        }
+    }
+    return cnt;
+}
+
+static void make_run(const Orc* o, Run* r, uint32_t ei, const uint8_t* order) {
+    memset(r, 0, sizeof(*r));
+    r->o = o;
+    r->ei = ei;
+    memcpy(r->vs, order, o->qv);
+    r->seed_dirs[0] = o->eidx[o->qe_u[ei] * ORC_MAXQV + o->qe_v[ei]];
+    r->seed_dirs[1] = o->eidx[o->qe_v[ei] * ORC_MAXQV + o->qe_u[ei]];
+    uint32_t k = 0;
+    for (uint32_t j = 0; j < o->qv; ++j) {
+        r->bn_off[j] = (uint8_t)k;
+        if (j < 2) continue;
+        /* backward neighbours: the first one generates candidates */
+        for (uint32_t t = 0; t < j; ++t) {
+            uint8_t d = o->eidx[r->vs[t] * ORC_MAXQV + r->vs[j]];
+            if (d == 255) continue;
+            r->bn_pos[k] = (uint8_t)t;
+            r->bn_dir[k] = d;
+            ++k;
+        }
+    }
+    r->bn_off[o->qv] = (uint8_t)k;
+}
+
+/* Per-edge order: endpoints of ei, then BFS-like by most visited neighbours. */
+static void per_edge_order(const Orc* o, uint32_t ei, uint8_t* vs) {
+    uint8_t vis[ORC_MAXQV] = {0};
+    vs[0] = o->qe_u[ei];
+    vs[1] = o->qe_v[ei];
+    vis[vs[0]] = vis[vs[1]] = 1;
+    for (uint32_t j = 2; j < o->qv; ++j) {
+        int best = -1, bn = -1;
+        for (uint32_t u = 0; u < o->qv; ++u) {
+            if (vis[u]) continue;
+            int c = 0;
+            for (uint32_t w = 0; w < o->qv; ++w) if (vis[w] && o->eidx[u * ORC_MAXQV + w] != 255) ++c;
+            if (c > bn) { bn = c; best = (int)u; }
+        }
+        vs[j] = (uint8_t)best;
+        vis[best] = 1;
+    }
+}
+
+static uint64_t count_batch(Orc* o, const uint8_t* edge_ok, int mode, const uint8_t* global_order) {
+    uint64_t total = 0;
+    for (uint32_t ei = 0; ei < o->qe; ++ei) {
+        o->last_edge_counts[ei] = 0;
+        if (!edge_ok[ei]) continue;
+        Run r;
+        uint8_t vs[ORC_MAXQV];
+        if (mode == ORC_GLOBAL) memcpy(vs, global_order, o->qv);
+        else per_edge_order(o, ei, vs);
+        make_run(o, &r, ei, vs);
+        uint64_t c = 0;
+        if (mode == ORC_GLOBAL) {
+            /* enumeration.cu:727-809 without masks: every dv, resolved first-edge list */
+            uint32_t d0 = o->eidx[vs[0] * ORC_MAXQV + vs[1]];
+            for (uint32_t x = 0; x < o->dv; ++x) {
+                const List *b, *a;
+                resolve(&r, d0, x, &b, &a);
+                for (int part = 0; part < 2; ++part) {
+                    const List* L = part ? a : b;
+                    if (!L) continue;
+                    for (uint32_t t = 0; t < L->n; ++t) {
+                        r.m[0] = x;
+                        r.m[1] = L->v[t];
+                        c += (o->qv == 2) ? 1 : dfs(&r, 2);
+                    }
+                }
+            }
+        } else {
+            uint32_t d0 = r.seed_dirs[0];
+            for (uint32_t x = 0; x < o->dv; ++x) {
+                const List* L = &o->delta[(size_t)d0 * o->dvcap + x];
+                for (uint32_t t = 0; t < L->n; ++t) {
+                    r.m[0] = x;
+                    r.m[1] = L->v[t];
+                    c += (o->qv == 2) ? 1 : dfs(&r, 2);
+                }
+            }
+        }
+        o->last_edge_counts[ei] = c;
+        total += c;
+    }
+    return total;
+}
+
+static void flush_pending(Orc* o) {
+    if (!o->n_pending) return;
+    uint64_t m;
+    uint64_t* s = sorted_copy(o->pending, o->n_pending, 1, &m);
+    merge_sorted(o, s, m, 1);
+    free(s);
+    o->n_pending = 0;
+}
+
+/* One batch.  edge_ok may be NULL (derived: both directions have delta keys,
+ * calig_helper_gamma.cu:436-444).  Returns the count, or UINT64_MAX on bad keys. */
+uint64_t orc_batch(void* h, uint32_t dv, const uint64_t* ins, uint64_t n_ins, const uint64_t* del,
+                   uint64_t n_del, const uint64_t* delta, uint64_t n_delta, const uint8_t* edge_ok,
+                   int mode, const uint8_t* global_order) {
+    Orc* o = (Orc*)h;
+    flush_pending(o);  /* BatchUpdateGlobalIndex of the previous batch */
+    grow_dv(o, dv);
+    o->dv = dv;
+    const uint64_t* arrs[3] = {ins, del, delta};
+    uint64_t ns[3] = {n_ins, n_del, n_delta};
+    for (int a = 0; a < 3; ++a)
+        for (uint64_t i = 0; i < ns[a]; ++i)
+            if (KD(arrs[a][i]) >= o->nd || KU(arrs[a][i]) >= dv || KV(arrs[a][i]) >= dv) return UINT64_MAX;
+    uint64_t m;
+    uint64_t* s = sorted_copy(ins, n_ins, 1, &m);
+    merge_sorted(o, s, m, 1);
+    free(s);
+    s = sorted_copy(del, n_del, 0, &m);
+    merge_sorted(o, s, m, 0);
+    free(s);
+    memset(o->last_edge_counts, 0, sizeof(o->last_edge_counts));
+    if (n_delta == 0) return 0;
+    /* RebuildUpdate: sorted, not unique */
+    for (size_t i = 0; i < (size_t)o->nd * o->dvcap; ++i) o->delta[i].n = 0;
+    s = sorted_copy(delta, n_delta, 0, &m);
+    uint32_t dcount[ORC_MAXD] = {0};
+    for (uint64_t i = 0; i < m; ++i) {
+        List* l = &o->delta[(size_t)KD(s[i]) * o->dvcap + KU(s[i])];
+        list_reserve(l, l->n + 1);
+        l->v[l->n++] = KV(s[i]);
+        dcount[KD(s[i])]++;
+    }
+    free(s);
+    uint8_t ok[ORC_MAXQE];
+    for (uint32_t e = 0; e < o->qe; ++e) {
+        if (edge_ok) ok[e] = edge_ok[e];
+        else
+            ok[e] = dcount[o->eidx[o->qe_u[e] * ORC_MAXQV + o->qe_v[e]]] &&
+                    dcount[o->eidx[o->qe_v[e] * ORC_MAXQV + o->qe_u[e]]];
+    }
+    uint64_t c = count_batch(o, ok, mode, global_order);
+    o->pending = (uint64_t*)realloc(o->pending, n_delta * 8);
+    memcpy(o->pending, delta, n_delta * 8);
+    o->n_pending = n_delta;
+    return c;
+}
+
+void orc_edge_counts(void* h, uint64_t* out) {
+    Orc* o = (Orc*)h;
+    memcpy(out, o->last_edge_counts, o->qe * 8);
+}
+
+/* Sorted keys of the main index after any pending merge-back. */
+uint64_t orc_dump(void* h, uint64_t* out, uint64_t cap) {
+    Orc* o = (Orc*)h;
+    flush_pending(o);
+    uint64_t n = 0;
+    for (uint32_t d = 0; d < o->nd; ++d)
+        for (uint32_t u = 0; u < o->dv; ++u) {
+            const List* l = &o->main[(size_t)d * o->dvcap + u];
+            for (uint32_t t = 0; t < l->n; ++t) {
+                if (out && n < cap) out[n] = ((uint64_t)d << 59) | ((uint64_t)u << 32) | l->v[t];
+                ++n;
+            }
+        }
+    return n;
+}
+
+/* Fraction check helper: number of main entries whose mirror entry is missing. */
+uint64_t orc_asymmetry(void* h) {
+    Orc* o = (Orc*)h;
+    uint64_t bad = 0;
+    for (uint32_t a = 0; a < o->qv; ++a)
+        for (uint32_t b = 0; b < o->qv; ++b) {
+            uint8_t d = o->eidx[a * ORC_MAXQV + b];
+            if (d == 255) continue;
+            uint8_t r = o->eidx[b * ORC_MAXQV + a];
+            for (uint32_t u = 0; u < o->dv; ++u) {
+                const List* l = &o->main[(size_t)d * o->dvcap + u];
+                for (uint32_t t = 0; t < l->n; ++t)
+                    if (!list_has(&o->main[(size_t)r * o->dvcap + l->v[t]], u)) ++bad;
+            }
+        }
+    return bad;
+}
+
+/* ---- brute force: label-preserving injective embeddings of Q in G ----
+ * G as sorted CSR (off[n+1], adj), vertex labels glab; Q as labels + edges. */
+typedef struct {
+    uint32_t n;
+    const uint64_t* off;
+    const uint32_t* adj;
+    const uint32_t* glab;
+    uint32_t qv;
+    const uint32_t* qlab;
+    uint8_t qadj[ORC_MAXQV][ORC_MAXQV];
+    uint8_t order[ORC_MAXQV];
+    uint32_t m[ORC_MAXQV];
+} BF;
+
+static int g_has(const BF* b, uint32_t x, uint32_t y) {
+    uint64_t lo = b->off[x], hi = b->off[x + 1];
+    while (lo < hi) {
+        uint64_t mid = (lo + hi) >> 1;
+        if (b->adj[mid] < y) lo = mid + 1; else hi = mid;
+    }
+    return lo < b->off[x + 1] && b->adj[lo] == y;
+}
+
+static uint64_t bf_rec(BF* b, uint32_t j) {
+    if (j == b->qv) return 1;
+    uint32_t u = b->order[j];
+    /* parent: first earlier query neighbour (connected order) */
+    int par = -1;
+    for (uint32_t t = 0; t < j; ++t) if (b->qadj[b->order[t]][u]) { par = (int)t; break; }
+    uint64_t c = 0;
+    if (par < 0) {
+        for (uint32_t x = 0; x < b->n; ++x) {
+            if (b->glab[x] != b->qlab[u]) continue;
+            int ok = 1;
+            for (uint32_t t = 0; t < j && ok; ++t) ok = b->m[t] != x;
+            if (!ok) continue;
+            b->m[j] = x;
+            c += bf_rec(b, j + 1);
+        }
+        return c;
+    }
+    uint32_t pv = b->m[par];
+    for (uint64_t p = b->off[pv]; p < b->off[pv + 1]; ++p) {
+        uint32_t x = b->adj[p];
+        if (b->glab[x] != b->qlab[u]) continue;
+        int ok = 1;
+        for (uint32_t t = 0; t < j && ok; ++t) {
+            if (b->m[t] == x) ok = 0;
+            else if (b->qadj[b->order[t]][u] && !g_has(b, b->m[t], x)) ok = 0;
+        }
+        if (!ok) continue;
+        b->m[j] = x;
+        c += bf_rec(b, j + 1);
+    }
+    return c;
+}
+
+uint64_t orc_bruteforce(uint32_t n, const uint64_t* off, const uint32_t* adj, const uint32_t* glab,
+                        uint32_t qv, const uint32_t* qlab, uint32_t qe, const uint32_t* qedges) {
+    BF b;
+    memset(&b, 0, sizeof(b));
+    b.n = n; b.off = off; b.adj = adj; b.glab = glab; b.qv = qv; b.qlab = qlab;
+    for (uint32_t i = 0; i < qe; ++i) {
+        b.qadj[qedges[2 * i]][qedges[2 * i + 1]] = 1;
+        b.qadj[qedges[2 * i + 1]][qedges[2 * i]] = 1;
+    }
+    /* BFS order from vertex 0 keeps every later vertex adjacent to an earlier one */
+    uint8_t vis[ORC_MAXQV] = {0};
+    uint32_t k = 0;
+    for (uint32_t s = 0; s < qv; ++s) {
+        if (vis[s]) continue;
+        vis[s] = 1;
+        b.order[k++] = (uint8_t)s;
+        for (uint32_t h = k - 1; h < k; ++h)
+            for (uint32_t w = 0; w < qv; ++w)
+                if (!vis[w] && b.qadj[b.order[h]][w]) { vis[w] = 1; b.order[k++] = (uint8_t)w; }
+    }
+    return bf_rec(&b, 0);
+}
