@@ -1,0 +1,89 @@
+// CaLiG candidate index (Stage 1 producer of the per-batch keys).
+//
+// Restates the reference's CaLiG maintenance (index/calig.{h,cpp}) with flat
+// storage: per data vertex v and query vertex ui of v's label, one sorted
+// candidate list per query neighbour uj of ui (the reference's
+// G[v].cand[ui][uj] hash sets, calig.h:28-33), plus the LI bitmask G_Li
+// (calig.h:82) and the per-(v,ui) "checked" bit (calig.h:32).  The update
+// algorithm keeps the reference's phase structure so the emitted delta
+// multisets are identical:
+//   updateIndex     calig.cpp:950-1069
+//   ConstructUpdate calig.cpp:776-804
+//   mergeDeltas     calig.cpp:1071-1088 (deltas are returned per batch)
+#pragma once
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace cgb {
+
+struct DeltaOp {  // calig.h:35
+    uint32_t vi, vj, ui, uj;
+};
+
+class CaLiGIndex {
+public:
+    // Loading (reference text formats, calig.cpp:111-216, 719-733).
+    std::string load_query(const std::string& path);
+    std::string load_graph(const std::string& path);
+    std::string load_updates(const std::string& path);
+
+    // constructCand + staticFilter (calig.cpp:325-356, 705-717)
+    void construct();
+
+    // One batch over update[start, start+count) (ints; two per edge).
+    void update_index(uint32_t start, uint32_t count);
+    void construct_update(uint32_t start, uint32_t count);
+
+    uint32_t num_update_ints() const { return (uint32_t)update_.size(); }
+    uint32_t num_vertices() const { return (uint32_t)glabel_.size(); }
+    uint32_t query_size() const { return qn_; }
+    const std::vector<uint32_t>& li() const { return li_; }
+    const std::vector<std::vector<uint32_t>>& query_nbrs() const { return qnei_; }
+    const std::vector<int>& query_labels() const { return qlabel_; }
+
+    // candidate list of (v, ui -> uj); nullptr if v has no slot for ui
+    const std::vector<uint32_t>* cand(uint32_t v, uint32_t ui, uint32_t uj) const;
+
+    // deltas of the last batch
+    std::vector<DeltaOp> delta_ins, delta_del, delta_update;
+
+private:
+    // query
+    uint32_t qn_ = 0;
+    std::vector<int> qlabel_;
+    std::vector<std::vector<uint32_t>> qnei_;
+    std::vector<std::vector<std::vector<uint32_t>>> rep_;  // per ui: groups of same-label neighbours (size > 1)
+    std::vector<std::vector<int>> rep_of_label_;            // per ui, per label slot -> group index or -1
+    std::vector<int> label_slot_;                           // raw label -> dense label index or -1
+    std::vector<std::vector<uint32_t>> qlist_;              // dense label -> query vertices ascending
+    std::vector<uint32_t> block_off_;                       // per ui: offset of its lists in a vertex block
+    std::vector<uint32_t> block_size_;                      // per dense label
+    std::vector<int> npos_;                                 // ui*qn + uj -> position in qnei_[ui]
+
+    // data
+    std::vector<int> glabel_;        // dense label index or -1 (pruned)
+    std::vector<std::vector<uint32_t>> nei_;
+    std::vector<uint64_t> cbase_;    // per vertex: first list index
+    std::vector<std::vector<uint32_t>> lists_;
+    std::vector<uint32_t> li_, checked_;
+    std::vector<int> update_;
+
+    inline std::vector<uint32_t>& C(uint32_t v, uint32_t ui, uint32_t uj) {
+        return lists_[cbase_[v] + block_off_[ui] + (uint32_t)npos_[ui * qn_ + uj]];
+    }
+    inline bool lit(uint32_t v, uint32_t u) const { return (li_[v] >> u) & 1u; }
+    bool has_slot(uint32_t v, uint32_t u) const {
+        return glabel_[v] >= 0 && glabel_[v] == label_slot_[qlabel_[u]];
+    }
+    bool check_nei(uint32_t v, uint32_t u);
+    bool try_nei(uint32_t v, uint32_t u, const std::vector<uint32_t>& group, size_t th,
+                 std::vector<uint32_t>& used);
+
+    struct Task { uint32_t u, v; };
+    struct Tmp { uint32_t ui, uj, vi, vj; };
+    void add_and_check(std::vector<Task>& add, std::vector<Task>& add_del, std::vector<Task>& activated);
+    void del_and_check(std::vector<Task>& del);
+};
+
+}  // namespace cgb

@@ -70,10 +70,9 @@ __device__ __forceinline__ uint64_t pack_duv(uint32_t d, uint32_t u, uint32_t v,
     return ((uint64_t)d << (2 * B)) | ((uint64_t)u << B) | (uint64_t)v;
 }
 
-// Edits: ((d,u,v) << 1) | op, op 0 = add, 1 = remove.  Invalid keys raise err
-// bit 1 and are turned into a no-op remove of (0,0,0) ... which is harmless
-// only if it does not exist; instead they are mapped past the end (all ones)
-// and ignored by the merge.
+// Edits: ((d,u,v) << 1) | op, op 0 = add, 1 = remove.  Keys whose direction
+// or vertex ids are out of range raise error bit 1 and become the all-ones
+// marker, which sorts last and is skipped by the merge.
 __global__ void k_pack_edits(const uint64_t* __restrict__ in, uint64_t n, uint32_t op, PackInfo pi,
                              uint64_t* __restrict__ out, unsigned int* err) {
     uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -133,6 +132,7 @@ struct MergeArgs {
     const int* num_runs;
     uint32_t B;
     unsigned int* err;
+    unsigned long long* stats;   // [5] merge bytes (edits 8 B, old run 4 B/word, new run 4 B/word, record 32 B), [6] runs
 };
 
 __device__ __forceinline__ uint32_t round4(uint32_t x) { return (x + 3u) & ~3u; }
@@ -209,6 +209,8 @@ __global__ void k_merge_runs(MergeArgs a) {
         }
         if (lane == 0) {
             *recp = make_uint4((uint32_t)off, outn, old.z, old.w);
+            atomicAdd(a.stats + 5, 8ull * yl + 4ull * xl + 4ull * outn + 32ull);
+            atomicAdd(a.stats + 6, 1ull);
             long long dl = (long long)round4(outn) - (long long)round4(xl);
             if (dl) atomicAdd((unsigned long long*)a.live_words, (unsigned long long)dl);
             // unused tail of the allocation is dead space until compaction
@@ -290,32 +292,118 @@ struct DfsArgs {
     const uint32_t* seed_pre;
     unsigned long long* counts;  // [qe]
     unsigned int* work_next;
+    unsigned int* err;
+    unsigned long long* stats;   // [8]: seeds, chunks, tested, tails, algorithmic bytes read
+    unsigned long long budget_ns;  // per-launch wall-clock budget (0 = unlimited)
 };
+
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Resolved candidate list of one (direction, vertex): the old run (pool) and,
+// when visible, this batch's delta run (dval); the two are disjoint.
+struct ListRef {
+    const uint32_t* m;
+    uint32_t ml;
+    const uint32_t* d;
+    uint32_t dl;
+};
+
+__device__ __forceinline__ bool sorted_has(const uint32_t* __restrict__ p, uint32_t n, uint32_t x) {
+    uint32_t lo = 0, len = n;
+    while (len > 0) {
+        uint32_t half = len >> 1;
+        if (__ldg(p + lo + half) < x) { lo += half + 1; len -= half + 1; }
+        else len = half;
+    }
+    return lo < n && __ldg(p + lo) == x;
+}
+
+__device__ __forceinline__ bool list_has(const ListRef& L, uint32_t x) {
+    return sorted_has(L.m, L.ml, x) || (L.dl && sorted_has(L.d, L.dl, x));
+}
 
 __device__ __forceinline__ bool list_contains(const uint32_t* __restrict__ pool, const uint32_t* __restrict__ dval,
                                               const uint4& r, uint32_t x) {
-    // main part
-    {
-        const uint32_t* p = pool + r.x;
-        uint32_t lo = 0, n = r.y;
-        while (n > 0) {
-            uint32_t half = n >> 1;
-            if (__ldg(p + lo + half) < x) { lo += half + 1; n -= half + 1; }
-            else n = half;
-        }
-        if (lo < r.y && __ldg(p + lo) == x) return true;
+    return sorted_has(pool + r.x, r.y, x) || (r.w && sorted_has(dval + r.z, r.w, x));
+}
+
+__device__ __forceinline__ uint32_t list_at(const ListRef& L, uint32_t i) {
+    return i < L.ml ? __ldg(L.m + i) : __ldg(L.d + (i - L.ml));
+}
+
+// |A ∩ B| (and ∩ C when C != nullptr) by probing the shortest list's elements.
+__device__ uint64_t inter_count(const ListRef& A, const ListRef& Bl, const ListRef* C) {
+    const ListRef* s = &A;
+    const ListRef* o1 = &Bl;
+    if (Bl.ml + Bl.dl < A.ml + A.dl) { s = &Bl; o1 = &A; }
+    uint64_t c = 0;
+    const uint32_t n = s->ml + s->dl;
+    for (uint32_t i = 0; i < n; ++i) {
+        const uint32_t x = list_at(*s, i);
+        if (list_has(*o1, x) && (!C || list_has(*C, x))) ++c;
     }
-    if (r.w) {
-        const uint32_t* p = dval + r.z;
-        uint32_t lo = 0, n = r.w;
-        while (n > 0) {
-            uint32_t half = n >> 1;
-            if (__ldg(p + lo + half) < x) { lo += half + 1; n -= half + 1; }
-            else n = half;
+    return c;
+}
+
+// Number of injective assignments of the tail leaves given the matched core
+// m[0..n_core) (m[n_core-1] passed as `last`), as a product over label groups
+// of inclusion-exclusion over the group's candidate lists minus the core.
+__device__ unsigned long long tail_count(const EdgePlan& P, const uint32_t* m, uint32_t last, const uint4* rec,
+                                         uint32_t dvcap, const uint32_t* pool, const uint32_t* dval) {
+    const uint32_t nc = P.n_core, n = P.n;
+    auto mv = [&](uint32_t pos) { return pos == nc - 1 ? last : m[pos]; };
+    unsigned long long prod = 1;
+    uint32_t t = nc;
+    while (t < n && prod) {
+        uint32_t e = t;
+        while (e < n && P.tail_gid[e] == P.tail_gid[t]) ++e;
+        const uint32_t k = e - t;
+        ListRef L[3];
+        uint64_t sz[3];
+        for (uint32_t i = 0; i < k; ++i) {
+            const uint32_t bk = P.bn_off[t + i];
+            uint4 r = rec[(size_t)P.bn_dir[bk] * dvcap + mv(P.bn_pos[bk])];
+            if (!P.bn_dvis[bk]) r.w = 0;
+            L[i] = ListRef{pool + r.x, r.y, dval + r.z, r.w};
+            uint64_t c = (uint64_t)r.y + r.w;
+            for (uint32_t q = 0; q < nc; ++q)
+                if (list_has(L[i], mv(q))) --c;
+            sz[i] = c;
         }
-        if (lo < r.w && __ldg(p + lo) == x) return true;
+        unsigned long long g;
+        if (k == 1) {
+            g = sz[0];
+        } else {
+            // pairwise (and triple) intersections, core vertices excluded
+            auto inter_ex = [&](uint32_t i, uint32_t j) {
+                uint64_t c = inter_count(L[i], L[j], nullptr);
+                for (uint32_t q = 0; q < nc; ++q)
+                    if (list_has(L[i], mv(q)) && list_has(L[j], mv(q))) --c;
+                return c;
+            };
+            if (k == 2) {
+                g = sz[0] * sz[1] - inter_ex(0, 1);
+            } else {
+                uint64_t i01 = inter_ex(0, 1), i02 = inter_ex(0, 2), i12 = inter_ex(1, 2);
+                uint64_t i012 = inter_count(L[0], L[1], &L[2]);
+                for (uint32_t q = 0; q < nc; ++q)
+                    if (list_has(L[0], mv(q)) && list_has(L[1], mv(q)) && list_has(L[2], mv(q))) --i012;
+                g = sz[0] * sz[1] * sz[2] - i01 * sz[2] - i02 * sz[1] - i12 * sz[0] + 2 * i012;
+            }
+        }
+        prod *= g;
+        t = e;
     }
-    return false;
+    return prod;
+}
+
+__device__ __forceinline__ unsigned long long warp_sum(unsigned long long x) {
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(kFull, x, o);
+    return x;
 }
 
 __global__ void __launch_bounds__(kDfsWarps * 32) k_dfs_count(DfsArgs a) {
@@ -337,8 +425,13 @@ __global__ void __launch_bounds__(kDfsWarps * 32) k_dfs_count(DfsArgs a) {
 
     // per-depth state held by lane == depth
     uint32_t st_ncand = 0, st_pos = 0, st_next = 0, st_len = 0, st_gen = 0;
-    unsigned long long cnt = 0;
+    unsigned long long cnt = 0;  // lane-local partial count of the current edge
+    unsigned long long n_seeds = 0, n_chunks = 0, n_tested = 0, n_tail = 0;
+    unsigned long long n_bytes = 0;  // algorithmic bytes: seed keys, records, list words, probe sectors
     int cur_ei = -1;
+    const unsigned long long t_start = global_ns();
+    uint32_t steps = 0;
+    bool out_of_time = false;
 
     for (;;) {
         uint32_t item = 0;
@@ -348,7 +441,8 @@ __global__ void __launch_bounds__(kDfsWarps * 32) k_dfs_count(DfsArgs a) {
         int ei = 0;
         while (ei + 1 < (int)a.qe && s_pre[ei + 1] <= item) ++ei;
         if (ei != cur_ei) {
-            if (cur_ei >= 0 && lane == 0 && cnt) atomicAdd(a.counts + cur_ei, cnt);
+            const unsigned long long c = warp_sum(cnt);
+            if (cur_ei >= 0 && lane == 0 && c) atomicAdd(a.counts + cur_ei, c);
             cnt = 0;
             cur_ei = ei;
         }
@@ -358,9 +452,19 @@ __global__ void __launch_bounds__(kDfsWarps * 32) k_dfs_count(DfsArgs a) {
             m[0] = (uint32_t)((key >> a.B) & vmask);
             m[1] = (uint32_t)(key & vmask);
         }
-        const uint32_t n = P.n;
-        if (n == 2) { cnt += 1; __syncwarp(); continue; }
+        ++n_seeds;
+        if (lane == 0) n_bytes += 8;
         __syncwarp();
+        const uint32_t nc = P.n_core;
+        if (nc == 2) {  // the seed edge alone is the core: only the tail remains
+            if (lane == 0) {
+                cnt += (P.n == 2) ? 1ull : tail_count(P, m, m[1], a.rec, a.dvcap, a.pool, a.dval);
+                ++n_tail;
+            }
+            __syncwarp();
+            continue;
+        }
+        const bool has_tail = nc < P.n;
 
         // set up depth j: resolve BN records, choose the shortest list as generator
         auto setup = [&](uint32_t j) {
@@ -373,21 +477,27 @@ __global__ void __launch_bounds__(kDfsWarps * 32) k_dfs_count(DfsArgs a) {
                 if (!P.bn_dvis[k]) r.w = 0;
                 bn[k] = r;
                 len = r.y + r.w;
+                n_bytes += 16;
             }
-            // argmin (len, lane)
             uint32_t best = len, bl = lane;
             for (int o = 16; o > 0; o >>= 1) {
                 uint32_t ol = __shfl_xor_sync(kFull, best, o);
                 uint32_t oi = __shfl_xor_sync(kFull, bl, o);
                 if (ol < best || (ol == best && oi < bl)) { best = ol; bl = oi; }
             }
-            if (lane == j) { st_ncand = 0; st_pos = 0; st_next = 0; st_len = best; st_gen = bl; }
+            if (lane == j) { st_ncand = 0; st_pos = 0; st_next = 0; st_len = nb ? best : 0; st_gen = bl; }
             __syncwarp();
         };
 
         setup(2);
         uint32_t j = 2;
         while (j >= 2) {
+            if (a.budget_ns && ((++steps & 1023u) == 0)) {
+                // bounded run: give up (and report) once the budget is spent
+                unsigned long long now = global_ns();
+                out_of_time = __shfl_sync(kFull, (now - t_start) > a.budget_ns ? 1 : 0, 0) != 0;
+                if (out_of_time) break;
+            }
             const uint32_t ncand = __shfl_sync(kFull, st_ncand, j);
             const uint32_t pos = __shfl_sync(kFull, st_pos, j);
             if (pos < ncand) {
@@ -409,16 +519,30 @@ __global__ void __launch_bounds__(kDfsWarps * 32) k_dfs_count(DfsArgs a) {
                 uint32_t c = 0;
                 if (ok) {
                     c = idx < gr.y ? __ldg(a.pool + gr.x + idx) : __ldg(a.dval + gr.z + (idx - gr.y));
+                    n_bytes += 4;
                     for (uint32_t t = 0; t < j; ++t) ok &= (c != m[t]);
                     for (uint32_t k = o0; k < o1 && ok; ++k) {
                         if (k == o0 + g) continue;
-                        ok = list_contains(a.pool, a.dval, bn[k], c);
+                        const uint4 r = bn[k];
+                        // binary search touches ~log2(len)+1 sectors of each part
+                        n_bytes += 32u * (33u - __clz(r.y | 1u));
+                        if (r.w) n_bytes += 32u * (33u - __clz(r.w | 1u));
+                        ok = list_contains(a.pool, a.dval, r, c);
                     }
+                    ++n_tested;
                 }
-                const uint32_t bal = __ballot_sync(kFull, ok);
-                if (j == n - 1) {
-                    cnt += __popc(bal);
+                ++n_chunks;
+                if (j == nc - 1) {
+                    if (has_tail) {
+                        if (ok) {
+                            cnt += tail_count(P, m, c, a.rec, a.dvcap, a.pool, a.dval);
+                            ++n_tail;
+                        }
+                    } else {
+                        cnt += ok ? 1ull : 0ull;
+                    }
                 } else {
+                    const uint32_t bal = __ballot_sync(kFull, ok);
                     if (ok) s_cand[w][j][__popc(bal & ((1u << lane) - 1u))] = c;
                     if (lane == j) { st_ncand = __popc(bal); st_pos = 0; }
                 }
@@ -428,8 +552,21 @@ __global__ void __launch_bounds__(kDfsWarps * 32) k_dfs_count(DfsArgs a) {
             }
             --j;
         }
+        if (out_of_time) {
+            if (lane == 0) atomicOr(a.err, 8u);
+            break;
+        }
     }
-    if (cur_ei >= 0 && lane == 0 && cnt) atomicAdd(a.counts + cur_ei, cnt);
+    const unsigned long long c = warp_sum(cnt);
+    if (cur_ei >= 0 && lane == 0 && c) atomicAdd(a.counts + cur_ei, c);
+    const unsigned long long tested = warp_sum(n_tested), tails = warp_sum(n_tail), bytes = warp_sum(n_bytes);
+    if (lane == 0) {
+        atomicAdd(a.stats + 0, n_seeds);
+        atomicAdd(a.stats + 1, n_chunks);
+        atomicAdd(a.stats + 2, tested);
+        atomicAdd(a.stats + 3, tails);
+        atomicAdd(a.stats + 4, bytes);
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -547,11 +684,13 @@ struct cgb_handle {
     size_t druns_cap = 0;
     uint32_t* d_seed = nullptr;  // [0..kMaxQE) lo, [kMaxQE..2kMaxQE+1) pre
     unsigned long long* d_counts = nullptr;  // [kMaxQE]
+    unsigned long long* d_stats = nullptr;   // [8]
+    unsigned long long last_stats[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     void* d_temp = nullptr; size_t temp_cap = 0;
 
     uint64_t last_counts[kMaxQE] = {0};
     float last_t[4] = {0, 0, 0, 0};
-    cudaEvent_t ev[5] = {};
+    cudaEvent_t ev[6] = {};
 };
 
 namespace {
@@ -630,6 +769,27 @@ cgb_status ensure_dvcap(cgb_handle* h, uint32_t dv) {
 cgb_status compact_pool(cgb_handle* h, unsigned long long new_cap) {
     const uint64_t n = (uint64_t)h->nd * h->dv;
     if (new_cap < h->pool_cap) new_cap = h->pool_cap;
+    uint32_t* sizes = nullptr;
+    unsigned long long* offs = nullptr;
+    unsigned long long live = 0;
+    CK(cudaMalloc(&sizes, std::max<uint64_t>(n, 1) * sizeof(uint32_t)));
+    CK(cudaMalloc(&offs, (n + 1) * sizeof(unsigned long long)));
+    CK(cudaMemsetAsync(offs, 0, (n + 1) * sizeof(unsigned long long), h->stream));
+    if (n > 0) {
+        k_rec_sizes<<<grid_for(h, n), 256, 0, h->stream>>>(h->rec, h->dvcap, h->dv, h->nd, sizes, nullptr);
+        LAUNCHED();
+        k_u32_to_u64<<<grid_for(h, n), 256, 0, h->stream>>>(sizes, offs, n);
+        LAUNCHED();
+    }
+    size_t tb = 0;
+    CK(cub::DeviceScan::ExclusiveSum(nullptr, tb, offs, offs, (int64_t)n + 1, h->stream));
+    if (grow_temp(h, tb) != CGB_OK) return CGB_ERR_OOM;
+    CK(cub::DeviceScan::ExclusiveSum(h->d_temp, tb, offs, offs, (int64_t)n + 1, h->stream));
+    LAUNCHED();
+    CK(cudaMemcpyAsync(&live, offs + n, sizeof(live), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    // the destination must hold every live run plus the headroom requested
+    while (new_cap < live + (16ull << 20)) new_cap *= 2;
     uint32_t* dst = nullptr;
     if (h->pool_alt && new_cap == h->pool_cap) {
         dst = h->pool_alt;
@@ -638,31 +798,14 @@ cgb_status compact_pool(cgb_handle* h, unsigned long long new_cap) {
         h->pool_alt = nullptr;
         CK(cudaMalloc(&dst, new_cap * sizeof(uint32_t)));
     }
-    unsigned long long live = 0;
     if (n > 0) {
-        uint32_t* sizes = nullptr;
-        unsigned long long* offs = nullptr;
-        CK(cudaMalloc(&sizes, n * sizeof(uint32_t)));
-        CK(cudaMalloc(&offs, (n + 1) * sizeof(unsigned long long)));
-        k_rec_sizes<<<grid_for(h, n), 256, 0, h->stream>>>(h->rec, h->dvcap, h->dv, h->nd, sizes, nullptr);
-        LAUNCHED();
-        k_u32_to_u64<<<grid_for(h, n), 256, 0, h->stream>>>(sizes, offs, n);
-        LAUNCHED();
-        size_t tb = 0;
-        CK(cub::DeviceScan::ExclusiveSum(nullptr, tb, offs, offs, (int64_t)n + 1, h->stream));
-        // offs has n valid entries; scanning n+1 needs a defined last element
-        CK(cudaMemsetAsync(offs + n, 0, sizeof(unsigned long long), h->stream));
-        if (grow_temp(h, tb) != CGB_OK) return CGB_ERR_OOM;
-        CK(cub::DeviceScan::ExclusiveSum(h->d_temp, tb, offs, offs, (int64_t)n + 1, h->stream));
-        LAUNCHED();
         k_compact<<<grid_for(h, n * 32), 256, 0, h->stream>>>(h->rec, h->dvcap, h->dv, h->nd, h->pool, dst, offs);
         LAUNCHED();
         CK(cudaGetLastError());
-        CK(cudaMemcpyAsync(&live, offs + n, sizeof(live), cudaMemcpyDeviceToHost, h->stream));
-        CK(cudaStreamSynchronize(h->stream));
-        CK(cudaFree(sizes));
-        CK(cudaFree(offs));
     }
+    CK(cudaStreamSynchronize(h->stream));
+    CK(cudaFree(sizes));
+    CK(cudaFree(offs));
     uint32_t* old = h->pool;
     h->pool = dst;
     if (new_cap == h->pool_cap) {
@@ -787,6 +930,7 @@ cgb_status apply_edits(cgb_handle* h, const uint64_t* adds0, uint64_t n0, const 
     ma.num_runs = h->d_num_runs;
     ma.B = pi.B;
     ma.err = d_err;
+    ma.stats = h->d_stats;
     const int mg = std::max(1, std::min<int>((int)((n * 32 + 255) / 256), h->num_sms * 16));
     k_merge_runs<<<mg, 256, 0, h->stream>>>(ma);
     LAUNCHED();
@@ -797,6 +941,8 @@ cgb_status apply_edits(cgb_handle* h, const uint64_t* adds0, uint64_t n0, const 
 cgb_status sync_scalars(cgb_handle* h) {
     CK(cudaMemcpyAsync(h->h_scal, h->d_scal, 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, h->stream));
     CK(cudaMemcpyAsync(h->h_scal + 4, h->d_counts, kMaxQE * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                       h->stream));
+    CK(cudaMemcpyAsync(h->h_scal + 4 + kMaxQE, h->d_stats, 8 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
                        h->stream));
     CK(cudaStreamSynchronize(h->stream));
     h->h_pool_top = h->h_scal[0];
@@ -842,10 +988,11 @@ cgb_status cgb_create(const cgb_config* cfg, cgb_handle** out) {
     h->own_stream = true;
     CKC(cudaMalloc(&h->d_scal, 4 * sizeof(unsigned long long)));
     CKC(cudaMemset(h->d_scal, 0, 4 * sizeof(unsigned long long)));
-    CKC(cudaMallocHost(&h->h_scal, (4 + kMaxQE) * sizeof(unsigned long long)));
+    CKC(cudaMallocHost(&h->h_scal, (12 + kMaxQE) * sizeof(unsigned long long)));
     CKC(cudaMalloc(&h->d_num_runs, 2 * sizeof(int)));
     CKC(cudaMalloc(&h->d_seed, (3 * kMaxQE + 2) * sizeof(uint32_t)));
     CKC(cudaMalloc(&h->d_counts, kMaxQE * sizeof(unsigned long long)));
+    CKC(cudaMalloc(&h->d_stats, 8 * sizeof(unsigned long long)));
     CKC(cudaMalloc(&h->d_qe_dirs, 2 * kMaxQE));
     CKC(cudaMalloc(&h->d_edge_ok, kMaxQE));
     for (auto& ev : h->ev) CKC(cudaEventCreate(&ev));
@@ -861,7 +1008,7 @@ void cgb_destroy(cgb_handle* h) {
     void* ptrs[] = {h->rec, h->pool, h->pool_alt, h->d_scal, h->d_keys_in, h->d_pending, h->d_edits,
                     h->d_edits_alt, h->d_du, h->d_run_du, h->d_run_len, h->d_run_off, h->d_num_runs,
                     h->d_dkeys, h->d_dkeys_alt, h->d_dval, h->d_ddu, h->d_drun_du, h->d_drun_len, h->d_drun_off,
-                    h->d_seed, h->d_counts, h->d_temp, h->d_qe_dirs, h->d_edge_ok};
+                    h->d_seed, h->d_counts, h->d_stats, h->d_temp, h->d_qe_dirs, h->d_edge_ok};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (h->h_scal) cudaFreeHost(h->h_scal);
@@ -873,10 +1020,10 @@ void cgb_destroy(cgb_handle* h) {
 
 const char* cgb_last_error(const cgb_handle* h) { return h ? h->err.c_str() : "null handle"; }
 
-cgb_status cgb_load_query(cgb_handle* h, uint32_t qv, uint32_t qe, const uint32_t* edges) {
+cgb_status cgb_load_query(cgb_handle* h, uint32_t qv, const uint32_t* labels, uint32_t qe, const uint32_t* edges) {
     if (!h || !edges) return CGB_ERR_ARG;
     if (h->have_index) return fail(h, CGB_ERR_STATE, "query must be loaded before the index");
-    std::string e = cgb::build_query_meta(qv, qe, edges, h->q);
+    std::string e = cgb::build_query_meta(qv, qe, edges, labels, h->q);
     if (!e.empty()) return fail(h, CGB_ERR_ARG, "%s", e.c_str());
     h->nd = h->q.nd;
     uint8_t dirs[2 * kMaxQE];
@@ -893,7 +1040,7 @@ cgb_status cgb_load_query_file(cgb_handle* h, const char* path) {
     uint32_t qv = 0;
     std::string e = cgb::parse_query_file(path, labels, edges, qv);
     if (!e.empty()) return fail(h, CGB_ERR_IO, "%s", e.c_str());
-    return cgb_load_query(h, qv, (uint32_t)(edges.size() / 2), edges.data());
+    return cgb_load_query(h, qv, labels.data(), (uint32_t)(edges.size() / 2), edges.data());
 }
 
 uint32_t cgb_query_dir(const cgb_handle* h, uint32_t a, uint32_t b) {
@@ -926,7 +1073,7 @@ cgb_status cgb_build_index(cgb_handle* h, const uint64_t* keys, uint64_t n, uint
     }
     float avg[kMaxDir] = {0};
     for (uint32_t d = 0; d < h->nd; ++d) avg[d] = nodes[d] ? (float)card[d] / (float)nodes[d] : 0.f;
-    cgb::plan_edges(h->q, avg, h->plans);
+    cgb::plan_edges(h->q, avg, h->plans, !(h->cfg.flags & CGB_FLAG_ENUMERATE_TAIL));
     CK(cudaMemcpyToSymbol(c_plan, h->plans, sizeof(EdgePlan) * kMaxQE));
 
     h->dv = dv_count;
@@ -973,6 +1120,7 @@ cgb_status cgb_apply_batch_device(cgb_handle* h, uint32_t dv_count, const uint64
     unsigned int* d_err = (unsigned int*)(h->d_scal + 2);
     CK(cudaMemsetAsync(h->d_scal + 2, 0, 2 * sizeof(unsigned long long), h->stream));
     CK(cudaMemsetAsync(h->d_counts, 0, kMaxQE * sizeof(unsigned long long), h->stream));
+    CK(cudaMemsetAsync(h->d_stats, 0, 8 * sizeof(unsigned long long), h->stream));
     CK(cudaEventRecord(h->ev[0], h->stream));
 
     // 1. index update: pending delta (add) + ins (add) + del (remove)
@@ -1017,6 +1165,10 @@ cgb_status cgb_apply_batch_device(cgb_handle* h, uint32_t dv_count, const uint64
         da.seed_pre = h->d_seed + kMaxQE;
         da.counts = h->d_counts;
         da.work_next = (unsigned int*)(h->d_scal + 3);
+        da.err = d_err;
+        da.stats = h->d_stats;
+        da.budget_ns = h->cfg.dfs_budget_ms ? (unsigned long long)h->cfg.dfs_budget_ms * 1000000ull
+                                            : 600ull * 1000000000ull;
         int bps = h->cfg.dfs_blocks_per_sm ? (int)h->cfg.dfs_blocks_per_sm : 8;
         k_dfs_count<<<h->num_sms * bps, kDfsWarps * 32, 0, h->stream>>>(da);
         LAUNCHED();
@@ -1034,20 +1186,24 @@ cgb_status cgb_apply_batch_device(cgb_handle* h, uint32_t dv_count, const uint64
         CK(cudaEventRecord(h->ev[2], h->stream));
         CK(cudaEventRecord(h->ev[3], h->stream));
     }
+    CK(cudaEventRecord(h->ev[5], h->stream));
     if ((s = sync_scalars(h)) != CGB_OK) return s;
     float t01 = 0, t12 = 0, t23 = 0, t03 = 0;
     cudaEventElapsedTime(&t01, h->ev[0], h->ev[1]);
     cudaEventElapsedTime(&t12, h->ev[1], h->ev[2]);
     cudaEventElapsedTime(&t23, h->ev[2], h->ev[3]);
-    cudaEventElapsedTime(&t03, h->ev[0], h->ev[3]);
+    cudaEventElapsedTime(&t03, h->ev[0], h->ev[5]);
     h->last_t[0] = t01; h->last_t[1] = t12; h->last_t[2] = t23; h->last_t[3] = t03;
     if (h->h_scal[2]) {
         h->n_pending = 0;
-        return fail(h, (h->h_scal[2] & 4u) ? CGB_ERR_OOM : CGB_ERR_ARG,
-                    "batch rejected: error bits %llu (1/2 = key out of range, 4 = pool exhausted)", h->h_scal[2]);
+        cgb_status st = (h->h_scal[2] & 8u) ? CGB_ERR_TIMEOUT : (h->h_scal[2] & 4u) ? CGB_ERR_OOM : CGB_ERR_ARG;
+        return fail(h, st,
+                    "batch rejected: error bits %llu (1/2 = key out of range, 4 = pool exhausted, "
+                    "8 = matching exceeded its time budget)", h->h_scal[2]);
     }
     uint64_t total = 0;
     for (uint32_t e = 0; e < h->q.qe; ++e) { h->last_counts[e] = h->h_scal[4 + e]; total += h->h_scal[4 + e]; }
+    for (int i = 0; i < 8; ++i) h->last_stats[i] = h->h_scal[4 + kMaxQE + i];
     *out_count = total;
     if (h->cfg.flags & CGB_FLAG_NO_MERGE_BACK_DEFER) {
         if ((s = flush_pending(h)) != CGB_OK) return s;
@@ -1085,6 +1241,14 @@ cgb_status cgb_last_timings(const cgb_handle* h, float* t4) {
 }
 
 uint64_t cgb_kernel_launches(const cgb_handle* h) { return h ? h->launches : 0; }
+
+cgb_status cgb_last_stats(const cgb_handle* h, uint64_t* out8) {
+    if (!h || !out8) return CGB_ERR_ARG;
+    for (int i = 0; i < 8; ++i) out8[i] = h->last_stats[i];
+    return CGB_OK;
+}
+
+void* cgb_stream(const cgb_handle* h) { return h ? (void*)h->stream : nullptr; }
 
 cgb_status cgb_read_index(cgb_handle* h, uint64_t* out, uint64_t cap, uint64_t* n_out) {
     if (!h || !n_out) return CGB_ERR_ARG;

@@ -11,7 +11,9 @@
 // Query shapes follow the reference sampler's definitions
 // (sampler/graph_sampler.h:150-272): dense = BFS-sampled vertex set with all
 // induced edges and average degree >= 3; sparse = BFS tree plus random induced
-// edges up to 1.5n-1 edges; tree = DFS-grown tree of depth >= max(2,(n+2)/3).
+// edges up to 1.5n-1 edges; tree = random-DFS tree of depth >= max(2,(n+2)/3)
+// (the reference grows trees by pushing every neighbour of the stack top,
+// which yields stars on graphs whose degree exceeds the pattern size).
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
@@ -132,17 +134,38 @@ bool adjacent(const Adj& A, uint32_t x, uint32_t y) {
     return std::binary_search(A.nbr.begin() + A.off[x], A.nbr.begin() + A.off[x + 1], y);
 }
 
-// Returns vertices (order of discovery) and tree edges.
+// Returns vertices (order of discovery) and tree edges.  BFS growth attaches
+// every unvisited neighbour of the dequeued vertex (shuffled) until k vertices
+// are reached; tree (dfs) growth is a random depth-first walk that attaches one
+// unvisited neighbour of the stack top at a time, backtracking when there is
+// none, so trees come out deep rather than star-shaped.
 void grow(const Adj& A, uint32_t start, uint32_t k, bool dfs, std::mt19937_64& rng,
           std::vector<uint32_t>& vs, std::vector<std::pair<uint32_t, uint32_t>>& tree) {
     vs.assign(1, start);
     tree.clear();
     std::unordered_set<uint32_t> seen{start};
+    if (dfs) {
+        std::vector<uint32_t> stack{start};
+        while (!stack.empty() && vs.size() < k) {
+            uint32_t v = stack.back();
+            std::vector<uint32_t> nb;
+            for (uint64_t p = A.off[v]; p < A.off[v + 1]; ++p)
+                if (!seen.count(A.nbr[p])) nb.push_back(A.nbr[p]);
+            if (nb.empty()) { stack.pop_back(); continue; }
+            uint32_t u = nb[std::uniform_int_distribution<size_t>(0, nb.size() - 1)(rng)];
+            seen.insert(u);
+            vs.push_back(u);
+            tree.emplace_back(v, u);
+            // occasionally branch from an earlier vertex instead of going deeper
+            if (stack.size() > 1 && (rng() & 3) == 0) stack.pop_back();
+            stack.push_back(u);
+        }
+        return;
+    }
     std::deque<uint32_t> frontier{start};
     while (!frontier.empty() && vs.size() < k) {
-        uint32_t v;
-        if (dfs) { v = frontier.back(); frontier.pop_back(); }
-        else { v = frontier.front(); frontier.pop_front(); }
+        uint32_t v = frontier.front();
+        frontier.pop_front();
         std::vector<uint32_t> nb(A.nbr.begin() + A.off[v], A.nbr.begin() + A.off[v + 1]);
         std::shuffle(nb.begin(), nb.end(), rng);
         for (uint32_t u : nb) {

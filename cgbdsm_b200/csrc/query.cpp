@@ -37,11 +37,13 @@ std::string parse_query_file(const std::string& path, std::vector<uint32_t>& lab
     return "";
 }
 
-std::string build_query_meta(uint32_t qv, uint32_t qe, const uint32_t* edges, QueryMeta& q) {
+std::string build_query_meta(uint32_t qv, uint32_t qe, const uint32_t* edges, const uint32_t* labels,
+                             QueryMeta& q) {
     if (qv < 2 || qv > (uint32_t)kMaxQV) return "query must have 2..12 vertices";
     if (qe == 0 || 2 * qe > (uint32_t)kMaxDir) return "query must have 1..16 edges (5-bit directed index)";
     q = QueryMeta();
     q.qv = qv;
+    if (labels) q.labels.assign(labels, labels + qv);
     q.nbrs.assign(qv, {});
     for (uint32_t i = 0; i < qe; ++i) {
         uint32_t a = edges[2 * i], b = edges[2 * i + 1];
@@ -75,34 +77,68 @@ std::string build_query_meta(uint32_t qv, uint32_t qe, const uint32_t* edges, Qu
             ++e;
         }
     q.qe = e;
+    // connected patterns only: every vertex after the first edge needs a
+    // backward neighbour to draw candidates from
+    std::vector<int> seen(qv, 0);
+    std::vector<uint32_t> st{0};
+    seen[0] = 1;
+    while (!st.empty()) {
+        uint32_t u = st.back();
+        st.pop_back();
+        for (uint32_t w : q.nbrs[u])
+            if (!seen[w]) { seen[w] = 1; st.push_back(w); }
+    }
+    for (uint32_t u = 0; u < qv; ++u)
+        if (!seen[u]) return "query pattern must be connected";
     return "";
 }
 
 // Per-edge vertex order: ei's endpoints first (the delta edge is the seed),
-// then greedily the unvisited vertex with the most visited neighbours, ties
-// broken by the smallest estimated candidate count (min avg run length over
-// its backward edges), then by vertex id.  The tie-breaking criteria restate
-// the reference's global-order rules 1 and 4 (plan.cpp:595-708); the start is
-// the delta edge instead of a global edge because matching is seeded from the
-// delta lists.
-void plan_edges(const QueryMeta& q, const float* avg_deg, EdgePlan* plans) {
+// then greedily the unvisited core vertex with the most visited neighbours,
+// ties broken by the smallest estimated candidate count (min avg run length
+// over its backward edges), then by vertex id.  The tie-breaking criteria
+// restate the reference's global-order rules 1 and 4 (plan.cpp:595-708); the
+// start is the delta edge instead of a global edge because matching is seeded
+// from the delta lists.  Leaves (degree-1 vertices other than ei's endpoints)
+// go last, grouped by label, as the counted tail (the reference's tree
+// Cartesian-product tail, plan.cpp:899-952, which it enumerates); a label
+// group larger than 3 stays in the enumerated core.
+void plan_edges(const QueryMeta& q, const float* avg_deg, EdgePlan* plans, bool analytic_tail) {
     for (uint32_t ei = 0; ei < q.qe; ++ei) {
         EdgePlan& p = plans[ei];
         std::memset(&p, 0, sizeof(p));
         p.n = (uint8_t)q.qv;
         uint32_t a = q.qe_u[ei], b = q.qe_v[ei];
-        // seed from the endpoint whose other edges are more selective
         p.vs[0] = (uint8_t)a;
         p.vs[1] = (uint8_t)b;
         p.seed_dir = q.eidx[a * kMaxQV + b];
         std::vector<int> pos(q.qv, -1);
         pos[a] = 0;
         pos[b] = 1;
-        for (uint32_t j = 2; j < q.qv; ++j) {
+        // tail candidates grouped by label
+        std::vector<uint32_t> tail;
+        if (analytic_tail && q.qv > 2) {
+            std::vector<uint32_t> leaves;
+            for (uint32_t u = 0; u < q.qv; ++u)
+                if (u != a && u != b && q.nbrs[u].size() == 1) leaves.push_back(u);
+            auto lab = [&](uint32_t u) { return q.labels.empty() ? 0u : q.labels[u]; };
+            std::stable_sort(leaves.begin(), leaves.end(), [&](uint32_t x, uint32_t y) { return lab(x) < lab(y); });
+            for (size_t i = 0; i < leaves.size();) {
+                size_t j = i;
+                while (j < leaves.size() && lab(leaves[j]) == lab(leaves[i])) ++j;
+                if (j - i <= 3)
+                    for (size_t k = i; k < j; ++k) tail.push_back(leaves[k]);
+                i = j;
+            }
+        }
+        std::vector<char> is_tail(q.qv, 0);
+        for (uint32_t u : tail) is_tail[u] = 1;
+        const uint32_t n_core = q.qv - (uint32_t)tail.size();
+        for (uint32_t j = 2; j < n_core; ++j) {
             int best = -1, best_bn = -1;
             float best_est = 0.f;
             for (uint32_t u = 0; u < q.qv; ++u) {
-                if (pos[u] >= 0) continue;
+                if (pos[u] >= 0 || is_tail[u]) continue;
                 int nbn = 0;
                 float est = 3.4e38f;
                 for (uint32_t w : q.nbrs[u])
@@ -117,12 +153,19 @@ void plan_edges(const QueryMeta& q, const float* avg_deg, EdgePlan* plans) {
                     best_est = est;
                 }
             }
-            if (best < 0) {  // disconnected query: take the smallest unvisited vertex
-                for (uint32_t u = 0; u < q.qv; ++u)
-                    if (pos[u] < 0) { best = (int)u; break; }
-            }
-            pos[best] = (int)j;
+            pos[best] = (int)j;  // connected query: some core vertex is adjacent to the visited set
             p.vs[j] = (uint8_t)best;
+        }
+        p.n_core = (uint8_t)n_core;
+        std::memset(p.tail_gid, 255, sizeof(p.tail_gid));
+        uint8_t gid = 0;
+        for (size_t i = 0; i < tail.size(); ++i) {
+            const uint32_t j = n_core + (uint32_t)i;
+            p.vs[j] = (uint8_t)tail[i];
+            pos[tail[i]] = (int)j;
+            if (i > 0 && (q.labels.empty() ? 0u : q.labels[tail[i]]) != (q.labels.empty() ? 0u : q.labels[tail[i - 1]]))
+                ++gid;
+            p.tail_gid[j] = gid;
         }
         uint32_t k = 0;
         for (uint32_t j = 0; j < q.qv; ++j) {

@@ -16,7 +16,7 @@ constexpr int kMaxBN = 48;
 //   edge order graph.cpp:184-199  ((u, uu) with u < uu, u ascending then uu)
 struct QueryMeta {
     uint32_t qv = 0, qe = 0, nd = 0;
-    std::vector<uint32_t> labels;                  // file labels (unused by the GPU path)
+    std::vector<uint32_t> labels;                  // query labels; empty = unknown (all leaves may collide)
     std::vector<std::vector<uint32_t>> nbrs;       // sorted neighbour lists
     uint8_t eidx[kMaxQV * kMaxQV];                 // 255 = no edge
     uint8_t qe_u[kMaxQE], qe_v[kMaxQE];            // undirected edges
@@ -29,22 +29,33 @@ struct QueryMeta {
 // and for every later position the backward neighbours (BN) whose lists
 // constrain it.  bn_dvis marks BN directions whose delta part is visible to
 // ei (dir_to_edge < ei; enumeration.cu:937, cpu_dfs.cpp:76-77).
+//
+// Positions [n_core, n) form the tail: degree-1 query vertices (leaves) whose
+// single backward neighbour is a core vertex.  Their count is computed
+// instead of enumerated: per label group (tail_gid, contiguous) of k <= 3
+// leaves, the number of injective assignments of the group to its candidate
+// lists minus the matched core vertices, by inclusion-exclusion.  Leaves of
+// different labels have disjoint candidate lists, so groups multiply.
 struct EdgePlan {
     uint8_t n;
+    uint8_t n_core;
     uint8_t seed_dir;
     uint8_t vs[kMaxQV];
     uint8_t bn_off[kMaxQV + 1];
     uint8_t bn_pos[kMaxBN];
     uint8_t bn_dir[kMaxBN];
     uint8_t bn_dvis[kMaxBN];
-    uint8_t pad[3];
+    uint8_t tail_gid[kMaxQV];
+    uint8_t pad[2];
 };
 
 // Returns "" on success, else an error message.
-std::string build_query_meta(uint32_t qv, uint32_t qe, const uint32_t* edges, QueryMeta& q);
+std::string build_query_meta(uint32_t qv, uint32_t qe, const uint32_t* edges, const uint32_t* labels,
+                             QueryMeta& q);
 std::string parse_query_file(const std::string& path, std::vector<uint32_t>& labels,
                              std::vector<uint32_t>& edges, uint32_t& qv);
 // avg_deg[dir]: mean run length of direction dir in the initial index.
-void plan_edges(const QueryMeta& q, const float* avg_deg, EdgePlan* plans);
+// analytic_tail = false keeps every vertex in the enumerated core.
+void plan_edges(const QueryMeta& q, const float* avg_deg, EdgePlan* plans, bool analytic_tail = true);
 
 }  // namespace cgb

@@ -1,0 +1,277 @@
+"""ctypes binding of the engine's C ABI (include/cgbdsm.h).
+
+The engine itself is native (CUDA + C++ in libcgbdsm.so); this module only
+marshals arrays.  There is no Python or CPU fallback: if the shared library
+is missing or no CUDA device is present, construction raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Optional, Sequence
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libcgbdsm.so")
+
+_u32, _u64, _vp = ctypes.c_uint32, ctypes.c_uint64, ctypes.c_void_p
+
+STATUS = {0: "OK", 1: "ERR_ARG", 2: "ERR_CUDA", 3: "ERR_OOM", 4: "ERR_LIMIT", 5: "ERR_STATE",
+          6: "ERR_TIMEOUT", 7: "ERR_IO"}
+
+# Every entry point declared in include/cgbdsm.h (checked by tests/test_abi.py).
+EXPORTS = [
+    "cgb_default_config", "cgb_create", "cgb_destroy", "cgb_last_error", "cgb_load_query",
+    "cgb_load_query_file", "cgb_query_dir", "cgb_build_index", "cgb_apply_batch",
+    "cgb_apply_batch_device", "cgb_last_edge_counts", "cgb_read_index", "cgb_last_timings",
+    "cgb_kernel_launches", "cgb_last_stats", "cgb_stream", "cgb_producer_open", "cgb_producer_close", "cgb_producer_last_error",
+    "cgb_producer_num_batches", "cgb_producer_initial", "cgb_producer_next", "cgb_producer_vertex_map",
+]
+
+
+class CgbError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"{STATUS.get(status, status)}: {msg}")
+        self.status = status
+
+
+class Config(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int), ("pool_words", _u64), ("dfs_blocks_per_sm", _u32),
+                ("flags", _u32), ("dfs_budget_ms", _u32)]
+
+
+FLAG_NO_MERGE_BACK_DEFER = 0x1
+FLAG_ENUMERATE_TAIL = 0x2
+
+
+class BatchKeys(ctypes.Structure):
+    _fields_ = [("ins", ctypes.POINTER(_u64)), ("n_ins", _u64), ("dele", ctypes.POINTER(_u64)), ("n_del", _u64),
+                ("delta", ctypes.POINTER(_u64)), ("n_delta", _u64), ("edge_ok", ctypes.POINTER(ctypes.c_uint8)),
+                ("qe", _u32), ("dv_count", _u32), ("batch", _u32), ("num_edges", _u32),
+                ("ms_update_index", ctypes.c_double), ("ms_construct_update", ctypes.c_double),
+                ("ms_prepare", ctypes.c_double)]
+
+_lib_handle = None
+
+
+def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
+    """Loads libcgbdsm.so; raises if it has not been built."""
+    global _lib_handle
+    if _lib_handle is not None:
+        return _lib_handle
+    if not os.path.exists(path):
+        raise FileNotFoundError(f"{path} not built; run `python -m cgbdsm_b200.build`")
+    lib = ctypes.CDLL(path)
+    lib.cgb_default_config.argtypes = [ctypes.POINTER(Config)]
+    lib.cgb_create.argtypes = [ctypes.POINTER(Config), ctypes.POINTER(_vp)]
+    lib.cgb_destroy.argtypes = [_vp]
+    lib.cgb_last_error.argtypes = [_vp]
+    lib.cgb_last_error.restype = ctypes.c_char_p
+    lib.cgb_load_query.argtypes = [_vp, _u32, _vp, _u32, _vp]
+    lib.cgb_load_query_file.argtypes = [_vp, ctypes.c_char_p]
+    lib.cgb_query_dir.argtypes = [_vp, _u32, _u32]
+    lib.cgb_query_dir.restype = _u32
+    lib.cgb_build_index.argtypes = [_vp, _vp, _u64, _u32]
+    lib.cgb_apply_batch.argtypes = [_vp, _u32, _vp, _u64, _vp, _u64, _vp, _u64, _vp, ctypes.POINTER(_u64)]
+    lib.cgb_apply_batch_device.argtypes = [_vp, _u32, _vp, _u64, _vp, _u64, _vp, _u64, _vp, _vp,
+                                           ctypes.POINTER(_u64)]
+    lib.cgb_last_edge_counts.argtypes = [_vp, _vp, _u32]
+    lib.cgb_read_index.argtypes = [_vp, _vp, _u64, ctypes.POINTER(_u64)]
+    lib.cgb_last_timings.argtypes = [_vp, _vp]
+    lib.cgb_kernel_launches.argtypes = [_vp]
+    lib.cgb_kernel_launches.restype = _u64
+    lib.cgb_last_stats.argtypes = [_vp, _vp]
+    lib.cgb_stream.argtypes = [_vp]
+    lib.cgb_stream.restype = _vp
+    lib.cgb_producer_open.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, _u32, _u32,
+                                      ctypes.POINTER(_vp)]
+    lib.cgb_producer_close.argtypes = [_vp]
+    lib.cgb_producer_last_error.argtypes = [_vp]
+    lib.cgb_producer_last_error.restype = ctypes.c_char_p
+    lib.cgb_producer_num_batches.argtypes = [_vp]
+    lib.cgb_producer_num_batches.restype = _u32
+    lib.cgb_producer_initial.argtypes = [_vp, ctypes.POINTER(ctypes.POINTER(_u64)), ctypes.POINTER(_u64),
+                                         ctypes.POINTER(_u32)]
+    lib.cgb_producer_next.argtypes = [_vp, ctypes.POINTER(BatchKeys)]
+    lib.cgb_producer_vertex_map.argtypes = [_vp, ctypes.POINTER(ctypes.POINTER(_u32)), ctypes.POINTER(_u32)]
+    for name in EXPORTS:
+        getattr(lib, name)
+    _lib_handle = lib
+    return lib
+
+
+def _arr(a: Optional[np.ndarray]) -> tuple[int, int]:
+    if a is None or len(a) == 0:
+        return 0, 0
+    assert a.dtype == np.uint64 and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data, len(a)
+
+
+class Engine:
+    """One engine instance on one CUDA device (C ABI handle)."""
+
+    def __init__(self, device: int = 0, pool_words: int = 0, dfs_blocks_per_sm: int = 0, flags: int = 0,
+                 dfs_budget_ms: int = 0):
+        self.lib = load_library()
+        cfg = Config(device, pool_words, dfs_blocks_per_sm, flags, dfs_budget_ms)
+        h = _vp()
+        st = self.lib.cgb_create(ctypes.byref(cfg), ctypes.byref(h))
+        self.h = h.value
+        if st != 0:
+            msg = self.lib.cgb_last_error(self.h).decode() if self.h else ""
+            self.close()
+            raise CgbError(st, msg)
+        self.qe = 0
+
+    def _check(self, st: int) -> None:
+        if st != 0:
+            raise CgbError(st, self.lib.cgb_last_error(self.h).decode())
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.lib.cgb_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def load_query(self, qv: int, edges: Sequence[tuple[int, int]], labels: Optional[Sequence[int]] = None) -> None:
+        e = np.asarray(edges, dtype=np.uint32).reshape(-1)
+        lab = None if labels is None else np.asarray(labels, dtype=np.uint32)
+        self._check(self.lib.cgb_load_query(self.h, qv, lab.ctypes.data if lab is not None else None,
+                                            len(e) // 2, e.ctypes.data))
+        self.qe = len(e) // 2
+
+    def load_query_file(self, path: str) -> None:
+        self._check(self.lib.cgb_load_query_file(self.h, path.encode()))
+        from .workloads import read_query
+        _, edges = read_query(path)
+        self.qe = len(edges)
+
+    def query_dir(self, a: int, b: int) -> int:
+        return self.lib.cgb_query_dir(self.h, a, b)
+
+    def build_index(self, keys: np.ndarray, dv_count: int) -> None:
+        keys = np.ascontiguousarray(keys, dtype=np.uint64)
+        p, n = _arr(keys)
+        self._check(self.lib.cgb_build_index(self.h, p, n, dv_count))
+
+    def apply_batch(self, dv_count: int, ins: np.ndarray, dele: np.ndarray, delta: np.ndarray,
+                    edge_ok: Optional[np.ndarray] = None) -> int:
+        ins = np.ascontiguousarray(ins, dtype=np.uint64)
+        dele = np.ascontiguousarray(dele, dtype=np.uint64)
+        delta = np.ascontiguousarray(delta, dtype=np.uint64)
+        pi, ni = _arr(ins)
+        pd, nd = _arr(dele)
+        pD, nD = _arr(delta)
+        ok = None
+        if edge_ok is not None:
+            ok = np.ascontiguousarray(edge_ok, dtype=np.uint8)
+        out = _u64(0)
+        self._check(self.lib.cgb_apply_batch(self.h, dv_count, pi, ni, pd, nd, pD, nD,
+                                             ok.ctypes.data if ok is not None else None,
+                                             ctypes.byref(out)))
+        return out.value
+
+    def apply_batch_device(self, dv_count: int, ins_ptr: int, n_ins: int, del_ptr: int, n_del: int,
+                           delta_ptr: int, n_delta: int, stream: int = 0) -> int:
+        out = _u64(0)
+        self._check(self.lib.cgb_apply_batch_device(self.h, dv_count, ins_ptr, n_ins, del_ptr, n_del,
+                                                    delta_ptr, n_delta, None, stream or None,
+                                                    ctypes.byref(out)))
+        return out.value
+
+    def edge_counts(self) -> np.ndarray:
+        out = np.zeros(max(self.qe, 1), dtype=np.uint64)
+        self._check(self.lib.cgb_last_edge_counts(self.h, out.ctypes.data, self.qe))
+        return out[: self.qe]
+
+    def read_index(self) -> np.ndarray:
+        n = _u64(0)
+        self._check(self.lib.cgb_read_index(self.h, None, 0, ctypes.byref(n)))
+        out = np.zeros(max(n.value, 1), dtype=np.uint64)
+        self._check(self.lib.cgb_read_index(self.h, out.ctypes.data, n.value, ctypes.byref(n)))
+        return out[: n.value]
+
+    def timings(self) -> np.ndarray:
+        t = np.zeros(4, dtype=np.float32)
+        self._check(self.lib.cgb_last_timings(self.h, t.ctypes.data))
+        return t
+
+    def stats(self) -> dict:
+        out = np.zeros(8, dtype=np.uint64)
+        self._check(self.lib.cgb_last_stats(self.h, out.ctypes.data))
+        return {"seeds": int(out[0]), "chunks": int(out[1]), "tested": int(out[2]), "tails": int(out[3]),
+                "match_bytes": int(out[4]), "update_bytes": int(out[5]), "touched_runs": int(out[6])}
+
+    def stream(self) -> int:
+        return int(self.lib.cgb_stream(self.h) or 0)
+
+    def kernel_launches(self) -> int:
+        return int(self.lib.cgb_kernel_launches(self.h))
+
+
+def _copy(p, n, dtype=np.uint64) -> np.ndarray:
+    if n == 0:
+        return np.zeros(0, dtype=dtype)
+    return np.ctypeslib.as_array(p, (n,)).copy()
+
+
+class Producer:
+    """Stage-1 producer (CaLiG index + host staging) through the C ABI; CPU only."""
+
+    def __init__(self, query: str, data: str, update: str, batch_size_ints: int, threads: int = 0):
+        self.lib = load_library()
+        h = _vp()
+        st = self.lib.cgb_producer_open(query.encode(), data.encode(), update.encode(), batch_size_ints,
+                                        threads, ctypes.byref(h))
+        self.h = h.value
+        if st != 0:
+            msg = self.lib.cgb_producer_last_error(self.h).decode() if self.h else ""
+            self.close()
+            raise CgbError(st, msg)
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.lib.cgb_producer_close(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def num_batches(self) -> int:
+        return self.lib.cgb_producer_num_batches(self.h)
+
+    def initial(self) -> tuple[np.ndarray, int]:
+        p = ctypes.POINTER(_u64)()
+        n = _u64(0)
+        dv = _u32(0)
+        st = self.lib.cgb_producer_initial(self.h, ctypes.byref(p), ctypes.byref(n), ctypes.byref(dv))
+        if st != 0:
+            raise CgbError(st, self.lib.cgb_producer_last_error(self.h).decode())
+        return _copy(p, n.value), dv.value
+
+    def next(self) -> dict:
+        bk = BatchKeys()
+        st = self.lib.cgb_producer_next(self.h, ctypes.byref(bk))
+        if st != 0:
+            raise CgbError(st, self.lib.cgb_producer_last_error(self.h).decode())
+        return {"ins": _copy(bk.ins, bk.n_ins), "del": _copy(bk.dele, bk.n_del),
+                "delta": _copy(bk.delta, bk.n_delta), "edge_ok": _copy(bk.edge_ok, bk.qe, np.uint8),
+                "dv": bk.dv_count, "batch": bk.batch, "num_edges": bk.num_edges,
+                "ms": {"update_index": bk.ms_update_index, "construct_update": bk.ms_construct_update,
+                       "prepare": bk.ms_prepare}}
+
+    def new2old(self) -> np.ndarray:
+        p = ctypes.POINTER(_u32)()
+        n = _u32(0)
+        self.lib.cgb_producer_vertex_map(self.h, ctypes.byref(p), ctypes.byref(n))
+        return _copy(p, n.value, np.uint32)

@@ -1,0 +1,117 @@
+"""Seeded synthetic workloads in the reference's text formats.
+
+The reference measures on public graphs that are not available here; these
+configurations stand in for them with the shapes, sizes and distributions
+the engine is measured on (seeds fixed so every run sees the same input):
+
+  c1  Erdos-Renyi 10,000 vertices / 50,000 edges, 8 uniform labels,
+      10% (5,000 edges) held out and re-inserted in batches of 1,000,
+      5-vertex dense pattern (densest induced BFS sample, see gen.cpp).
+  c2  R-MAT(0.57,0.19,0.19,0.05) 1,000,000 vertices / 10,000,000 edges,
+      16 labels Zipf(1.2), 1,000,000 held out, batches of 100,000,
+      9-vertex dense pattern with <= 16 edges.
+  c3  R-MAT 4,000,000 / 34,000,000, 32 labels Zipf(1.0), 3,400,000 held
+      out, batches of 1,000,000, 7-vertex tree and sparse patterns.
+Small seeded variants ("t*") are used by the parity tests.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+GEN_LIB = os.path.join(_HERE, "libcgbgen.so")
+
+
+@dataclass(frozen=True)
+class WorkloadSpec:
+    name: str
+    kind: int            # 0 = Erdos-Renyi, 1 = R-MAT
+    n: int
+    m: int
+    labels: int
+    zipf: float          # <= 0: uniform labels
+    holdout: int
+    batch_edges: int     # insertions per batch (reference CLI batch_size = 2x, F2)
+    qshape: int          # 0 dense, 1 sparse, 2 tree
+    qsize: int
+    seed_graph: int
+    seed_labels: int
+    seed_holdout: int
+    seed_query: int
+    max_qedges: int = 16
+
+    @property
+    def num_batches(self) -> int:
+        return (self.holdout + self.batch_edges - 1) // self.batch_edges
+
+    @property
+    def cli_batch_size(self) -> int:
+        """The reference CLI's [batch_size] counts ints, two per edge (main_calig.cpp:104, F2)."""
+        return 2 * self.batch_edges
+
+
+SPECS = {
+    "c1": WorkloadSpec("c1", 0, 10_000, 50_000, 8, 0.0, 5_000, 1_000, 0, 5, 1, 2, 3, 11),
+    "c2": WorkloadSpec("c2", 1, 1_000_000, 10_000_000, 16, 1.2, 1_000_000, 100_000, 0, 9, 21, 22, 23, 24),
+    "c3_tree": WorkloadSpec("c3_tree", 1, 4_000_000, 34_000_000, 32, 1.0, 3_400_000, 1_000_000, 2, 7,
+                            31, 32, 33, 34),
+    "c3_sparse": WorkloadSpec("c3_sparse", 1, 4_000_000, 34_000_000, 32, 1.0, 3_400_000, 1_000_000, 1, 7,
+                              31, 32, 33, 35),
+    # small parity workloads (CPU oracle finishes in seconds)
+    "t_er5": WorkloadSpec("t_er5", 0, 2_000, 40_000, 4, 0.0, 4_000, 500, 0, 5, 101, 102, 103, 7),
+    "t_er6": WorkloadSpec("t_er6", 0, 3_000, 60_000, 3, 0.0, 6_000, 1_000, 0, 6, 111, 112, 113, 5),
+    "t_er_sparse": WorkloadSpec("t_er_sparse", 0, 3_000, 45_000, 3, 0.0, 4_500, 750, 1, 6, 121, 122, 123, 9),
+    "t_er_tree": WorkloadSpec("t_er_tree", 0, 3_000, 30_000, 3, 0.0, 3_000, 600, 2, 5, 131, 132, 133, 13),
+    "t_rmat": WorkloadSpec("t_rmat", 1, 8_192, 60_000, 8, 1.0, 6_000, 1_000, 0, 5, 141, 142, 143, 17),
+    "t_tiny": WorkloadSpec("t_tiny", 0, 300, 2_400, 2, 0.0, 400, 50, 0, 4, 151, 152, 153, 3),
+}
+
+
+def _gen():
+    if not os.path.exists(GEN_LIB):
+        raise FileNotFoundError(f"{GEN_LIB} not built; run `python -m cgbdsm_b200.build`")
+    lib = ctypes.CDLL(GEN_LIB)
+    f = lib.cgbgen_workload
+    f.argtypes = [ctypes.c_char_p] * 3 + [ctypes.c_int, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_double,
+                                          ctypes.c_double, ctypes.c_double, ctypes.c_uint32, ctypes.c_double,
+                                          ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64,
+                                          ctypes.c_int, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint64,
+                                          ctypes.POINTER(ctypes.c_uint32)]
+    return f
+
+
+def materialize(spec: WorkloadSpec, directory: str) -> dict[str, str]:
+    """Writes data.graph, update.graph and query.graph for spec (cached by name)."""
+    d = os.path.join(directory, spec.name)
+    paths = {k: os.path.join(d, f"{k}.graph") for k in ("data", "update", "query")}
+    stamp = os.path.join(d, "spec.txt")
+    if all(os.path.exists(p) for p in paths.values()) and os.path.exists(stamp):
+        if open(stamp).read() == repr(spec):
+            return paths
+    os.makedirs(d, exist_ok=True)
+    qe = ctypes.c_uint32(0)
+    rc = _gen()(paths["data"].encode(), paths["update"].encode(), paths["query"].encode(), spec.kind, spec.n,
+                spec.m, 0.57, 0.19, 0.19, spec.labels, spec.zipf, spec.holdout, spec.seed_graph,
+                spec.seed_labels, spec.seed_holdout, spec.qshape, spec.qsize, spec.max_qedges, spec.seed_query,
+                ctypes.byref(qe))
+    if rc != 0:
+        raise RuntimeError(f"workload generation failed for {spec.name}: rc={rc}")
+    with open(stamp, "w") as f:
+        f.write(repr(spec))
+    return paths
+
+
+def read_query(path: str) -> tuple[list[int], list[tuple[int, int]]]:
+    labels: dict[int, int] = {}
+    edges: list[tuple[int, int]] = []
+    for line in open(path):
+        t = line.split()
+        if not t:
+            continue
+        if t[0] == "v":
+            labels[int(t[1])] = int(t[2])
+        elif t[0] == "e":
+            edges.append((int(t[1]), int(t[2])))
+    return [labels[i] for i in range(len(labels))], edges

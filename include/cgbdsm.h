@@ -46,9 +46,12 @@ typedef struct {
     uint64_t pool_words;     /* neighbour-run pool capacity in u32 words; 0 = automatic     */
     uint32_t dfs_blocks_per_sm; /* persistent DFS blocks per SM; 0 = automatic              */
     uint32_t flags;          /* CGB_FLAG_* below                                           */
+    uint32_t dfs_budget_ms;  /* wall-clock budget of one matching launch; past it the batch
+                                fails with CGB_ERR_TIMEOUT (count incomplete); 0 = 600 s   */
 } cgb_config;
 
 #define CGB_FLAG_NO_MERGE_BACK_DEFER 0x1u /* apply the delta merge-back eagerly after matching */
+#define CGB_FLAG_ENUMERATE_TAIL 0x2u      /* enumerate degree-1 tail vertices instead of counting them */
 
 /* Limits (reference: utils/config.h:5-6; key layout calig_helper_gamma.cu:228-229). */
 #define CGB_MAX_QV 12
@@ -65,12 +68,17 @@ void cgb_destroy(cgb_handle* h);
 /* Text of the last error on this handle ("" if none).  Valid until the next call. */
 const char* cgb_last_error(const cgb_handle* h);
 
-/* Loads the query pattern: qv vertices (<= 12), qe undirected edges given as
- * (a, b) pairs, a != b.  Directed indices follow graph.cpp:137-148 (CSR order:
- * vertex ascending, neighbour ascending); undirected edge order graph.cpp:184-199.
- * Replaces CPUGraphLoader::SetQueryMeta + GPUGraphLoader::LoadQuery
- * (graph.cpp:123-209, graph_gpu.cu:156-172).  2*qe must be <= 32. */
-cgb_status cgb_load_query(cgb_handle* h, uint32_t qv, uint32_t qe, const uint32_t* edges);
+/* Loads the query pattern: qv vertices (<= 12, connected), their labels
+ * (NULL = unknown), qe undirected edges given as (a, b) pairs, a != b.
+ * Directed indices follow graph.cpp:137-148 (CSR order: vertex ascending,
+ * neighbour ascending); undirected edge order graph.cpp:184-199.  Labels let
+ * the matcher count degree-1 tail vertices of different labels independently;
+ * they must be the labels the producer used (lists of a direction (a -> b)
+ * hold only vertices of b's label).  Replaces CPUGraphLoader::SetQueryMeta +
+ * GPUGraphLoader::LoadQuery (graph.cpp:123-209, graph_gpu.cu:156-172).
+ * 2*qe must be <= 32. */
+cgb_status cgb_load_query(cgb_handle* h, uint32_t qv, const uint32_t* labels, uint32_t qe,
+                          const uint32_t* edges);
 /* Same, from a query file in the reference text format (graph.cpp:43-121). */
 cgb_status cgb_load_query_file(cgb_handle* h, const char* path);
 /* Directed index of query edge (a -> b), or 255 if not an edge. */
@@ -126,11 +134,64 @@ cgb_status cgb_last_edge_counts(const cgb_handle* h, uint64_t* out, uint32_t cap
 cgb_status cgb_read_index(cgb_handle* h, uint64_t* out, uint64_t cap, uint64_t* n);
 
 /* Timing of the last batch on the device (CUDA events, milliseconds):
- * t[0] index update, t[1] delta lists, t[2] matching, t[3] total. */
+ * t[0] index update, t[1] delta lists, t[2] matching, t[3] the whole batch
+ * (first to last device operation, before the final count read-back). */
 cgb_status cgb_last_timings(const cgb_handle* h, float* t4);
 
 /* Number of kernels this engine has launched so far. */
 uint64_t cgb_kernel_launches(const cgb_handle* h);
+
+/* Work counters of the last batch (8 entries): [0] seeds (delta edges
+ * expanded), [1] 32-candidate chunks evaluated, [2] candidates tested,
+ * [3] tail counts, [4] matching algorithmic bytes (seed keys 8 B, list records
+ * 16 B, candidate words 4 B, one 32 B sector per binary-search step),
+ * [5] index-update algorithmic bytes (edits 8 B, old and new run words 4 B,
+ * record 32 B per touched run), [6] touched runs, [7] reserved. */
+cgb_status cgb_last_stats(const cgb_handle* h, uint64_t* out8);
+
+/* The engine's CUDA stream (a cudaStream_t) on which all its work runs. */
+void* cgb_stream(const cgb_handle* h);
+
+/* ------------------------------------------------------------------------
+ * Stage-1 producer: the CaLiG candidate index on the host and the host
+ * staging that turns its deltas into the keys above.  Replaces, per batch,
+ * CaLiG::updateIndex / ConstructUpdate / mergeDeltas (calig.cpp:950-1088)
+ * and CaLiGHelperGamma::PrepareUpdateAll / PrepareUpdateIndex
+ * (calig_helper_gamma.cu:363-445); at open, CaLiG::inputQ/inputG/inputUpdate,
+ * constructCand, staticFilter and ConvertGlobalIndex's key generation
+ * (calig.cpp:111-216, 325-356, 705-733; calig_helper_gamma.cu:238-311).
+ * Compressed ids are assigned append-only to vertices with any LI bit, in
+ * ascending original-id order per batch.
+ * ------------------------------------------------------------------------ */
+typedef struct cgb_producer cgb_producer;
+
+typedef struct {
+    const uint64_t* ins;   uint64_t n_ins;
+    const uint64_t* del;   uint64_t n_del;
+    const uint64_t* delta; uint64_t n_delta;
+    const uint8_t* edge_ok;  /* qe entries */
+    uint32_t qe;
+    uint32_t dv_count;
+    uint32_t batch;
+    uint32_t num_edges;      /* insertions listed in this batch */
+    double ms_update_index;  /* reference timer [S1] updateIndex (main_calig.cpp:224-226) */
+    double ms_construct_update;
+    double ms_prepare;       /* [S1] PrepareUpdateAll + PrepareUpdateIndex */
+} cgb_batch_keys;
+
+/* batch_size_ints counts ints, two per edge, as the reference CLI does
+ * (main_calig.cpp:65-69, 103-104); UINT32_MAX = one batch. */
+cgb_status cgb_producer_open(const char* query_path, const char* data_path, const char* update_path,
+                             uint32_t batch_size_ints, uint32_t threads, cgb_producer** out);
+void cgb_producer_close(cgb_producer* p);
+const char* cgb_producer_last_error(const cgb_producer* p);
+uint32_t cgb_producer_num_batches(const cgb_producer* p);
+/* Initial index keys (pointer valid until close) and compressed-vertex count. */
+cgb_status cgb_producer_initial(cgb_producer* p, const uint64_t** keys, uint64_t* n, uint32_t* dv_count);
+/* Runs Stage 1 for the next batch; arrays valid until the next call. */
+cgb_status cgb_producer_next(cgb_producer* p, cgb_batch_keys* out);
+/* Compressed id -> original vertex id (valid until the next producer call). */
+cgb_status cgb_producer_vertex_map(const cgb_producer* p, const uint32_t** new2old, uint32_t* n);
 
 #ifdef __cplusplus
 }

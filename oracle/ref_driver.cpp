@@ -82,6 +82,10 @@ struct RefPipeline {
     uint64_t total_count = 0;
     int dfs_parallel = 0;
     int do_count = 1;
+    // bounded sampling of the count (bench baseline): stop after budget_ms
+    double sample_budget_ms = 0;
+    uint64_t sample_rows_done = 0, sample_rows_total = 0;
+    double sample_ms = 0;
 
     // calig_helper_gamma.cu:77-105 (UpdateVertexMappingCPU) and :132-154
     // (buildGlobalVertexMapping): every vertex with any LI bit gets the next
@@ -241,7 +245,11 @@ struct RefPipeline {
     }
 
     // enumeration.cu:727-809 without masks, then cpu_dfs.cpp:137-170.
+    // With sample_budget_ms > 0 the rows are counted in chunks until the budget
+    // is spent; rows_done / rows_total are recorded for extrapolation.
     uint64_t count_matches() {
+        auto t_begin = Clock::now();
+        sample_rows_done = sample_rows_total = 0;
         const OrderPerEdge& go = plan->global_order_;
         const uint32_t qv0 = go.vs_[0], qv1 = go.vs_[1];
         const uint32_t idx = eidx(qv0, qv1);
@@ -264,14 +272,22 @@ struct RefPipeline {
             }
             const uint64_t n = rows.size() / 2;
             last_seed_rows += n;
+            sample_rows_total += n;
             if (n == 0) continue;
-            if (dfs_parallel) {
-                tbb::task_arena arena;
-                total += cpuExtendBFSAllBitCountParallel(rows.data(), n, 2, *mirror, query, *plan, arena);
-            } else {
-                total += cpuExtendBFSAllBitCount(rows.data(), n, 2, *mirror, query, *plan);
+            const uint64_t chunk = sample_budget_ms > 0 ? 4096 : n;
+            for (uint64_t r0 = 0; r0 < n; r0 += chunk) {
+                if (sample_budget_ms > 0 && ms_since(t_begin) > sample_budget_ms) break;
+                const uint64_t k = std::min(chunk, n - r0);
+                if (dfs_parallel) {
+                    tbb::task_arena arena;
+                    total += cpuExtendBFSAllBitCountParallel(rows.data() + 2 * r0, k, 2, *mirror, query, *plan, arena);
+                } else {
+                    total += cpuExtendBFSAllBitCount(rows.data() + 2 * r0, k, 2, *mirror, query, *plan);
+                }
+                sample_rows_done += k;
             }
         }
+        sample_ms = ms_since(t_begin);
         return total;
     }
 
@@ -311,6 +327,13 @@ void cgbref_close(void* h) { delete (RefPipeline*)h; }
 void cgbref_set_parallel_dfs(void* h, int on) { ((RefPipeline*)h)->dfs_parallel = on; }
 // 0 = skip the match count (S1/staging/mirror only).
 void cgbref_set_count(void* h, int on) { ((RefPipeline*)h)->do_count = on; }
+// Bounded count: stop after budget_ms (0 = complete count).
+void cgbref_set_sample_budget(void* h, double ms) { ((RefPipeline*)h)->sample_budget_ms = ms; }
+// Rows counted / rows total / ms spent in the last batch's count.
+void cgbref_last_sample(void* h, uint64_t* done, uint64_t* total, double* ms) {
+    auto* p = (RefPipeline*)h;
+    *done = p->sample_rows_done; *total = p->sample_rows_total; *ms = p->sample_ms;
+}
 uint32_t cgbref_num_batches(void* h) { return ((RefPipeline*)h)->num_batches; }
 uint32_t cgbref_num_updates(void* h) { return ((RefPipeline*)h)->num_updates; }
 uint32_t cgbref_num_dir(void* h) { return ((RefPipeline*)h)->num_dir; }

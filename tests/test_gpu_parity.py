@@ -1,0 +1,158 @@
+"""GPU parity: the engine (through the C ABI) against the oracle.
+
+Counts and index contents must be bit-exact:
+  * against the reference's own CPU path (oracle/_ref) on seeded workloads,
+  * against the C restatement (oracle/oracle.c) on random key streams and on
+    the edge cases the reference's pipeline has (empty delta, vertex-id growth,
+    duplicate inserts, removal of absent keys, invalid keys).
+"""
+import numpy as np
+import pytest
+
+from cgbdsm_b200 import CgbError, Engine
+from cgbdsm_b200.engine import FLAG_ENUMERATE_TAIL
+from cgbdsm_b200.workloads import SPECS, materialize, read_query
+from oracle import bind
+
+pytestmark = pytest.mark.gpu
+
+PIPELINE_CASES = ["t_tiny", "t_er5", "t_er6", "t_er_sparse", "t_er_tree"]
+
+
+def _key(d, u, v):
+    return (np.uint64(d) << np.uint64(59)) | (np.uint64(u) << np.uint64(32)) | np.uint64(v)
+
+
+@pytest.mark.parametrize("flags", [0, FLAG_ENUMERATE_TAIL], ids=["counted_tail", "enumerated_tail"])
+@pytest.mark.parametrize("name", PIPELINE_CASES)
+def test_engine_matches_reference_cpu_path(name, flags, workdir):
+    if not bind.have_ref():
+        pytest.skip("oracle/_ref/libcgbref.so not built")
+    spec = SPECS[name]
+    p = materialize(spec, workdir)
+    ref = bind.RefPipeline(p["query"], p["data"], p["update"], spec.cli_batch_size)
+    qlabels, qedges = read_query(p["query"])
+    eng = Engine(flags=flags)
+    eng.load_query(len(qlabels), qedges, qlabels)
+    orc = bind.Oracle(len(qlabels), qedges)
+    init = ref.init_keys()
+    eng.build_index(init, ref.dv_count)
+    orc.build(init, ref.dv_count)
+    assert np.array_equal(eng.read_index(), orc.dump())
+    nb = 0
+    while ref.step() >= 0:
+        r = ref.last()
+        c = eng.apply_batch(r["dv"], r["ins"], r["del"], r["delta"], r["edge_ok"])
+        co = orc.batch(r["dv"], r["ins"], r["del"], r["delta"], r["edge_ok"], bind.PER_EDGE)
+        assert c == r["count"], f"{name} batch {nb}: engine {c} != reference {r['count']}"
+        assert np.array_equal(eng.edge_counts(), orc.edge_counts())
+        assert co == c
+        nb += 1
+    assert np.array_equal(eng.read_index(), orc.dump())
+    ref.close()
+    eng.close()
+
+
+def _random_query(rng, qv, extra):
+    edges = set()
+    for v in range(1, qv):  # spanning tree
+        edges.add((int(rng.integers(0, v)), v))
+    cand = [(a, b) for a in range(qv) for b in range(a + 1, qv) if (a, b) not in edges]
+    rng.shuffle(cand)
+    for e in cand[:extra]:
+        edges.add(e)
+    return sorted(edges)
+
+
+def _sym_keys(orc, pairs_by_edge):
+    """pairs_by_edge: list of (a, b, x, y) = query edge (a,b) realised by data edge (x,y)."""
+    ks = []
+    for a, b, x, y in pairs_by_edge:
+        ks.append(_key(orc.L.orc_dir(orc.h, a, b), x, y))
+        ks.append(_key(orc.L.orc_dir(orc.h, b, a), y, x))
+    return np.array(ks, dtype=np.uint64) if ks else np.zeros(0, np.uint64)
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_random_symmetric_streams(seed):
+    rng = np.random.default_rng(1000 + seed)
+    qv = int(rng.integers(3, 7))
+    qedges = _random_query(rng, qv, int(rng.integers(0, 4)))
+    dv0 = 60
+    eng = Engine()
+    eng.load_query(qv, qedges)
+    orc = bind.Oracle(qv, qedges)
+
+    def rand_pairs(n, dv):
+        out = []
+        for _ in range(n):
+            a, b = qedges[int(rng.integers(0, len(qedges)))]
+            x, y = rng.choice(dv, 2, replace=False)
+            out.append((a, b, int(x), int(y)))
+        return out
+
+    init = np.unique(_sym_keys(orc, rand_pairs(900, dv0)))
+    eng.build_index(init, dv0)
+    orc.build(init, dv0)
+    dv = dv0
+    for b in range(6):
+        dv += int(rng.integers(0, 8))
+        ins = _sym_keys(orc, rand_pairs(int(rng.integers(0, 80)), dv))
+        cur = orc.dump()
+        dele = cur[rng.choice(len(cur), min(len(cur), int(rng.integers(0, 60))), replace=False)] if len(cur) else cur
+        # removing a key also removes its mirror, keeping the lists symmetric
+        rev = []
+        for k in dele:
+            d = int(k >> np.uint64(59)); u = int((k >> np.uint64(32)) & np.uint64(0x7FFFFFF)); v = int(k & np.uint64(0xFFFFFFFF))
+            src = [s for s in range(qv) for t in range(qv) if orc.L.orc_dir(orc.h, s, t) == d][0]
+            dst = [t for t in range(qv) if orc.L.orc_dir(orc.h, src, t) == d][0]
+            rev.append(_key(orc.L.orc_dir(orc.h, dst, src), v, u))
+        dele = np.concatenate([dele, np.array(rev, dtype=np.uint64)]) if len(rev) else dele
+        delta_pairs = rand_pairs(int(rng.integers(0, 40)), dv)
+        delta = _sym_keys(orc, delta_pairs)
+        # delta keys are also removed from the old index (ConstructUpdate, calig.cpp:776-804)
+        dele = np.concatenate([dele, delta]).astype(np.uint64)
+        c = eng.apply_batch(dv, ins, dele, delta)
+        co = orc.batch(dv, ins, dele, delta, None, bind.PER_EDGE)
+        assert c == co, f"seed {seed} batch {b}: engine {c} != oracle {co}"
+        assert np.array_equal(eng.edge_counts(), orc.edge_counts())
+        assert np.array_equal(eng.read_index(), orc.dump())
+    eng.close()
+
+
+def test_edge_cases():
+    qedges = [(0, 1), (1, 2), (0, 2)]
+    eng = Engine()
+    eng.load_query(3, qedges)
+    orc = bind.Oracle(3, qedges)
+    d01, d10 = eng.query_dir(0, 1), eng.query_dir(1, 0)
+    assert d01 == orc.L.orc_dir(orc.h, 0, 1) and d10 == orc.L.orc_dir(orc.h, 1, 0)
+    # empty initial index
+    eng.build_index(np.zeros(0, np.uint64), 4)
+    orc.build(np.zeros(0, np.uint64), 4)
+    assert len(eng.read_index()) == 0
+    # empty batch
+    assert eng.apply_batch(4, np.zeros(0, np.uint64), np.zeros(0, np.uint64), np.zeros(0, np.uint64)) == 0
+    # triangle 0-1-2 fully in delta: counted once per query edge? only via the max edge
+    tri = []
+    for (a, b), (x, y) in zip(qedges, [(0, 1), (1, 2), (0, 2)]):
+        tri += [_key(eng.query_dir(a, b), x, y), _key(eng.query_dir(b, a), y, x)]
+    tri = np.array(tri, dtype=np.uint64)
+    dup_ins = np.concatenate([tri[:2], tri[:2]])  # duplicate inserts are deduplicated
+    c = eng.apply_batch(5, dup_ins, tri, tri)  # dv grows 4 -> 5
+    co = orc.batch(5, dup_ins, tri, tri, None, bind.PER_EDGE)
+    assert c == co
+    assert np.array_equal(eng.read_index(), orc.dump())
+    # removing keys that are absent is a no-op; delta empty -> no matching, no merge-back
+    absent = np.array([_key(d01, 3, 4)], dtype=np.uint64)
+    assert eng.apply_batch(5, np.zeros(0, np.uint64), absent, np.zeros(0, np.uint64)) == 0
+    orc.batch(5, np.zeros(0, np.uint64), absent, np.zeros(0, np.uint64), None, bind.PER_EDGE)
+    assert np.array_equal(eng.read_index(), orc.dump())
+    # out-of-range keys are rejected with ERR_ARG and leave the handle usable
+    bad = np.array([_key(d01, 7, 1)], dtype=np.uint64)
+    with pytest.raises(CgbError):
+        eng.apply_batch(5, bad, np.zeros(0, np.uint64), np.zeros(0, np.uint64))
+    # decreasing dv_count is rejected
+    with pytest.raises(CgbError):
+        eng.apply_batch(4, np.zeros(0, np.uint64), np.zeros(0, np.uint64), np.zeros(0, np.uint64))
+    eng.close()
