@@ -46,6 +46,7 @@ namespace {
 
 constexpr uint32_t kFull = 0xffffffffu;
 constexpr int kDfsWarps = 8;  // warps per DFS block
+constexpr uint32_t kTaskCap = 1u << 20;  // stolen-range queue capacity (64 MiB)
 
 __constant__ EdgePlan c_plan[kMaxQE];
 
@@ -293,8 +294,13 @@ struct DfsArgs {
     unsigned long long* counts;  // [qe]
     unsigned int* work_next;
     unsigned int* err;
-    unsigned long long* stats;   // [8]: seeds, chunks, tested, tails, algorithmic bytes read
+    unsigned long long* stats;   // [8]: seeds, chunks, tested, tails, algorithmic bytes read, .., .., stolen tasks
     unsigned long long budget_ns;  // per-launch wall-clock budget (0 = unlimited)
+    uint32_t* tasks;             // stolen-range queue [task_cap][16 words]
+    uint32_t task_cap;
+    unsigned int* qctr;          // [8]: tail, head, created, completed, hungry, -, seeds issued
+    uint32_t epoch;              // per-launch tag written as a task's ready flag (never 0)
+    uint32_t force_split;        // split every long shallow range, hungry warps or not (tests)
 };
 
 __device__ __forceinline__ unsigned long long global_ns() {
@@ -335,66 +341,180 @@ __device__ __forceinline__ uint32_t list_at(const ListRef& L, uint32_t i) {
     return i < L.ml ? __ldg(L.m + i) : __ldg(L.d + (i - L.ml));
 }
 
-// |A ∩ B| (and ∩ C when C != nullptr) by probing the shortest list's elements.
-__device__ uint64_t inter_count(const ListRef& A, const ListRef& Bl, const ListRef* C) {
-    const ListRef* s = &A;
-    const ListRef* o1 = &Bl;
-    if (Bl.ml + Bl.dl < A.ml + A.dl) { s = &Bl; o1 = &A; }
-    uint64_t c = 0;
-    const uint32_t n = s->ml + s->dl;
-    for (uint32_t i = 0; i < n; ++i) {
-        const uint32_t x = list_at(*s, i);
-        if (list_has(*o1, x) && (!C || list_has(*C, x))) ++c;
+// Number of x in the intersection of the resolved lists bn[ids[0..nl)] with x
+// not among the matched core vertices m[0..nc).  Warp-cooperative; the result
+// is warp-uniform.  One list: its length minus the core vertices it holds.
+// Several: the shortest list is scanned 32 elements at a time and each
+// element probed in the others.
+__device__ unsigned long long isect_count(const uint4* bn, const uint8_t* ids, uint32_t nl, const uint32_t* m,
+                                          uint32_t nc, const uint32_t* __restrict__ pool,
+                                          const uint32_t* __restrict__ dval, uint32_t lane,
+                                          unsigned long long& bytes) {
+    if (nl == 1) {
+        const uint4 r = bn[ids[0]];
+        bool in = false;
+        if (lane < nc) {
+            in = list_contains(pool, dval, r, m[lane]);
+            bytes += 32u * (33u - __clz(r.y | 1u));
+        }
+        return (unsigned long long)(r.y + r.w) - __popc(__ballot_sync(kFull, in));
+    }
+    uint32_t g = 0, glen = 0xffffffffu;
+    for (uint32_t i = 0; i < nl; ++i) {
+        const uint4 r = bn[ids[i]];
+        if (r.y + r.w < glen) { glen = r.y + r.w; g = i; }
+    }
+    const uint4 gr = bn[ids[g]];
+    unsigned long long c = 0;
+    for (uint32_t base = 0; base < glen; base += 32) {
+        const uint32_t idx = base + lane;
+        bool ok = idx < glen;
+        if (ok) {
+            const uint32_t x = idx < gr.y ? __ldg(pool + gr.x + idx) : __ldg(dval + gr.z + (idx - gr.y));
+            bytes += 4;
+            for (uint32_t t = 0; t < nc; ++t) ok &= (x != m[t]);
+            for (uint32_t i = 0; i < nl && ok; ++i) {
+                if (i == g) continue;
+                const uint4 r = bn[ids[i]];
+                bytes += 32u * (33u - __clz(r.y | 1u));
+                ok = list_contains(pool, dval, r, x);
+            }
+        }
+        c += __popc(__ballot_sync(kFull, ok));
     }
     return c;
 }
 
-// Number of injective assignments of the tail leaves given the matched core
-// m[0..n_core) (m[n_core-1] passed as `last`), as a product over label groups
-// of inclusion-exclusion over the group's candidate lists minus the core.
-__device__ unsigned long long tail_count(const EdgePlan& P, const uint32_t* m, uint32_t last, const uint4* rec,
-                                         uint32_t dvcap, const uint32_t* pool, const uint32_t* dval) {
+// Number of injective assignments of the tail vertices given the matched core
+// m[0..n_core): per label group, inclusion-exclusion over the sizes of the
+// members' candidate sets and of their intersections (core vertices
+// excluded); groups multiply.  Warp-cooperative, warp-uniform result.
+__device__ unsigned long long tail_count_warp(const EdgePlan& P, const uint32_t* m, uint4* bn, const uint4* rec,
+                                              uint32_t dvcap, const uint32_t* __restrict__ pool,
+                                              const uint32_t* __restrict__ dval, uint32_t lane,
+                                              unsigned long long& bytes) {
     const uint32_t nc = P.n_core, n = P.n;
-    auto mv = [&](uint32_t pos) { return pos == nc - 1 ? last : m[pos]; };
+    // resolve every tail BN record once
+    for (uint32_t k = P.bn_off[nc] + lane; k < P.bn_off[n]; k += 32) {
+        uint4 r = rec[(size_t)P.bn_dir[k] * dvcap + m[P.bn_pos[k]]];
+        if (!P.bn_dvis[k]) r.w = 0;
+        bn[k] = r;
+        bytes += 16;
+    }
+    __syncwarp();
     unsigned long long prod = 1;
     uint32_t t = nc;
     while (t < n && prod) {
         uint32_t e = t;
         while (e < n && P.tail_gid[e] == P.tail_gid[t]) ++e;
         const uint32_t k = e - t;
-        ListRef L[3];
-        uint64_t sz[3];
-        for (uint32_t i = 0; i < k; ++i) {
-            const uint32_t bk = P.bn_off[t + i];
-            uint4 r = rec[(size_t)P.bn_dir[bk] * dvcap + mv(P.bn_pos[bk])];
-            if (!P.bn_dvis[bk]) r.w = 0;
-            L[i] = ListRef{pool + r.x, r.y, dval + r.z, r.w};
-            uint64_t c = (uint64_t)r.y + r.w;
-            for (uint32_t q = 0; q < nc; ++q)
-                if (list_has(L[i], mv(q))) --c;
-            sz[i] = c;
+        unsigned long long sc[8];
+        for (uint32_t mask = 1; mask < (1u << k); ++mask) {
+            uint8_t ids[kMaxBN];
+            uint32_t nl = 0;
+            for (uint32_t i = 0; i < k; ++i)
+                if (mask & (1u << i))
+                    for (uint32_t q = P.bn_off[t + i]; q < P.bn_off[t + i + 1]; ++q) ids[nl++] = (uint8_t)q;
+            sc[mask] = isect_count(bn, ids, nl, m, nc, pool, dval, lane, bytes);
         }
         unsigned long long g;
-        if (k == 1) {
-            g = sz[0];
-        } else {
-            // pairwise (and triple) intersections, core vertices excluded
-            auto inter_ex = [&](uint32_t i, uint32_t j) {
-                uint64_t c = inter_count(L[i], L[j], nullptr);
-                for (uint32_t q = 0; q < nc; ++q)
-                    if (list_has(L[i], mv(q)) && list_has(L[j], mv(q))) --c;
-                return c;
-            };
-            if (k == 2) {
-                g = sz[0] * sz[1] - inter_ex(0, 1);
+        if (k == 1) g = sc[1];
+        else if (k == 2) g = sc[1] * sc[2] - sc[3];
+        else g = sc[1] * sc[2] * sc[4] - sc[3] * sc[4] - sc[5] * sc[2] - sc[6] * sc[1] + 2 * sc[7];
+        prod *= g;
+        t = e;
+    }
+    return prod;
+}
+
+// At the last core depth j = n_core - 1 the prefix m[0..j) is fixed while all
+// candidates of position j are scanned.  Subsets of a tail group whose lists
+// hang only off prefix vertices have counts that do not depend on the
+// candidate: tail_prepare computes them once per prefix (excluding the prefix
+// vertices); tail_eval then only subtracts whether the candidate itself lies
+// in the set, and scans only the subsets that involve position j.
+constexpr unsigned long long kDynamic = ~0ull;
+
+__device__ void tail_prepare(const EdgePlan& P, const uint32_t* m, uint4* bn, unsigned long long* cache,
+                             const uint4* rec, uint32_t dvcap, const uint32_t* __restrict__ pool,
+                             const uint32_t* __restrict__ dval, uint32_t lane, unsigned long long& bytes) {
+    const uint32_t nc = P.n_core, n = P.n, j = nc - 1;
+    for (uint32_t k = P.bn_off[nc] + lane; k < P.bn_off[n]; k += 32) {
+        if (P.bn_pos[k] >= j) continue;
+        uint4 r = rec[(size_t)P.bn_dir[k] * dvcap + m[P.bn_pos[k]]];
+        if (!P.bn_dvis[k]) r.w = 0;
+        bn[k] = r;
+        bytes += 16;
+    }
+    __syncwarp();
+    uint32_t t = nc;
+    while (t < n) {
+        uint32_t e = t;
+        while (e < n && P.tail_gid[e] == P.tail_gid[t]) ++e;
+        const uint32_t k = e - t;
+        for (uint32_t mask = 1; mask < (1u << k); ++mask) {
+            uint8_t ids[kMaxBN];
+            uint32_t nl = 0;
+            bool dynamic = false;
+            for (uint32_t i = 0; i < k; ++i)
+                if (mask & (1u << i))
+                    for (uint32_t q = P.bn_off[t + i]; q < P.bn_off[t + i + 1]; ++q) {
+                        ids[nl++] = (uint8_t)q;
+                        dynamic |= P.bn_pos[q] == j;
+                    }
+            const unsigned long long v = dynamic ? kDynamic : isect_count(bn, ids, nl, m, j, pool, dval, lane, bytes);
+            if (lane == 0) cache[t * 8 + mask] = v;
+        }
+        t = e;
+    }
+    __syncwarp();
+}
+
+// Tail count for the core embedding m[0..n_core) (m[j] = the candidate).
+__device__ unsigned long long tail_eval(const EdgePlan& P, const uint32_t* m, uint4* bn,
+                                        const unsigned long long* cache, const uint4* rec, uint32_t dvcap,
+                                        const uint32_t* __restrict__ pool, const uint32_t* __restrict__ dval,
+                                        uint32_t lane, unsigned long long& bytes) {
+    const uint32_t nc = P.n_core, n = P.n, j = nc - 1;
+    const uint32_t c = m[j];
+    for (uint32_t k = P.bn_off[nc] + lane; k < P.bn_off[n]; k += 32) {
+        if (P.bn_pos[k] != j) continue;
+        uint4 r = rec[(size_t)P.bn_dir[k] * dvcap + c];
+        if (!P.bn_dvis[k]) r.w = 0;
+        bn[k] = r;
+        bytes += 16;
+    }
+    __syncwarp();
+    unsigned long long prod = 1;
+    uint32_t t = nc;
+    while (t < n && prod) {
+        uint32_t e = t;
+        while (e < n && P.tail_gid[e] == P.tail_gid[t]) ++e;
+        const uint32_t k = e - t;
+        unsigned long long sc[8];
+        for (uint32_t mask = 1; mask < (1u << k); ++mask) {
+            uint8_t ids[kMaxBN];
+            uint32_t nl = 0;
+            for (uint32_t i = 0; i < k; ++i)
+                if (mask & (1u << i))
+                    for (uint32_t q = P.bn_off[t + i]; q < P.bn_off[t + i + 1]; ++q) ids[nl++] = (uint8_t)q;
+            const unsigned long long cv = cache[t * 8 + mask];
+            if (cv != kDynamic) {
+                bool in = true;
+                if (lane < nl) {
+                    const uint4 r = bn[ids[lane]];
+                    in = list_contains(pool, dval, r, c);
+                    bytes += 32u * (33u - __clz(r.y | 1u));
+                }
+                sc[mask] = cv - (__all_sync(kFull, in) ? 1ull : 0ull);
             } else {
-                uint64_t i01 = inter_ex(0, 1), i02 = inter_ex(0, 2), i12 = inter_ex(1, 2);
-                uint64_t i012 = inter_count(L[0], L[1], &L[2]);
-                for (uint32_t q = 0; q < nc; ++q)
-                    if (list_has(L[0], mv(q)) && list_has(L[1], mv(q)) && list_has(L[2], mv(q))) --i012;
-                g = sz[0] * sz[1] * sz[2] - i01 * sz[2] - i02 * sz[1] - i12 * sz[0] + 2 * i012;
+                sc[mask] = isect_count(bn, ids, nl, m, nc, pool, dval, lane, bytes);
             }
         }
+        unsigned long long g;
+        if (k == 1) g = sc[1];
+        else if (k == 2) g = sc[1] * sc[2] - sc[3];
+        else g = sc[1] * sc[2] * sc[4] - sc[3] * sc[4] - sc[5] * sc[2] - sc[6] * sc[1] + 2 * sc[7];
         prod *= g;
         t = e;
     }
@@ -406,10 +526,23 @@ __device__ __forceinline__ unsigned long long warp_sum(unsigned long long x) {
     return x;
 }
 
+// Work units of the DFS: seeds (delta edges) from a counter, and stolen
+// ranges from a queue.  A task is 16 words: w0 = ei | depth << 8 | generator
+// << 16, w1/w2 = [lo, hi) of the generator list, w3 = ready flag, w4..15 =
+// the matched prefix.  A warp at a shallow depth whose remaining range is long
+// while other warps are hungry publishes the upper half of the range.
+// Termination: a warp leaves when completed == seeds + created (completed
+// read first); a unit's pushes happen before its completion, so equality
+// means no unit is active and none can be created.
+constexpr uint32_t kTaskWords = 16;
+constexpr uint32_t kSplitMaxDepth = 5;
+constexpr uint32_t kSplitMinRemaining = 96;
+
 __global__ void __launch_bounds__(kDfsWarps * 32) k_dfs_count(DfsArgs a) {
     __shared__ uint32_t s_cand[kDfsWarps][kMaxQV][32];
     __shared__ uint4 s_bn[kDfsWarps][kMaxBN];
     __shared__ uint32_t s_m[kDfsWarps][kMaxQV];
+    __shared__ unsigned long long s_tc[kDfsWarps][kMaxQV * 8];
     __shared__ uint32_t s_pre[kMaxQE + 1];
     __shared__ uint32_t s_lo[kMaxQE];
 
@@ -422,24 +555,100 @@ __global__ void __launch_bounds__(kDfsWarps * 32) k_dfs_count(DfsArgs a) {
     const uint64_t vmask = (1ull << a.B) - 1ull;
     uint32_t* m = s_m[w];
     uint4* bn = s_bn[w];
+    volatile unsigned int* vq = a.qctr;  // [0] tail, [1] head, [2] created, [3] completed, [4] hungry
 
     // per-depth state held by lane == depth
     uint32_t st_ncand = 0, st_pos = 0, st_next = 0, st_len = 0, st_gen = 0;
     unsigned long long cnt = 0;  // lane-local partial count of the current edge
-    unsigned long long n_seeds = 0, n_chunks = 0, n_tested = 0, n_tail = 0;
+    unsigned long long n_seeds = 0, n_chunks = 0, n_tested = 0, n_tail = 0, n_tasks = 0;
     unsigned long long n_bytes = 0;  // algorithmic bytes: seed keys, records, list words, probe sectors
     int cur_ei = -1;
     const unsigned long long t_start = global_ns();
     uint32_t steps = 0;
     bool out_of_time = false;
+    bool hungry = false;
+    uint32_t idle_spins = 0;
 
     for (;;) {
-        uint32_t item = 0;
-        if (lane == 0) item = atomicAdd(a.work_next, 1u);
+        // ---- acquire a unit: 1 = seed, 2 = task, 3 = all done, 0 = nothing yet
+        uint32_t kind = 0, item = 0;
+        if (lane == 0) {
+            if (vq[6] < total) {  // vq[6] mirrors work_next without incrementing it
+                item = atomicAdd(a.work_next, 1u);
+                if (item < total) kind = 1;
+                else atomicMax((unsigned int*)&a.qctr[6], total);
+            }
+            if (!kind) {
+                const unsigned int h = vq[1];
+                if (h < vq[0] && atomicCAS((unsigned int*)&a.qctr[1], h, h + 1) == h) {
+                    kind = 2;
+                    item = h;
+                } else {
+                    const unsigned int done = vq[3];
+                    __threadfence();
+                    const unsigned int made = vq[2];
+                    if (done == total + made && vq[6] >= total) kind = 3;
+                }
+            }
+        }
+        kind = __shfl_sync(kFull, kind, 0);
         item = __shfl_sync(kFull, item, 0);
-        if (item >= total) break;
+        if (kind == 3) break;
+        if (kind == 0) {
+            if (lane == 0 && !hungry) atomicAdd((unsigned int*)&a.qctr[4], 1u);
+            hungry = true;
+            __nanosleep(256 + 32 * (idle_spins & 31));
+            ++idle_spins;
+            if ((idle_spins & 255u) == 0) {
+                const bool late = a.budget_ns && (global_ns() - t_start) > a.budget_ns;
+                if (__shfl_sync(kFull, late ? 1 : 0, 0)) { out_of_time = true; break; }
+            }
+            continue;
+        }
+        if (hungry) {
+            if (lane == 0) atomicSub((unsigned int*)&a.qctr[4], 1u);
+            hungry = false;
+        }
+        idle_spins = 0;
+
         int ei = 0;
-        while (ei + 1 < (int)a.qe && s_pre[ei + 1] <= item) ++ei;
+        uint32_t jbase = 2, tgen = 0, tlo = 0, thi = 0;
+        if (kind == 1) {
+            while (ei + 1 < (int)a.qe && s_pre[ei + 1] <= item) ++ei;
+            const uint64_t key = a.dkeys[s_lo[ei] + (item - s_pre[ei])];
+            if (lane == 0) {
+                m[0] = (uint32_t)((key >> a.B) & vmask);
+                m[1] = (uint32_t)(key & vmask);
+                n_bytes += 8;
+            }
+            ++n_seeds;
+        } else {
+            // the producer reserved the slot before publishing; wait (bounded) for the data
+            volatile uint32_t* tk = a.tasks + (size_t)item * kTaskWords;
+            uint32_t ready = 0;
+            if (lane == 0) {
+                for (uint32_t it = 0; it < (1u << 22); ++it) {
+                    if (tk[3] == a.epoch) { ready = 1; break; }
+                    __nanosleep(64);
+                }
+            }
+            ready = __shfl_sync(kFull, ready, 0);
+            if (!ready) {  // never published: give up cleanly
+                if (lane == 0) atomicOr(a.err, 16u);
+                break;
+            }
+            __threadfence();
+            const uint32_t wv = lane < kTaskWords ? tk[lane] : 0;
+            const uint32_t w0 = __shfl_sync(kFull, wv, 0);
+            ei = (int)(w0 & 0xffu);
+            jbase = (w0 >> 8) & 0xffu;
+            tgen = (w0 >> 16) & 0xffu;
+            tlo = __shfl_sync(kFull, wv, 1);
+            thi = __shfl_sync(kFull, wv, 2);
+            if (lane >= 4 && lane < 4 + kMaxQV) m[lane - 4] = wv;
+            ++n_tasks;
+        }
+        __syncwarp();
         if (ei != cur_ei) {
             const unsigned long long c = warp_sum(cnt);
             if (cur_ei >= 0 && lane == 0 && c) atomicAdd(a.counts + cur_ei, c);
@@ -447,24 +656,16 @@ __global__ void __launch_bounds__(kDfsWarps * 32) k_dfs_count(DfsArgs a) {
             cur_ei = ei;
         }
         const EdgePlan& P = c_plan[ei];
-        const uint64_t key = a.dkeys[s_lo[ei] + (item - s_pre[ei])];
-        if (lane == 0) {
-            m[0] = (uint32_t)((key >> a.B) & vmask);
-            m[1] = (uint32_t)(key & vmask);
-        }
-        ++n_seeds;
-        if (lane == 0) n_bytes += 8;
-        __syncwarp();
         const uint32_t nc = P.n_core;
-        if (nc == 2) {  // the seed edge alone is the core: only the tail remains
-            if (lane == 0) {
-                cnt += (P.n == 2) ? 1ull : tail_count(P, m, m[1], a.rec, a.dvcap, a.pool, a.dval);
-                ++n_tail;
-            }
+        const bool has_tail = nc < P.n;
+        if (kind == 1 && nc == 2) {  // the seed edge alone is the core: only the tail remains
+            const unsigned long long tc =
+                (P.n == 2) ? 1ull : tail_count_warp(P, m, bn, a.rec, a.dvcap, a.pool, a.dval, lane, n_bytes);
+            if (lane == 0) { cnt += tc; ++n_tail; }
             __syncwarp();
+            if (lane == 0) { __threadfence(); atomicAdd((unsigned int*)&a.qctr[3], 1u); }
             continue;
         }
-        const bool has_tail = nc < P.n;
 
         // set up depth j: resolve BN records, choose the shortest list as generator
         auto setup = [&](uint32_t j) {
@@ -487,11 +688,15 @@ __global__ void __launch_bounds__(kDfsWarps * 32) k_dfs_count(DfsArgs a) {
             }
             if (lane == j) { st_ncand = 0; st_pos = 0; st_next = 0; st_len = nb ? best : 0; st_gen = bl; }
             __syncwarp();
+            if (has_tail && j == nc - 1 && nb && best)
+                tail_prepare(P, m, bn, s_tc[w], a.rec, a.dvcap, a.pool, a.dval, lane, n_bytes);
         };
 
-        setup(2);
-        uint32_t j = 2;
-        while (j >= 2) {
+        setup(jbase);
+        if (kind == 2 && lane == jbase) { st_gen = tgen; st_next = tlo; st_len = thi; }
+        __syncwarp();
+        uint32_t j = jbase;
+        while (j >= jbase) {
             if (a.budget_ns && ((++steps & 1023u) == 0)) {
                 // bounded run: give up (and report) once the budget is spent
                 unsigned long long now = global_ns();
@@ -509,9 +714,36 @@ __global__ void __launch_bounds__(kDfsWarps * 32) k_dfs_count(DfsArgs a) {
                 continue;
             }
             const uint32_t gnext = __shfl_sync(kFull, st_next, j);
-            const uint32_t glen = __shfl_sync(kFull, st_len, j);
+            uint32_t glen = __shfl_sync(kFull, st_len, j);
             if (gnext < glen) {
                 const uint32_t g = __shfl_sync(kFull, st_gen, j);
+                // share the rest of a long shallow range with hungry warps
+                if (j <= kSplitMaxDepth && glen - gnext >= kSplitMinRemaining) {
+                    uint32_t slot = 0xffffffffu;
+                    if (lane == 0 && (vq[4] > 0 || a.force_split)) {
+                        const unsigned int t = vq[0];
+                        if (t < a.task_cap && atomicCAS((unsigned int*)&a.qctr[0], t, t + 1) == t) {
+                            atomicAdd((unsigned int*)&a.qctr[2], 1u);
+                            slot = t;
+                        }
+                    }
+                    slot = __shfl_sync(kFull, slot, 0);
+                    if (slot != 0xffffffffu) {
+                        const uint32_t mid = gnext + 32u + (((glen - gnext - 32u) / 2u) & ~31u);
+                        uint32_t* tk = a.tasks + (size_t)slot * kTaskWords;
+                        uint32_t v = 0;
+                        if (lane == 0) v = (uint32_t)ei | (j << 8) | (g << 16);
+                        else if (lane == 1) v = mid;
+                        else if (lane == 2) v = glen;
+                        else if (lane >= 4 && lane < 4 + kMaxQV) v = (lane - 4 < j) ? m[lane - 4] : 0u;
+                        if (lane < kTaskWords && lane != 3) tk[lane] = v;
+                        __threadfence();
+                        __syncwarp();
+                        if (lane == 0) *(volatile uint32_t*)(tk + 3) = a.epoch;
+                        if (lane == j) st_len = mid;
+                        glen = mid;
+                    }
+                }
                 const uint32_t o0 = P.bn_off[j], o1 = P.bn_off[j + 1];
                 const uint4 gr = bn[o0 + g];
                 const uint32_t idx = gnext + lane;
@@ -534,9 +766,18 @@ __global__ void __launch_bounds__(kDfsWarps * 32) k_dfs_count(DfsArgs a) {
                 ++n_chunks;
                 if (j == nc - 1) {
                     if (has_tail) {
-                        if (ok) {
-                            cnt += tail_count(P, m, c, a.rec, a.dvcap, a.pool, a.dval);
-                            ++n_tail;
+                        // every surviving candidate completes a core embedding: count its tail
+                        uint32_t bal = __ballot_sync(kFull, ok);
+                        while (bal) {
+                            const int l = __ffs(bal) - 1;
+                            bal &= bal - 1;
+                            const uint32_t cl = __shfl_sync(kFull, c, l);
+                            if (lane == 0) m[j] = cl;
+                            __syncwarp();
+                            const unsigned long long tc =
+                                tail_eval(P, m, bn, s_tc[w], a.rec, a.dvcap, a.pool, a.dval, lane, n_bytes);
+                            if (lane == 0) { cnt += tc; ++n_tail; }
+                            __syncwarp();
                         }
                     } else {
                         cnt += ok ? 1ull : 0ull;
@@ -556,7 +797,10 @@ __global__ void __launch_bounds__(kDfsWarps * 32) k_dfs_count(DfsArgs a) {
             if (lane == 0) atomicOr(a.err, 8u);
             break;
         }
+        if (lane == 0) { __threadfence(); atomicAdd((unsigned int*)&a.qctr[3], 1u); }
     }
+    if (out_of_time && lane == 0) atomicOr(a.err, 8u);
+    if (hungry && lane == 0) atomicSub((unsigned int*)&a.qctr[4], 1u);
     const unsigned long long c = warp_sum(cnt);
     if (cur_ei >= 0 && lane == 0 && c) atomicAdd(a.counts + cur_ei, c);
     const unsigned long long tested = warp_sum(n_tested), tails = warp_sum(n_tail), bytes = warp_sum(n_bytes);
@@ -566,6 +810,7 @@ __global__ void __launch_bounds__(kDfsWarps * 32) k_dfs_count(DfsArgs a) {
         atomicAdd(a.stats + 2, tested);
         atomicAdd(a.stats + 3, tails);
         atomicAdd(a.stats + 4, bytes);
+        atomicAdd(a.stats + 7, n_tasks);
     }
 }
 
@@ -645,6 +890,8 @@ struct cgb_handle {
     cgb_config cfg{};
     int device = 0;
     int num_sms = 148;
+    int dfs_occupancy = 0;  // resident DFS blocks per SM
+    uint32_t dfs_epoch = 0; // launch counter used as the task ready tag
     cudaStream_t stream = nullptr;
     bool own_stream = false;
     std::string err;
@@ -685,6 +932,8 @@ struct cgb_handle {
     uint32_t* d_seed = nullptr;  // [0..kMaxQE) lo, [kMaxQE..2kMaxQE+1) pre
     unsigned long long* d_counts = nullptr;  // [kMaxQE]
     unsigned long long* d_stats = nullptr;   // [8]
+    uint32_t* d_tasks = nullptr;             // stolen-range queue
+    unsigned int* d_qctr = nullptr;          // queue counters [8]
     unsigned long long last_stats[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     void* d_temp = nullptr; size_t temp_cap = 0;
 
@@ -993,6 +1242,9 @@ cgb_status cgb_create(const cgb_config* cfg, cgb_handle** out) {
     CKC(cudaMalloc(&h->d_seed, (3 * kMaxQE + 2) * sizeof(uint32_t)));
     CKC(cudaMalloc(&h->d_counts, kMaxQE * sizeof(unsigned long long)));
     CKC(cudaMalloc(&h->d_stats, 8 * sizeof(unsigned long long)));
+    CKC(cudaMalloc(&h->d_tasks, (size_t)kTaskCap * kTaskWords * sizeof(uint32_t)));
+    CKC(cudaMalloc(&h->d_qctr, 8 * sizeof(unsigned int)));
+    CKC(cudaMemset(h->d_tasks, 0, (size_t)kTaskCap * kTaskWords * sizeof(uint32_t)));
     CKC(cudaMalloc(&h->d_qe_dirs, 2 * kMaxQE));
     CKC(cudaMalloc(&h->d_edge_ok, kMaxQE));
     for (auto& ev : h->ev) CKC(cudaEventCreate(&ev));
@@ -1008,7 +1260,7 @@ void cgb_destroy(cgb_handle* h) {
     void* ptrs[] = {h->rec, h->pool, h->pool_alt, h->d_scal, h->d_keys_in, h->d_pending, h->d_edits,
                     h->d_edits_alt, h->d_du, h->d_run_du, h->d_run_len, h->d_run_off, h->d_num_runs,
                     h->d_dkeys, h->d_dkeys_alt, h->d_dval, h->d_ddu, h->d_drun_du, h->d_drun_len, h->d_drun_off,
-                    h->d_seed, h->d_counts, h->d_stats, h->d_temp, h->d_qe_dirs, h->d_edge_ok};
+                    h->d_seed, h->d_counts, h->d_stats, h->d_tasks, h->d_qctr, h->d_temp, h->d_qe_dirs, h->d_edge_ok};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (h->h_scal) cudaFreeHost(h->h_scal);
@@ -1121,6 +1373,7 @@ cgb_status cgb_apply_batch_device(cgb_handle* h, uint32_t dv_count, const uint64
     CK(cudaMemsetAsync(h->d_scal + 2, 0, 2 * sizeof(unsigned long long), h->stream));
     CK(cudaMemsetAsync(h->d_counts, 0, kMaxQE * sizeof(unsigned long long), h->stream));
     CK(cudaMemsetAsync(h->d_stats, 0, 8 * sizeof(unsigned long long), h->stream));
+    CK(cudaMemsetAsync(h->d_qctr, 0, 8 * sizeof(unsigned int), h->stream));
     CK(cudaEventRecord(h->ev[0], h->stream));
 
     // 1. index update: pending delta (add) + ins (add) + del (remove)
@@ -1167,9 +1420,21 @@ cgb_status cgb_apply_batch_device(cgb_handle* h, uint32_t dv_count, const uint64
         da.work_next = (unsigned int*)(h->d_scal + 3);
         da.err = d_err;
         da.stats = h->d_stats;
+        da.tasks = h->d_tasks;
+        da.task_cap = kTaskCap;
+        da.qctr = h->d_qctr;
+        da.epoch = ++h->dfs_epoch ? h->dfs_epoch : ++h->dfs_epoch;
+        da.force_split = (h->cfg.flags & CGB_FLAG_FORCE_SPLIT) ? 1u : 0u;
         da.budget_ns = h->cfg.dfs_budget_ms ? (unsigned long long)h->cfg.dfs_budget_ms * 1000000ull
                                             : 600ull * 1000000000ull;
-        int bps = h->cfg.dfs_blocks_per_sm ? (int)h->cfg.dfs_blocks_per_sm : 8;
+        // persistent grid: exactly the blocks that can be resident at once
+        if (h->dfs_occupancy == 0) {
+            int occ = 0;
+            CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_dfs_count, kDfsWarps * 32, 0));
+            h->dfs_occupancy = std::max(occ, 1);
+        }
+        int bps = h->dfs_occupancy;
+        if (h->cfg.dfs_blocks_per_sm) bps = std::min(bps, (int)h->cfg.dfs_blocks_per_sm);
         k_dfs_count<<<h->num_sms * bps, kDfsWarps * 32, 0, h->stream>>>(da);
         LAUNCHED();
         CK(cudaGetLastError());
@@ -1194,12 +1459,14 @@ cgb_status cgb_apply_batch_device(cgb_handle* h, uint32_t dv_count, const uint64
     cudaEventElapsedTime(&t23, h->ev[2], h->ev[3]);
     cudaEventElapsedTime(&t03, h->ev[0], h->ev[5]);
     h->last_t[0] = t01; h->last_t[1] = t12; h->last_t[2] = t23; h->last_t[3] = t03;
+    for (int i = 0; i < 8; ++i) h->last_stats[i] = h->h_scal[4 + kMaxQE + i];
     if (h->h_scal[2]) {
         h->n_pending = 0;
-        cgb_status st = (h->h_scal[2] & 8u) ? CGB_ERR_TIMEOUT : (h->h_scal[2] & 4u) ? CGB_ERR_OOM : CGB_ERR_ARG;
+        cgb_status st = (h->h_scal[2] & 24u) ? CGB_ERR_TIMEOUT : (h->h_scal[2] & 4u) ? CGB_ERR_OOM : CGB_ERR_ARG;
         return fail(h, st,
                     "batch rejected: error bits %llu (1/2 = key out of range, 4 = pool exhausted, "
-                    "8 = matching exceeded its time budget)", h->h_scal[2]);
+                    "8 = matching exceeded its time budget, 16 = a queued task was never published)",
+                    h->h_scal[2]);
     }
     uint64_t total = 0;
     for (uint32_t e = 0; e < h->q.qe; ++e) { h->last_counts[e] = h->h_scal[4 + e]; total += h->h_scal[4 + e]; }

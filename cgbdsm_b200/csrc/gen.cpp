@@ -222,6 +222,7 @@ int cgbgen_workload(const char* graph_path, const char* update_path, const char*
                     uint64_t seed_graph, uint64_t seed_labels, uint64_t seed_holdout,
                     int qshape, uint32_t qsize, uint32_t max_qedges, uint64_t seed_query,
                     uint32_t* out_qedges) {
+    const bool query_only = graph_path == nullptr;  // graph/stream already written
     Workload W;
     gen_edges(W, n, m, kind, a, b, c, seed_graph);
     gen_labels(W, num_labels, zipf_s, seed_labels);
@@ -241,8 +242,8 @@ int cgbgen_workload(const char* graph_path, const char* update_path, const char*
     for (size_t i = 0; i < W.edges.size(); ++i)
         if (!held[i]) initial.push_back(W.edges[i]);
 
-    if (write_graph(graph_path, W, initial) != 0) return -1;
-    {
+    if (!query_only && write_graph(graph_path, W, initial) != 0) return -1;
+    if (!query_only) {
         FILE* f = std::fopen(update_path, "w");
         if (!f) return -2;
         std::vector<char> buf(1 << 22);

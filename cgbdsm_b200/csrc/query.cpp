@@ -99,10 +99,18 @@ std::string build_query_meta(uint32_t qv, uint32_t qe, const uint32_t* edges, co
 // over its backward edges), then by vertex id.  The tie-breaking criteria
 // restate the reference's global-order rules 1 and 4 (plan.cpp:595-708); the
 // start is the delta edge instead of a global edge because matching is seeded
-// from the delta lists.  Leaves (degree-1 vertices other than ei's endpoints)
-// go last, grouped by label, as the counted tail (the reference's tree
-// Cartesian-product tail, plan.cpp:899-952, which it enumerates); a label
-// group larger than 3 stays in the enumerated core.
+// from the delta lists.
+//
+// Tail: a maximal set of mutually non-adjacent vertices (other than ei's
+// endpoints) whose removal leaves the core connected, chosen by ascending
+// query degree.  All neighbours of a tail vertex are core vertices, so once
+// the core is matched each tail vertex's candidates are one intersection of
+// resolved lists, independent of the other tail vertices except for
+// injectivity: the tail is counted, not enumerated.  This is the reference's
+// Cartesian-product tail (plan.cpp:899-952, enumerated there by
+// cartesian_product.cu:304-427).  Tail vertices are grouped by label (only
+// same-label vertices can collide); groups are limited to 3 members, extra
+// members go back to the core.
 void plan_edges(const QueryMeta& q, const float* avg_deg, EdgePlan* plans, bool analytic_tail) {
     for (uint32_t ei = 0; ei < q.qe; ++ei) {
         EdgePlan& p = plans[ei];
@@ -115,30 +123,85 @@ void plan_edges(const QueryMeta& q, const float* avg_deg, EdgePlan* plans, bool 
         std::vector<int> pos(q.qv, -1);
         pos[a] = 0;
         pos[b] = 1;
-        // tail candidates grouped by label
+        auto lab = [&](uint32_t u) { return q.labels.empty() ? 0u : q.labels[u]; };
         std::vector<uint32_t> tail;
         if (analytic_tail && q.qv > 2) {
-            std::vector<uint32_t> leaves;
+            std::vector<char> in_t(q.qv, 0);
+            std::vector<uint32_t> cand;
             for (uint32_t u = 0; u < q.qv; ++u)
-                if (u != a && u != b && q.nbrs[u].size() == 1) leaves.push_back(u);
-            auto lab = [&](uint32_t u) { return q.labels.empty() ? 0u : q.labels[u]; };
-            std::stable_sort(leaves.begin(), leaves.end(), [&](uint32_t x, uint32_t y) { return lab(x) < lab(y); });
-            for (size_t i = 0; i < leaves.size();) {
+                if (u != a && u != b) cand.push_back(u);
+            std::stable_sort(cand.begin(), cand.end(),
+                             [&](uint32_t x, uint32_t y) { return q.nbrs[x].size() < q.nbrs[y].size(); });
+            auto core_connected = [&]() {
+                std::vector<char> seen(q.qv, 0);
+                std::vector<uint32_t> st{a};
+                seen[a] = 1;
+                uint32_t reached = 1, need = 0;
+                for (uint32_t u = 0; u < q.qv; ++u) need += in_t[u] ? 0 : 1;
+                while (!st.empty()) {
+                    uint32_t u = st.back();
+                    st.pop_back();
+                    for (uint32_t w : q.nbrs[u])
+                        if (!in_t[w] && !seen[w]) { seen[w] = 1; ++reached; st.push_back(w); }
+                }
+                return reached == need;
+            };
+            for (uint32_t u : cand) {
+                bool adj = false;
+                for (uint32_t w : q.nbrs[u]) adj |= in_t[w] != 0;
+                if (adj) continue;
+                in_t[u] = 1;
+                if (!core_connected()) in_t[u] = 0;
+            }
+            for (uint32_t u : cand)
+                if (in_t[u]) tail.push_back(u);
+            std::stable_sort(tail.begin(), tail.end(), [&](uint32_t x, uint32_t y) { return lab(x) < lab(y); });
+            std::vector<uint32_t> kept;
+            for (size_t i = 0; i < tail.size();) {
                 size_t j = i;
-                while (j < leaves.size() && lab(leaves[j]) == lab(leaves[i])) ++j;
-                if (j - i <= 3)
-                    for (size_t k = i; k < j; ++k) tail.push_back(leaves[k]);
+                while (j < tail.size() && lab(tail[j]) == lab(tail[i])) ++j;
+                for (size_t k = i; k < j && k < i + 3; ++k) kept.push_back(tail[k]);
                 i = j;
             }
+            tail.swap(kept);
         }
         std::vector<char> is_tail(q.qv, 0);
         for (uint32_t u : tail) is_tail[u] = 1;
         const uint32_t n_core = q.qv - (uint32_t)tail.size();
+        // last core vertex: the one with the fewest tail neighbours (its
+        // tail lists must be re-scanned per candidate), among those whose
+        // removal keeps the rest of the core connected
+        int last = -1;
+        if (n_core > 2) {
+            int best_t = 1 << 30, best_c = -1;
+            for (uint32_t u = 0; u < q.qv; ++u) {
+                if (is_tail[u] || u == a || u == b) continue;
+                std::vector<char> seen(q.qv, 0);
+                std::vector<uint32_t> st{a};
+                seen[a] = 1;
+                uint32_t reached = 1;
+                while (!st.empty()) {
+                    uint32_t x = st.back();
+                    st.pop_back();
+                    for (uint32_t w : q.nbrs[x])
+                        if (!is_tail[w] && w != u && !seen[w]) { seen[w] = 1; ++reached; st.push_back(w); }
+                }
+                if (reached != n_core - 1) continue;
+                int nt = 0, ncn = 0;
+                for (uint32_t w : q.nbrs[u]) { nt += is_tail[w] ? 1 : 0; ncn += is_tail[w] ? 0 : 1; }
+                if (nt < best_t || (nt == best_t && ncn > best_c)) { best_t = nt; best_c = ncn; last = (int)u; }
+            }
+        }
         for (uint32_t j = 2; j < n_core; ++j) {
+            if (last >= 0 && j == n_core - 1) {
+                pos[last] = (int)j;
+                p.vs[j] = (uint8_t)last;
+                break;
+            }
             int best = -1, best_bn = -1;
             float best_est = 0.f;
             for (uint32_t u = 0; u < q.qv; ++u) {
-                if (pos[u] >= 0 || is_tail[u]) continue;
+                if (pos[u] >= 0 || is_tail[u] || (int)u == last) continue;
                 int nbn = 0;
                 float est = 3.4e38f;
                 for (uint32_t w : q.nbrs[u])
@@ -153,7 +216,7 @@ void plan_edges(const QueryMeta& q, const float* avg_deg, EdgePlan* plans, bool 
                     best_est = est;
                 }
             }
-            pos[best] = (int)j;  // connected query: some core vertex is adjacent to the visited set
+            pos[best] = (int)j;  // the core minus `last` is connected, so some vertex is adjacent
             p.vs[j] = (uint8_t)best;
         }
         p.n_core = (uint8_t)n_core;
@@ -163,8 +226,7 @@ void plan_edges(const QueryMeta& q, const float* avg_deg, EdgePlan* plans, bool 
             const uint32_t j = n_core + (uint32_t)i;
             p.vs[j] = (uint8_t)tail[i];
             pos[tail[i]] = (int)j;
-            if (i > 0 && (q.labels.empty() ? 0u : q.labels[tail[i]]) != (q.labels.empty() ? 0u : q.labels[tail[i - 1]]))
-                ++gid;
+            if (i > 0 && lab(tail[i]) != lab(tail[i - 1])) ++gid;
             p.tail_gid[j] = gid;
         }
         uint32_t k = 0;

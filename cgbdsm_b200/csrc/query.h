@@ -30,12 +30,13 @@ struct QueryMeta {
 // constrain it.  bn_dvis marks BN directions whose delta part is visible to
 // ei (dir_to_edge < ei; enumeration.cu:937, cpu_dfs.cpp:76-77).
 //
-// Positions [n_core, n) form the tail: degree-1 query vertices (leaves) whose
-// single backward neighbour is a core vertex.  Their count is computed
-// instead of enumerated: per label group (tail_gid, contiguous) of k <= 3
-// leaves, the number of injective assignments of the group to its candidate
-// lists minus the matched core vertices, by inclusion-exclusion.  Leaves of
-// different labels have disjoint candidate lists, so groups multiply.
+// Positions [n_core, n) form the tail: mutually non-adjacent vertices whose
+// neighbours are all core vertices (so every neighbour is a backward
+// neighbour).  Their count is computed instead of enumerated: per label group
+// (tail_gid, contiguous) of k <= 3 vertices, the number of injective
+// assignments of the group to its candidate sets (intersections of resolved
+// lists) minus the matched core vertices, by inclusion-exclusion.  Vertices of
+// different labels have disjoint candidate sets, so groups multiply.
 struct EdgePlan {
     uint8_t n;
     uint8_t n_core;

@@ -43,6 +43,7 @@ class Config(ctypes.Structure):
 
 FLAG_NO_MERGE_BACK_DEFER = 0x1
 FLAG_ENUMERATE_TAIL = 0x2
+FLAG_FORCE_SPLIT = 0x4
 
 
 class BatchKeys(ctypes.Structure):
@@ -206,7 +207,8 @@ class Engine:
         out = np.zeros(8, dtype=np.uint64)
         self._check(self.lib.cgb_last_stats(self.h, out.ctypes.data))
         return {"seeds": int(out[0]), "chunks": int(out[1]), "tested": int(out[2]), "tails": int(out[3]),
-                "match_bytes": int(out[4]), "update_bytes": int(out[5]), "touched_runs": int(out[6])}
+                "match_bytes": int(out[4]), "update_bytes": int(out[5]), "touched_runs": int(out[6]),
+                "stolen_tasks": int(out[7])}
 
     def stream(self) -> int:
         return int(self.lib.cgb_stream(self.h) or 0)

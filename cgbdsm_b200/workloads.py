@@ -103,6 +103,18 @@ def materialize(spec: WorkloadSpec, directory: str) -> dict[str, str]:
     return paths
 
 
+def materialize_query(spec: WorkloadSpec, path: str, seed_query: int) -> int:
+    """Writes only the query pattern of spec with another query seed (graph
+    and stream are regenerated in memory, not written).  Returns its edge count."""
+    qe = ctypes.c_uint32(0)
+    rc = _gen()(None, None, path.encode(), spec.kind, spec.n, spec.m, 0.57, 0.19, 0.19, spec.labels, spec.zipf,
+                spec.holdout, spec.seed_graph, spec.seed_labels, spec.seed_holdout, spec.qshape, spec.qsize,
+                spec.max_qedges, seed_query, ctypes.byref(qe))
+    if rc != 0:
+        raise RuntimeError(f"query generation failed: rc={rc}")
+    return qe.value
+
+
 def read_query(path: str) -> tuple[list[int], list[tuple[int, int]]]:
     labels: dict[int, int] = {}
     edges: list[tuple[int, int]] = []

@@ -51,7 +51,8 @@ typedef struct {
 } cgb_config;
 
 #define CGB_FLAG_NO_MERGE_BACK_DEFER 0x1u /* apply the delta merge-back eagerly after matching */
-#define CGB_FLAG_ENUMERATE_TAIL 0x2u      /* enumerate degree-1 tail vertices instead of counting them */
+#define CGB_FLAG_ENUMERATE_TAIL 0x2u      /* enumerate the independent tail instead of counting it */
+#define CGB_FLAG_FORCE_SPLIT 0x4u         /* share every long shallow DFS range through the work queue */
 
 /* Limits (reference: utils/config.h:5-6; key layout calig_helper_gamma.cu:228-229). */
 #define CGB_MAX_QV 12

@@ -10,20 +10,21 @@ import numpy as np
 import pytest
 
 from cgbdsm_b200 import CgbError, Engine
-from cgbdsm_b200.engine import FLAG_ENUMERATE_TAIL
+from cgbdsm_b200.engine import FLAG_ENUMERATE_TAIL, FLAG_FORCE_SPLIT
 from cgbdsm_b200.workloads import SPECS, materialize, read_query
 from oracle import bind
 
 pytestmark = pytest.mark.gpu
 
-PIPELINE_CASES = ["t_tiny", "t_er5", "t_er6", "t_er_sparse", "t_er_tree"]
+PIPELINE_CASES = ["t_tiny", "t_er5", "t_er6", "t_er_sparse", "t_er_tree", "t_rmat"]
 
 
 def _key(d, u, v):
     return (np.uint64(d) << np.uint64(59)) | (np.uint64(u) << np.uint64(32)) | np.uint64(v)
 
 
-@pytest.mark.parametrize("flags", [0, FLAG_ENUMERATE_TAIL], ids=["counted_tail", "enumerated_tail"])
+@pytest.mark.parametrize("flags", [0, FLAG_ENUMERATE_TAIL, FLAG_FORCE_SPLIT | FLAG_ENUMERATE_TAIL, FLAG_FORCE_SPLIT],
+                         ids=["counted_tail", "enumerated_tail", "stolen_enumerated", "stolen_counted"])
 @pytest.mark.parametrize("name", PIPELINE_CASES)
 def test_engine_matches_reference_cpu_path(name, flags, workdir):
     if not bind.have_ref():
@@ -73,25 +74,31 @@ def _sym_keys(orc, pairs_by_edge):
     return np.array(ks, dtype=np.uint64) if ks else np.zeros(0, np.uint64)
 
 
-@pytest.mark.parametrize("seed", range(6))
+@pytest.mark.parametrize("seed", range(8))
 def test_random_symmetric_streams(seed):
     rng = np.random.default_rng(1000 + seed)
     qv = int(rng.integers(3, 7))
     qedges = _random_query(rng, qv, int(rng.integers(0, 4)))
     dv0 = 60
-    eng = Engine()
+    eng = Engine(flags=FLAG_FORCE_SPLIT if seed % 2 else 0)
     eng.load_query(qv, qedges)
     orc = bind.Oracle(qv, qedges)
 
     def rand_pairs(n, dv):
+        # a third of the pairs touch vertex 0 or 1, so some lists are long
+        # enough (> 96) for the DFS to split them through the work queue
         out = []
         for _ in range(n):
             a, b = qedges[int(rng.integers(0, len(qedges)))]
             x, y = rng.choice(dv, 2, replace=False)
+            if rng.random() < 0.33:
+                x = int(rng.integers(0, 2))
+                if y == x:
+                    y = 2
             out.append((a, b, int(x), int(y)))
         return out
 
-    init = np.unique(_sym_keys(orc, rand_pairs(900, dv0)))
+    init = np.unique(_sym_keys(orc, rand_pairs(2500, dv0)))
     eng.build_index(init, dv0)
     orc.build(init, dv0)
     dv = dv0
@@ -156,3 +163,26 @@ def test_edge_cases():
     with pytest.raises(CgbError):
         eng.apply_batch(4, np.zeros(0, np.uint64), np.zeros(0, np.uint64), np.zeros(0, np.uint64))
     eng.close()
+
+
+@pytest.mark.parametrize("name", ["t_er5", "t_er_sparse"])
+def test_cli_drop_in_total(name, workdir):
+    """The drop-in CLI prints the reference's `Num Positive Matches` total."""
+    import os
+    import re
+    import subprocess
+
+    if not bind.have_ref():
+        pytest.skip("oracle/_ref/libcgbref.so not built")
+    spec = SPECS[name]
+    p = materialize(spec, workdir)
+    exe = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "cgbdsm_b200", "cgbdsm")
+    out = subprocess.run([exe, p["query"], p["data"], p["update"], "0", str(spec.cli_batch_size)],
+                         capture_output=True, text=True, timeout=300)
+    assert out.returncode == 0, out.stderr
+    got = int(re.search(r"Num Positive Matches: (\d+)", out.stdout).group(1))
+    ref = bind.RefPipeline(p["query"], p["data"], p["update"], spec.cli_batch_size)
+    while ref.step() >= 0:
+        pass
+    assert got == ref.L.cgbref_total_count(ref.h)
+    ref.close()
