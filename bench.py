@@ -15,8 +15,10 @@ restarts, so every cycle sees identical work.
 Stage 1 (the CaLiG producer that makes the keys) runs before timing.
 
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-For N > 1 run under torchrun; every rank is an independent replica of the
-engine on its own GPU (replicas; scaling "weak").
+For N > 1 run under torchrun: every rank keeps a full index replica and
+applies every batch; the matching of each batch is split by seed (rank r
+expands delta edges i with i % N == r); counts are summed and step times
+maxed over ranks (NCCL).  Total work per batch is fixed: scaling "strong".
 """
 from __future__ import annotations
 
@@ -99,17 +101,24 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(rows)}
 
 
+def log(msg: str) -> None:
+    print(f"[bench {time.strftime('%H:%M:%S')}] {msg}", file=sys.stderr, flush=True)
+
+
 def setup_workload(rank: int):
     from cgbdsm_b200 import Producer
     from cgbdsm_b200.workloads import SPECS, materialize, read_query
 
     spec = SPECS[WORKLOAD]
+    log(f"generating workload {spec.name}")
     paths = materialize(spec, os.environ.get("CGB_BENCH_DIR", f"/tmp/cgb_bench_r{rank}"))
+    log("stage 1 (CaLiG producer) for every batch")
     t0 = time.perf_counter()
     prod = Producer(paths["query"], paths["data"], paths["update"], spec.cli_batch_size)
     init, dv0 = prod.initial()
     batches = [prod.next() for _ in range(prod.num_batches)]
     s1_s = time.perf_counter() - t0
+    log(f"stage 1 done in {s1_s:.1f} s: {len(init)} initial keys, {len(batches)} batches")
     ql, qe = read_query(paths["query"])
     prod.close()
     return spec, paths, ql, qe, init, dv0, batches, s1_s
@@ -117,24 +126,18 @@ def setup_workload(rank: int):
 
 def run_ours(args) -> None:
     import torch
-    import torch.distributed as dist
 
-    from cgbdsm_b200 import Engine
+    from cgbdsm_b200 import Engine, dist
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    rank, world, local = dist.env()
     torch.cuda.set_device(local)
-    if world > 1:
-        import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
-                                device_id=torch.device("cuda", local))
+    dist.init("nccl", timeout_s=600)
 
     spec, paths, ql, qe, init, dv0, batches, s1_s = setup_workload(rank)
     nb = len(batches)
 
     def new_engine():
-        e = Engine(device=local, dfs_budget_ms=args.budget_ms)
+        e = Engine(device=local, dfs_budget_ms=args.budget_ms, shard_index=rank, num_shards=world)
         e.load_query(len(ql), qe, ql)
         e.build_index(init, dv0)
         return e
@@ -175,51 +178,42 @@ def run_ours(args) -> None:
         st = e.stats()
         st["launches"] = e.kernel_launches() - l0
         state["pos"] += 1
+        log(f"batch {b} ({'device' if device_keys else 'host'} keys): {ms:.1f} ms, count {c}, "
+            f"phases {[round(float(x), 2) for x in tm[:3]]}")
         return b, c, ms, tm, st
 
     for _ in range(args.warmup):
         one_step(True)
-    if world > 1:
-        dist.barrier()
+    dist.barrier()
     torch.cuda.synchronize()
     recs = []
     with ClockSampler(local) as clk:
         for _ in range(args.steps):
             recs.append(one_step(True))
     torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
+    dist.barrier()
     launches = sum(r[4]["launches"] for r in recs)
 
-    total_ms = sum(r[2] for r in recs)
-    edges = sum(batches[r[0]]["num_edges"] for r in recs)
-    matches = sum(r[1] for r in recs)
-    if world > 1:
-        tt = torch.tensor([total_ms], dtype=torch.float64, device=f"cuda:{local}")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        total_ms = float(tt.item())
-        ed = torch.tensor([edges, matches], dtype=torch.float64, device=f"cuda:{local}")
-        dist.all_reduce(ed, op=dist.ReduceOp.SUM)
-        edges, matches = float(ed[0].item()), float(ed[1].item())
+    step_ms = dist.max_values([r[2] for r in recs])          # max over ranks, per step
+    counts = dist.sum_counts([int(r[1]) for r in recs])       # shard counts summed, per step
+    total_ms = sum(step_ms)
+    edges = sum(batches[r[0]]["num_edges"] for r in recs)     # every rank sees the same batches
+    matches = sum(counts)
 
     # e2e through the host-buffer C-ABI call (same batches, same cycle)
     state["eng"].close()
     state["eng"] = new_engine()
     state["pos"] = 0
-    for _ in range(args.warmup):
-        one_step(False)
-    e2e_recs = [one_step(False) for _ in range(args.steps)]
-    e2e_ms = sum(r[2] for r in e2e_recs)
+    if args.quick:
+        e2e_recs = recs
+    else:
+        for _ in range(args.warmup):
+            one_step(False)
+        e2e_recs = [one_step(False) for _ in range(args.steps)]
+    e2e_ms = sum(dist.max_values([r[2] for r in e2e_recs]))
     e2e_edges = sum(batches[r[0]]["num_edges"] for r in e2e_recs)
-    h2d = sum(8 * (len(batches[r[0]]["ins"]) + len(batches[r[0]]["del"]) + len(batches[r[0]]["delta"])
-                   + len(batches[r[0]]["edge_ok"]) // 8) for r in e2e_recs) / len(e2e_recs)
-    if world > 1:
-        t2 = torch.tensor([e2e_ms], dtype=torch.float64, device=f"cuda:{local}")
-        dist.all_reduce(t2, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t2.item())
-        e2 = torch.tensor([e2e_edges], dtype=torch.float64, device=f"cuda:{local}")
-        dist.all_reduce(e2, op=dist.ReduceOp.SUM)
-        e2e_edges = float(e2.item())
+    h2d = sum(8 * (len(batches[r[0]]["ins"]) + len(batches[r[0]]["del"]) + len(batches[r[0]]["delta"]))
+              + len(batches[r[0]]["edge_ok"]) for r in e2e_recs) / len(e2e_recs)
 
     # roofline of the dominant kernel (by time over the timed steps)
     match_ms = sum(float(r[3][2]) for r in recs)
@@ -232,7 +226,8 @@ def run_ours(args) -> None:
     else:
         kname, kbytes, kms = "k_merge_runs (index update)", upd_bytes, upd_ms
     achieved = (kbytes / 1e9) / (kms / 1e3) if kms > 0 else 0.0
-    lat = sorted(r[2] for r in recs)
+    upd_achieved = (upd_bytes / 1e9) / (upd_ms / 1e3) if upd_ms > 0 else 0.0
+    lat = sorted(step_ms)
 
     def pct(p):
         return lat[min(len(lat) - 1, int(round(p / 100.0 * (len(lat) - 1))))]
@@ -243,62 +238,70 @@ def run_ours(args) -> None:
         "unit": "edge updates/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": total_ms / max(1, len(recs)),
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
         "dtype": "u32/u64 integer", "data": "synthetic (seeded R-MAT stand-in for the public graphs)",
         "config": {"workload": "R-MAT 1,000,000 vertices / 10,000,000 edges, 16 labels Zipf(1.2), "
                                "1,000,000 insertions in batches of 100,000, 9-vertex dense pattern",
                    "batch_edges": spec.batch_edges, "batches_in_stream": nb,
                    "query_vertices": len(ql), "query_edges": len(qe),
-                   "l2": "flushed between steps (256 MiB write)", "parallelism": f"replicas x{world}"},
+                   "l2": "flushed between steps (256 MiB write)",
+                   "parallelism": f"{world} GPU(s): index replicated, seeds sharded"},
         "matches_per_s": matches / (total_ms / 1e3) if total_ms > 0 else 0.0,
+        "matches_per_batch": matches / max(1, len(recs)),
         "latency_ms": {"p50": pct(50), "p99": pct(99), "max": lat[-1]},
         "phase_ms_per_step": {"index_update": upd_ms / len(recs),
                               "delta_lists": sum(float(r[3][1]) for r in recs) / len(recs),
                               "matching": match_ms / len(recs)},
+        "work_per_step": {k: sum(r[4][k] for r in recs) / len(recs)
+                          for k in ("seeds", "chunks", "tested", "tails", "stolen_tasks", "touched_runs")},
         "e2e": {"value": e2e_edges / (e2e_ms / 1e3) if e2e_ms > 0 else 0.0, "unit": "edge updates/s",
                 "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": 8 * (4 + 16 + 8)},
         "gpu_launches": launches,
         "roofline": {"kernel": kname, "bound": "hbm", "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak if peak else None, "peak_source": peak_kind,
-                     "algorithmic_bytes_per_step": kbytes / len(recs), "traffic": None},
+                     "algorithmic_bytes_per_step": kbytes / len(recs), "traffic": None,
+                     "index_update_achieved_gbs": upd_achieved},
         "clocks": clk.summary(),
         "stage1_setup_s": round(s1_s, 2),
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        log("cpu baseline: reference CPU path on batch 0")
         line["cpu_baseline"] = reference_sample(paths, spec, args.cpu_budget_s, batches)
     if rank == 0:
         print(json.dumps(line), flush=True)
     state["eng"].close()
-    if world > 1:
-        dist.destroy_process_group()
+    dist.finish()
 
 
 def reference_sample(paths, spec, budget_s: float, batches=None) -> dict:
     """The reference's own CPU path (oracle/_ref: CaLiG + staging + CPUIndexMirror +
-    cpu_dfs) on batch 0 of the same stream, all host threads.  Stage 1 and the
-    index update run fully; the mask-free count is run for budget_s and
-    extrapolated by rows counted / rows total."""
+    cpu_dfs) on batch 0 of the same stream with all host threads.  Stage 1,
+    staging and the index mirror update run fully; the count (the reference
+    enumerates every embedding, mask-free seeding) runs for budget_s in a
+    supervised child process and is extrapolated by rows counted / rows total.
+    When not one row finishes in the budget, the count time is bounded below by
+    budget_s x rows_total and the value is an upper bound."""
     from oracle import bind
 
     threads = os.cpu_count() or 1
-    ref = bind.RefPipeline(paths["query"], paths["data"], paths["update"], spec.cli_batch_size, threads=threads)
-    ref.set_parallel_dfs(True)
-    ref.set_sample_budget(budget_s * 1e3)
-    t0 = time.perf_counter()
-    ref.step()
-    wall = time.perf_counter() - t0
-    r = ref.last()
-    done, total, ms = ref.last_sample()
-    tm = r["times_ms"]
-    count_ms = ms * (total / done) if done else float("inf")
-    batch_ms = tm["s1"] + tm["staging"] + tm["mirror"] + count_ms
-    ref.close()
-    return {"value": spec.batch_edges / (batch_ms / 1e3) if batch_ms > 0 else 0.0, "unit": "edge updates/s",
-            "cores": threads, "kind": "reference",
-            "sample": (f"batch 0 of the stream: Stage 1 {tm['s1']:.0f} ms + staging {tm['staging']:.0f} ms + "
-                       f"index mirror {tm['mirror']:.0f} ms measured; mask-free cpu_dfs count over {done} of "
-                       f"{total} seed rows in {ms/1e3:.1f} s, extrapolated to {count_ms/1e3:.1f} s"),
-            "stage1_ms": tm["s1"], "wall_s": round(wall, 1)}
+    r = bind.supervised_reference_batch(paths["query"], paths["data"], paths["update"], spec.cli_batch_size,
+                                        threads, budget_s)
+    fixed_ms = r["s1_ms"] + r["staging_ms"] + r["mirror_ms"]
+    if r["finished"]:
+        count_ms, kind = r["count_ms"], "measured"
+    elif r["rows_done"] > 0:
+        count_ms, kind = r["count_ms"] * r["rows_total"] / r["rows_done"], "extrapolated"
+    else:
+        count_ms, kind = r["count_ms"] * max(1, r["rows_total"]), "lower bound (no row finished)"
+    batch_ms = fixed_ms + count_ms
+    value = spec.batch_edges / (batch_ms / 1e3) if batch_ms > 0 else 0.0
+    return {"value": value, "unit": "edge updates/s", "cores": threads, "kind": "reference",
+            "sample": (f"batch 0 of the stream: Stage 1 {r['s1_ms']:.0f} ms + staging {r['staging_ms']:.0f} ms + "
+                       f"index mirror {r['mirror_ms']:.0f} ms measured; mask-free cpu_dfs count: "
+                       f"{r['rows_done']} of {r['rows_total']} seed rows in {r['count_ms']/1e3:.1f} s, "
+                       f"count time {kind}: {count_ms/1e3:.3g} s"
+                       + ("; value is an upper bound" if kind.startswith("lower") else "")),
+            "stage1_ms": r["s1_ms"], "count_time_kind": kind, "wall_s": round(r["wall_s"], 1)}
 
 
 def run_reference(args) -> None:
@@ -317,7 +320,7 @@ def run_reference(args) -> None:
         return
     vals = []
     cb = None
-    per_step_budget = max(2.0, min(args.cpu_budget_s, 120.0 / max(1, args.steps + args.warmup)))
+    per_step_budget = max(2.0, min(args.cpu_budget_s, 150.0 / max(1, args.steps + args.warmup)))
     for i in range(args.warmup + args.steps):
         cb = reference_sample(paths, spec, per_step_budget)
         if i >= args.warmup:
@@ -346,8 +349,12 @@ def main():
     ap.add_argument("--budget-ms", type=int, default=120000, help="matching time budget per batch")
     ap.add_argument("--cpu-budget-s", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--quick", action="store_true",
+                    help="profiling run: 1 warm-up + 1 step, no e2e leg, no CPU baseline (not a benchmark)")
     args = ap.parse_args()
-    if args.warmup < 3:
+    if args.quick:
+        args.steps, args.warmup, args.no_cpu_baseline = 1, 1, True
+    elif args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
         run_reference(args)

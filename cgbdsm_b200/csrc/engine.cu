@@ -301,6 +301,9 @@ struct DfsArgs {
     unsigned int* qctr;          // [8]: tail, head, created, completed, hungry, -, seeds issued
     uint32_t epoch;              // per-launch tag written as a task's ready flag (never 0)
     uint32_t force_split;        // split every long shallow range, hungry warps or not (tests)
+    uint32_t shard, num_shards;  // this engine expands seeds i with i % num_shards == shard
+    uint32_t steal;              // share long shallow ranges through the queue
+    uint32_t tail_cache;         // count prefix-only tail subsets once per prefix
 };
 
 __device__ __forceinline__ unsigned long long global_ns() {
@@ -551,7 +554,9 @@ __global__ void __launch_bounds__(kDfsWarps * 32) k_dfs_count(DfsArgs a) {
     if (threadIdx.x <= a.qe) s_pre[threadIdx.x] = a.seed_pre[threadIdx.x];
     if (threadIdx.x < a.qe) s_lo[threadIdx.x] = a.seed_lo[threadIdx.x];
     __syncthreads();
-    const uint32_t total = s_pre[a.qe];
+    // seeds of this shard: global seed i = shard + local * num_shards
+    const uint32_t all_seeds = s_pre[a.qe];
+    const uint32_t total = all_seeds > a.shard ? (all_seeds - a.shard + a.num_shards - 1) / a.num_shards : 0;
     const uint64_t vmask = (1ull << a.B) - 1ull;
     uint32_t* m = s_m[w];
     uint4* bn = s_bn[w];
@@ -567,6 +572,7 @@ __global__ void __launch_bounds__(kDfsWarps * 32) k_dfs_count(DfsArgs a) {
     uint32_t steps = 0;
     bool out_of_time = false;
     bool hungry = false;
+    bool tail_ready = false;
     uint32_t idle_spins = 0;
 
     for (;;) {
@@ -614,6 +620,7 @@ __global__ void __launch_bounds__(kDfsWarps * 32) k_dfs_count(DfsArgs a) {
         int ei = 0;
         uint32_t jbase = 2, tgen = 0, tlo = 0, thi = 0;
         if (kind == 1) {
+            item = a.shard + item * a.num_shards;
             while (ei + 1 < (int)a.qe && s_pre[ei + 1] <= item) ++ei;
             const uint64_t key = a.dkeys[s_lo[ei] + (item - s_pre[ei])];
             if (lane == 0) {
@@ -688,8 +695,7 @@ __global__ void __launch_bounds__(kDfsWarps * 32) k_dfs_count(DfsArgs a) {
             }
             if (lane == j) { st_ncand = 0; st_pos = 0; st_next = 0; st_len = nb ? best : 0; st_gen = bl; }
             __syncwarp();
-            if (has_tail && j == nc - 1 && nb && best)
-                tail_prepare(P, m, bn, s_tc[w], a.rec, a.dvcap, a.pool, a.dval, lane, n_bytes);
+            if (j == nc - 1) tail_ready = false;  // prefix changed: cached tail counts are stale
         };
 
         setup(jbase);
@@ -718,7 +724,7 @@ __global__ void __launch_bounds__(kDfsWarps * 32) k_dfs_count(DfsArgs a) {
             if (gnext < glen) {
                 const uint32_t g = __shfl_sync(kFull, st_gen, j);
                 // share the rest of a long shallow range with hungry warps
-                if (j <= kSplitMaxDepth && glen - gnext >= kSplitMinRemaining) {
+                if (a.steal && j <= kSplitMaxDepth && glen - gnext >= kSplitMinRemaining) {
                     uint32_t slot = 0xffffffffu;
                     if (lane == 0 && (vq[4] > 0 || a.force_split)) {
                         const unsigned int t = vq[0];
@@ -772,10 +778,17 @@ __global__ void __launch_bounds__(kDfsWarps * 32) k_dfs_count(DfsArgs a) {
                             const int l = __ffs(bal) - 1;
                             bal &= bal - 1;
                             const uint32_t cl = __shfl_sync(kFull, c, l);
+                            if (!tail_ready && a.tail_cache) {
+                                // first embedding of this prefix: count the prefix-only subsets once
+                                tail_prepare(P, m, bn, s_tc[w], a.rec, a.dvcap, a.pool, a.dval, lane, n_bytes);
+                                tail_ready = true;
+                            }
                             if (lane == 0) m[j] = cl;
                             __syncwarp();
                             const unsigned long long tc =
-                                tail_eval(P, m, bn, s_tc[w], a.rec, a.dvcap, a.pool, a.dval, lane, n_bytes);
+                                a.tail_cache
+                                    ? tail_eval(P, m, bn, s_tc[w], a.rec, a.dvcap, a.pool, a.dval, lane, n_bytes)
+                                    : tail_count_warp(P, m, bn, a.rec, a.dvcap, a.pool, a.dval, lane, n_bytes);
                             if (lane == 0) { cnt += tc; ++n_tail; }
                             __syncwarp();
                         }
@@ -1325,7 +1338,8 @@ cgb_status cgb_build_index(cgb_handle* h, const uint64_t* keys, uint64_t n, uint
     }
     float avg[kMaxDir] = {0};
     for (uint32_t d = 0; d < h->nd; ++d) avg[d] = nodes[d] ? (float)card[d] / (float)nodes[d] : 0.f;
-    cgb::plan_edges(h->q, avg, h->plans, !(h->cfg.flags & CGB_FLAG_ENUMERATE_TAIL));
+    cgb::plan_edges(h->q, avg, h->plans, !(h->cfg.flags & CGB_FLAG_ENUMERATE_TAIL),
+                    !(h->cfg.flags & CGB_FLAG_PLAIN_CORE_ORDER));
     CK(cudaMemcpyToSymbol(c_plan, h->plans, sizeof(EdgePlan) * kMaxQE));
 
     h->dv = dv_count;
@@ -1425,6 +1439,10 @@ cgb_status cgb_apply_batch_device(cgb_handle* h, uint32_t dv_count, const uint64
         da.qctr = h->d_qctr;
         da.epoch = ++h->dfs_epoch ? h->dfs_epoch : ++h->dfs_epoch;
         da.force_split = (h->cfg.flags & CGB_FLAG_FORCE_SPLIT) ? 1u : 0u;
+        da.num_shards = h->cfg.num_shards ? h->cfg.num_shards : 1u;
+        da.steal = (h->cfg.flags & CGB_FLAG_NO_STEAL) ? 0u : 1u;
+        da.tail_cache = (h->cfg.flags & CGB_FLAG_NO_TAIL_CACHE) ? 0u : 1u;
+        da.shard = h->cfg.shard_index < da.num_shards ? h->cfg.shard_index : 0u;
         da.budget_ns = h->cfg.dfs_budget_ms ? (unsigned long long)h->cfg.dfs_budget_ms * 1000000ull
                                             : 600ull * 1000000000ull;
         // persistent grid: exactly the blocks that can be resident at once

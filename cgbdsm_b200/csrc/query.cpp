@@ -111,7 +111,7 @@ std::string build_query_meta(uint32_t qv, uint32_t qe, const uint32_t* edges, co
 // cartesian_product.cu:304-427).  Tail vertices are grouped by label (only
 // same-label vertices can collide); groups are limited to 3 members, extra
 // members go back to the core.
-void plan_edges(const QueryMeta& q, const float* avg_deg, EdgePlan* plans, bool analytic_tail) {
+void plan_edges(const QueryMeta& q, const float* avg_deg, EdgePlan* plans, bool analytic_tail, bool pick_last) {
     for (uint32_t ei = 0; ei < q.qe; ++ei) {
         EdgePlan& p = plans[ei];
         std::memset(&p, 0, sizeof(p));
@@ -172,7 +172,7 @@ void plan_edges(const QueryMeta& q, const float* avg_deg, EdgePlan* plans, bool 
         // tail lists must be re-scanned per candidate), among those whose
         // removal keeps the rest of the core connected
         int last = -1;
-        if (n_core > 2) {
+        if (pick_last && n_core > 2) {
             int best_t = 1 << 30, best_c = -1;
             for (uint32_t u = 0; u < q.qv; ++u) {
                 if (is_tail[u] || u == a || u == b) continue;
@@ -215,6 +215,10 @@ void plan_edges(const QueryMeta& q, const float* avg_deg, EdgePlan* plans, bool 
                     best_bn = nbn;
                     best_est = est;
                 }
+            }
+            if (best < 0) {  // cannot happen for a connected core; fall back to any remaining vertex
+                for (uint32_t u = 0; u < q.qv; ++u)
+                    if (pos[u] < 0 && !is_tail[u] && (int)u != last) { best = (int)u; break; }
             }
             pos[best] = (int)j;  // the core minus `last` is connected, so some vertex is adjacent
             p.vs[j] = (uint8_t)best;

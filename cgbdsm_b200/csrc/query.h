@@ -57,6 +57,8 @@ std::string parse_query_file(const std::string& path, std::vector<uint32_t>& lab
                              std::vector<uint32_t>& edges, uint32_t& qv);
 // avg_deg[dir]: mean run length of direction dir in the initial index.
 // analytic_tail = false keeps every vertex in the enumerated core.
-void plan_edges(const QueryMeta& q, const float* avg_deg, EdgePlan* plans, bool analytic_tail = true);
+// pick_last = true puts the core vertex with the fewest tail neighbours last.
+void plan_edges(const QueryMeta& q, const float* avg_deg, EdgePlan* plans, bool analytic_tail = true,
+                bool pick_last = true);
 
 }  // namespace cgb

@@ -38,12 +38,15 @@ class CgbError(RuntimeError):
 
 class Config(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int), ("pool_words", _u64), ("dfs_blocks_per_sm", _u32),
-                ("flags", _u32), ("dfs_budget_ms", _u32)]
+                ("flags", _u32), ("dfs_budget_ms", _u32), ("shard_index", _u32), ("num_shards", _u32)]
 
 
 FLAG_NO_MERGE_BACK_DEFER = 0x1
 FLAG_ENUMERATE_TAIL = 0x2
 FLAG_FORCE_SPLIT = 0x4
+FLAG_NO_STEAL = 0x8
+FLAG_NO_TAIL_CACHE = 0x10
+FLAG_PLAIN_CORE_ORDER = 0x20
 
 
 class BatchKeys(ctypes.Structure):
@@ -113,9 +116,9 @@ class Engine:
     """One engine instance on one CUDA device (C ABI handle)."""
 
     def __init__(self, device: int = 0, pool_words: int = 0, dfs_blocks_per_sm: int = 0, flags: int = 0,
-                 dfs_budget_ms: int = 0):
+                 dfs_budget_ms: int = 0, shard_index: int = 0, num_shards: int = 1):
         self.lib = load_library()
-        cfg = Config(device, pool_words, dfs_blocks_per_sm, flags, dfs_budget_ms)
+        cfg = Config(device, pool_words, dfs_blocks_per_sm, flags, dfs_budget_ms, shard_index, num_shards)
         h = _vp()
         st = self.lib.cgb_create(ctypes.byref(cfg), ctypes.byref(h))
         self.h = h.value

@@ -48,11 +48,18 @@ typedef struct {
     uint32_t flags;          /* CGB_FLAG_* below                                           */
     uint32_t dfs_budget_ms;  /* wall-clock budget of one matching launch; past it the batch
                                 fails with CGB_ERR_TIMEOUT (count incomplete); 0 = 600 s   */
+    uint32_t shard_index;    /* multi-GPU: this engine matches the seeds (delta edges) i with */
+    uint32_t num_shards;     /* i % num_shards == shard_index; 0 or 1 = all seeds.  Every    */
+                             /* shard applies every batch to its own full index replica; the */
+                             /* batch count is the sum of the shards' counts.                */
 } cgb_config;
 
 #define CGB_FLAG_NO_MERGE_BACK_DEFER 0x1u /* apply the delta merge-back eagerly after matching */
 #define CGB_FLAG_ENUMERATE_TAIL 0x2u      /* enumerate the independent tail instead of counting it */
 #define CGB_FLAG_FORCE_SPLIT 0x4u         /* share every long shallow DFS range through the work queue */
+#define CGB_FLAG_NO_STEAL 0x8u            /* never share DFS ranges (one warp per seed)                 */
+#define CGB_FLAG_NO_TAIL_CACHE 0x10u      /* recount every tail subset for every core embedding        */
+#define CGB_FLAG_PLAIN_CORE_ORDER 0x20u   /* greedy core order only (no choice of the last core vertex) */
 
 /* Limits (reference: utils/config.h:5-6; key layout calig_helper_gamma.cu:228-229). */
 #define CGB_MAX_QV 12

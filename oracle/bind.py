@@ -80,6 +80,7 @@ class RefPipeline:
         L.cgbref_li.argtypes = [_vp, _vp, _u64]
         L.cgbref_li.restype = _u64
         L.cgbref_set_sample_budget.argtypes = [_vp, ctypes.c_double]
+        L.cgbref_set_progress.argtypes = [_vp, _vp]
         L.cgbref_last_sample.argtypes = [_vp, ctypes.POINTER(_u64), ctypes.POINTER(_u64),
                                          ctypes.POINTER(ctypes.c_double)]
         self.L = L
@@ -281,3 +282,67 @@ def read_updates(path: str) -> np.ndarray:
         if len(t) >= 3:
             out.append((int(t[1]), int(t[2])))
     return np.array(out, dtype=np.int64).reshape(-1, 2)
+
+
+# ---------------------------------------------------------------------------
+# Supervised sample of the reference CPU path (bench.py's reference arm and
+# cpu_baseline): the reference enumerates every embedding, and one seed row on
+# an R-MAT hub can run for hours, so the batch runs in a child process that
+# publishes progress in shared memory and is stopped at a deadline.
+# ---------------------------------------------------------------------------
+def _supervised_child(query, data, update, batch_size_ints, threads, shm_name):
+    from multiprocessing import shared_memory
+
+    os.environ["CGB_REF_THREADS"] = str(threads)
+    shm = shared_memory.SharedMemory(name=shm_name)
+    buf = np.ndarray((8,), dtype=np.uint64, buffer=shm.buf)
+    ref = RefPipeline(query, data, update, batch_size_ints, threads=threads)
+    ref.L.cgbref_set_progress(ref.h, buf.ctypes.data)
+    buf[7] = 1
+    ref.step()
+    buf[7] = 2
+    del buf
+    shm.close()
+
+
+def supervised_reference_batch(query: str, data: str, update: str, batch_size_ints: int, threads: int,
+                               count_budget_s: float, open_timeout_s: float = 300.0) -> dict:
+    """Runs batch 0 of the reference CPU path with all `threads`; Stage 1,
+    staging and the mirror update are timed fully, the count for at most
+    count_budget_s.  Returns the stage times (ms), rows counted / total and
+    the count time spent."""
+    import multiprocessing as mp
+    import time
+    from multiprocessing import shared_memory
+
+    shm = shared_memory.SharedMemory(create=True, size=64)
+    buf = np.ndarray((8,), dtype=np.uint64, buffer=shm.buf)
+    buf[:] = 0
+    ctx = mp.get_context("spawn")
+    p = ctx.Process(target=_supervised_child, args=(query, data, update, batch_size_ints, threads, shm.name))
+    t0 = time.time()
+    p.start()
+    try:
+        while buf[6] < 2 and p.is_alive() and time.time() - t0 < open_timeout_s:
+            time.sleep(0.05)
+        t_count = time.time()
+        while buf[6] < 3 and p.is_alive() and time.time() - t_count < count_budget_s:
+            time.sleep(0.05)
+        if buf[6] < 2:
+            raise RuntimeError(f"reference child stopped before counting (exit code {p.exitcode})")
+        out = {"s1_ms": buf[2] / 1e3, "staging_ms": buf[3] / 1e3, "mirror_ms": buf[4] / 1e3,
+               "rows_done": int(buf[0]), "rows_total": int(buf[1]),
+               "count_ms": (time.time() - t_count) * 1e3 if buf[6] < 3 else buf[5] / 1e3,
+               "finished": bool(buf[6] >= 3), "reached_count": bool(buf[6] >= 2),
+               "wall_s": time.time() - t0}
+    finally:
+        if p.is_alive():
+            p.terminate()
+        p.join(timeout=30)
+        if p.is_alive():
+            p.kill()
+            p.join(timeout=30)
+        del buf
+        shm.close()
+        shm.unlink()
+    return out

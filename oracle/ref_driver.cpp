@@ -22,6 +22,7 @@
 //                                cpu_dfs.h:21-29)
 // and then calls the reference's CPUIndexMirror and cpuExtendBFSAllBitCount.
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cstdint>
 #include <cstdio>
@@ -86,6 +87,10 @@ struct RefPipeline {
     double sample_budget_ms = 0;
     uint64_t sample_rows_done = 0, sample_rows_total = 0;
     double sample_ms = 0;
+    // optional progress block (shared with a supervising process):
+    // [0] rows done, [1] rows total, [2] S1 us, [3] staging us, [4] mirror us,
+    // [5] count us so far, [6] phase (1 = S1 done, 2 = counting, 3 = finished)
+    volatile uint64_t* progress = nullptr;
 
     // calig_helper_gamma.cu:77-105 (UpdateVertexMappingCPU) and :132-154
     // (buildGlobalVertexMapping): every vertex with any LI bit gets the next
@@ -183,6 +188,7 @@ struct RefPipeline {
         calig->ConstructUpdate(start, count);
         calig->mergeDeltas(b);
         t_s1_ms = ms_since(t0);
+        if (progress) { progress[2] = (uint64_t)(t_s1_ms * 1e3); progress[6] = 1; }
 
         t0 = Clock::now();
         // PrepareUpdateAll (calig_helper_gamma.cu:363-401)
@@ -222,6 +228,7 @@ struct RefPipeline {
         mirror->MergeInsert(ins_keys);
         mirror->MergeRemove(del_keys);
         t_mirror_ms = ms_since(t0);
+        if (progress) { progress[3] = (uint64_t)(t_stage_ms * 1e3); progress[4] = (uint64_t)(t_mirror_ms * 1e3); }
 
         last_count = 0;
         last_seed_rows = 0;
@@ -256,6 +263,25 @@ struct RefPipeline {
         const uint8_t d2e = mirror->DirToEdge(idx);
         std::vector<uint32_t> rows;
         uint64_t total = 0;
+        if (progress) {
+            // total seed rows first, so a supervisor can extrapolate from rows done
+            uint64_t all = 0;
+            for (uint32_t ei = 0; ei < QE_COUNT; ++ei) {
+                if (!edge_ok[ei]) continue;
+                const auto& io = plan->indexing_orders_[ei];
+                const uint32_t sa = eidx(io.vs_[0], io.vs_[1]), sb = eidx(io.vs_[1], io.vs_[0]);
+                const bool upd = (idx == sa || idx == sb);
+                for (uint32_t v = 0; v < dv_count; ++v) {
+                    uint32_t bl = 0, al = 0;
+                    if (upd) mirror->UpdateList(idx, v, bl); else mirror->MainList(idx, v, bl);
+                    if (d2e < ei) mirror->UpdateList(idx, v, al);
+                    all += bl + al;
+                }
+            }
+            progress[1] = all;
+            progress[0] = 0;
+            progress[6] = 2;
+        }
         for (uint32_t ei = 0; ei < QE_COUNT; ++ei) {
             if (!edge_ok[ei]) continue;
             const auto& io = plan->indexing_orders_[ei];
@@ -274,6 +300,19 @@ struct RefPipeline {
             last_seed_rows += n;
             sample_rows_total += n;
             if (n == 0) continue;
+            if (progress) {
+                // supervised sample: every row on its own across all host threads,
+                // with per-row progress (a supervisor stops the process at its deadline)
+                std::atomic<uint64_t> acc{0};
+                tbb::parallel_for((uint64_t)0, n, [&](uint64_t r) {
+                    acc += cpuExtendBFSAllBitCount(rows.data() + 2 * r, 1, 2, *mirror, query, *plan);
+                    __atomic_fetch_add((uint64_t*)&progress[0], 1ull, __ATOMIC_RELAXED);
+                    progress[5] = (uint64_t)(ms_since(t_begin) * 1e3);
+                });
+                total += acc.load();
+                sample_rows_done += n;
+                continue;
+            }
             const uint64_t chunk = sample_budget_ms > 0 ? 4096 : n;
             for (uint64_t r0 = 0; r0 < n; r0 += chunk) {
                 if (sample_budget_ms > 0 && ms_since(t_begin) > sample_budget_ms) break;
@@ -288,6 +327,7 @@ struct RefPipeline {
             }
         }
         sample_ms = ms_since(t_begin);
+        if (progress) progress[6] = 3;
         return total;
     }
 
@@ -329,6 +369,8 @@ void cgbref_set_parallel_dfs(void* h, int on) { ((RefPipeline*)h)->dfs_parallel 
 void cgbref_set_count(void* h, int on) { ((RefPipeline*)h)->do_count = on; }
 // Bounded count: stop after budget_ms (0 = complete count).
 void cgbref_set_sample_budget(void* h, double ms) { ((RefPipeline*)h)->sample_budget_ms = ms; }
+// Progress block written while stepping (see RefPipeline::progress).
+void cgbref_set_progress(void* h, uint64_t* p) { ((RefPipeline*)h)->progress = p; }
 // Rows counted / rows total / ms spent in the last batch's count.
 void cgbref_last_sample(void* h, uint64_t* done, uint64_t* total, double* ms) {
     auto* p = (RefPipeline*)h;

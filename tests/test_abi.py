@@ -27,6 +27,7 @@ def test_library_exports_every_declared_symbol():
 
 def test_default_config_without_gpu():
     lib = engine.load_library()
-    cfg = engine.Config(7, 1, 2, 3, 4)
+    cfg = engine.Config(7, 1, 2, 3, 4, 5, 6)
     lib.cgb_default_config(ctypes.byref(cfg))
-    assert (cfg.device, cfg.pool_words, cfg.dfs_blocks_per_sm, cfg.flags, cfg.dfs_budget_ms) == (0, 0, 0, 0, 0)
+    assert (cfg.device, cfg.pool_words, cfg.dfs_blocks_per_sm, cfg.flags, cfg.dfs_budget_ms, cfg.shard_index,
+            cfg.num_shards) == (0, 0, 0, 0, 0, 0, 0)

@@ -186,3 +186,33 @@ def test_cli_drop_in_total(name, workdir):
         pass
     assert got == ref.L.cgbref_total_count(ref.h)
     ref.close()
+
+
+@pytest.mark.parametrize("name", ["t_er_sparse", "t_rmat"])
+def test_seed_shards_sum_to_full_count(name, workdir):
+    """Multi-GPU split: shards (run one after another on one GPU) add up to the
+    unsharded count of every batch, and every shard keeps the full index."""
+    if not bind.have_ref():
+        pytest.skip("oracle/_ref/libcgbref.so not built")
+    spec = SPECS[name]
+    p = materialize(spec, workdir)
+    ref = bind.RefPipeline(p["query"], p["data"], p["update"], spec.cli_batch_size)
+    ref.set_count(False)
+    ql, qe = read_query(p["query"])
+    init = ref.init_keys()
+    engines = [Engine(shard_index=i, num_shards=3) for i in range(3)]
+    full = Engine()
+    for e in engines + [full]:
+        e.load_query(len(ql), qe, ql)
+        e.build_index(init, ref.dv_count)
+    while ref.step() >= 0:
+        r = ref.last()
+        args = (r["dv"], r["ins"], r["del"], r["delta"], r["edge_ok"])
+        parts = [e.apply_batch(*args) for e in engines]
+        assert sum(parts) == full.apply_batch(*args)
+    idx = full.read_index()
+    for e in engines:
+        assert np.array_equal(e.read_index(), idx)
+        e.close()
+    full.close()
+    ref.close()
