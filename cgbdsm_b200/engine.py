@@ -27,7 +27,11 @@ EXPORTS = [
     "cgb_apply_batch_device", "cgb_last_edge_counts", "cgb_read_index", "cgb_last_timings",
     "cgb_kernel_launches", "cgb_last_stats", "cgb_stream", "cgb_producer_open", "cgb_producer_close", "cgb_producer_last_error",
     "cgb_producer_num_batches", "cgb_producer_initial", "cgb_producer_next", "cgb_producer_vertex_map",
+    "cgb_merge_keys_noalloc",
 ]
+
+# Edits one cgb_merge_keys_noalloc call accepts (CGB_NOALLOC_MAX_EDITS).
+NOALLOC_MAX_EDITS = 1 << 18
 
 
 class CgbError(RuntimeError):
@@ -99,6 +103,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
                                          ctypes.POINTER(_u32)]
     lib.cgb_producer_next.argtypes = [_vp, ctypes.POINTER(BatchKeys)]
     lib.cgb_producer_vertex_map.argtypes = [_vp, ctypes.POINTER(ctypes.POINTER(_u32)), ctypes.POINTER(_u32)]
+    lib.cgb_merge_keys_noalloc.argtypes = [_vp, _u64, _vp, _u64, _vp, _u64, _u32, _vp, _vp, _vp]
     for name in EXPORTS:
         getattr(lib, name)
     _lib_handle = lib

@@ -201,6 +201,36 @@ cgb_status cgb_producer_next(cgb_producer* p, cgb_batch_keys* out);
 /* Compressed id -> original vertex id (valid until the next producer call). */
 cgb_status cgb_producer_vertex_map(const cgb_producer* p, const uint32_t** new2old, uint32_t* n);
 
+
+/* ------------------------------------------------------------------------
+ * Index update without device allocation.  No counterpart in the reference.
+ *
+ * For callers that cannot allocate device memory: code running while a CUDA
+ * graph is captured (cudaMalloc cannot be captured), hosts whose own
+ * allocator owns all device memory or caps it per tenant, plugins that may
+ * not grow a process's footprint after start-up.  Applies one batch of edits
+ * to an index given as one flat, sorted, duplicate-free key array:
+ *     out = (old U ins) \ del        (set semantics, as cgb_apply_batch)
+ * Inputs and outputs are device pointers the caller owns: old keys (sorted,
+ * u and v < dv_count), ins and del keys (any order, duplicates allowed),
+ * out (capacity >= n_old + n_ins), out_n (one u64: the output length, or
+ * UINT64_MAX if an edit key has u or v >= dv_count).  Work is enqueued on
+ * `stream` (a cudaStream_t; NULL = legacy default stream); nothing is
+ * synchronized.  All temporaries live in one static device array of 11.5 MiB
+ * that every GPU loading this library holds until the process exits; calls
+ * keep their contents in it, so calls whose work overlaps on one GPU race and
+ * must be ordered by the caller.  The first call on a device looks up the
+ * array's device address (cudaGetSymbolAddress) with that device current:
+ * make it before any stream capture.  Rejects more than CGB_NOALLOC_MAX_EDITS
+ * edits (n_ins + n_del) with CGB_ERR_LIMIT, before touching the device.
+ * Never calls cudaMalloc or cudaFree.
+ * ------------------------------------------------------------------------ */
+#define CGB_NOALLOC_MAX_EDITS (1u << 18)
+cgb_status cgb_merge_keys_noalloc(const uint64_t* old_keys_device, uint64_t n_old,
+                                  const uint64_t* ins_device, uint64_t n_ins,
+                                  const uint64_t* del_device, uint64_t n_del, uint32_t dv_count,
+                                  uint64_t* out_device, uint64_t* out_n_device, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
