@@ -331,18 +331,11 @@ __device__ __forceinline__ bool sorted_has(const uint32_t* __restrict__ p, uint3
     return lo < n && __ldg(p + lo) == x;
 }
 
-__device__ __forceinline__ bool list_has(const ListRef& L, uint32_t x) {
-    return sorted_has(L.m, L.ml, x) || (L.dl && sorted_has(L.d, L.dl, x));
-}
-
 __device__ __forceinline__ bool list_contains(const uint32_t* __restrict__ pool, const uint32_t* __restrict__ dval,
                                               const uint4& r, uint32_t x) {
     return sorted_has(pool + r.x, r.y, x) || (r.w && sorted_has(dval + r.z, r.w, x));
 }
 
-__device__ __forceinline__ uint32_t list_at(const ListRef& L, uint32_t i) {
-    return i < L.ml ? __ldg(L.m + i) : __ldg(L.d + (i - L.ml));
-}
 
 // Number of x in the intersection of the resolved lists bn[ids[0..nl)] with x
 // not among the matched core vertices m[0..nc).  Warp-cooperative; the result
@@ -537,15 +530,26 @@ __device__ __forceinline__ unsigned long long warp_sum(unsigned long long x) {
 // Termination: a warp leaves when completed == seeds + created (completed
 // read first); a unit's pushes happen before its completion, so equality
 // means no unit is active and none can be created.
+// Device-scope acquire load / release increment (cheaper than full fences).
+__device__ __forceinline__ unsigned int ld_acquire(const unsigned int* p) {
+    unsigned int v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void add_release(unsigned int* p, unsigned int v) {
+    asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
 constexpr uint32_t kTaskWords = 16;
 constexpr uint32_t kSplitMaxDepth = 5;
 constexpr uint32_t kSplitMinRemaining = 96;
 
-__global__ void __launch_bounds__(kDfsWarps * 32) k_dfs_count(DfsArgs a) {
+__global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
     __shared__ uint32_t s_cand[kDfsWarps][kMaxQV][32];
     __shared__ uint4 s_bn[kDfsWarps][kMaxBN];
     __shared__ uint32_t s_m[kDfsWarps][kMaxQV];
     __shared__ unsigned long long s_tc[kDfsWarps][kMaxQV * 8];
+    __shared__ uint2 s_rng[kDfsWarps][32];  // narrowed [lo, hi) per (backward list, part) of a chunk
     __shared__ uint32_t s_pre[kMaxQE + 1];
     __shared__ uint32_t s_lo[kMaxQE];
 
@@ -590,9 +594,9 @@ __global__ void __launch_bounds__(kDfsWarps * 32) k_dfs_count(DfsArgs a) {
                     kind = 2;
                     item = h;
                 } else {
-                    const unsigned int done = vq[3];
-                    __threadfence();
-                    const unsigned int made = vq[2];
+                    // completed is read with acquire before created (see termination above)
+                    const unsigned int done = ld_acquire((const unsigned int*)&a.qctr[3]);
+                    const unsigned int made = ld_acquire((const unsigned int*)&a.qctr[2]);
                     if (done == total + made && vq[6] >= total) kind = 3;
                 }
             }
@@ -603,7 +607,7 @@ __global__ void __launch_bounds__(kDfsWarps * 32) k_dfs_count(DfsArgs a) {
         if (kind == 0) {
             if (lane == 0 && !hungry) atomicAdd((unsigned int*)&a.qctr[4], 1u);
             hungry = true;
-            __nanosleep(256 + 32 * (idle_spins & 31));
+            __nanosleep(idle_spins < 64 ? 256u : 2048u);  // back off once the queue stays empty
             ++idle_spins;
             if ((idle_spins & 255u) == 0) {
                 const bool late = a.budget_ns && (global_ns() - t_start) > a.budget_ns;
@@ -670,7 +674,7 @@ __global__ void __launch_bounds__(kDfsWarps * 32) k_dfs_count(DfsArgs a) {
                 (P.n == 2) ? 1ull : tail_count_warp(P, m, bn, a.rec, a.dvcap, a.pool, a.dval, lane, n_bytes);
             if (lane == 0) { cnt += tc; ++n_tail; }
             __syncwarp();
-            if (lane == 0) { __threadfence(); atomicAdd((unsigned int*)&a.qctr[3], 1u); }
+            if (lane == 0) add_release((unsigned int*)&a.qctr[3], 1u);
             continue;
         }
 
@@ -759,13 +763,50 @@ __global__ void __launch_bounds__(kDfsWarps * 32) k_dfs_count(DfsArgs a) {
                     c = idx < gr.y ? __ldg(a.pool + gr.x + idx) : __ldg(a.dval + gr.z + (idx - gr.y));
                     n_bytes += 4;
                     for (uint32_t t = 0; t < j; ++t) ok &= (c != m[t]);
+                }
+                if (o1 - o0 > 1) {
+                    // Narrow every other backward list to the chunk's value range
+                    // [cmin, cmax] once (one lane per list part, two searches each),
+                    // so each candidate's probe runs over the narrowed window only.
+                    uint32_t cmin = ok ? c : 0xffffffffu, cmax = ok ? c : 0u;
+                    for (int o = 16; o > 0; o >>= 1) {
+                        cmin = min(cmin, __shfl_xor_sync(kFull, cmin, o));
+                        cmax = max(cmax, __shfl_xor_sync(kFull, cmax, o));
+                    }
+                    const uint32_t nparts = 2 * (o1 - o0);
+                    if (lane < nparts && cmin <= cmax) {
+                        const uint32_t k = o0 + (lane >> 1);
+                        const uint4 r = bn[k];
+                        const uint32_t* p = (lane & 1) ? a.dval + r.z : a.pool + r.x;
+                        const uint32_t n = (lane & 1) ? r.w : r.y;
+                        uint32_t lo = 0, len = n;
+                        while (len > 0) {
+                            const uint32_t half = len >> 1;
+                            if (__ldg(p + lo + half) < cmin) { lo += half + 1; len -= half + 1; }
+                            else len = half;
+                        }
+                        uint32_t hi = lo;
+                        len = n - lo;
+                        while (len > 0) {
+                            const uint32_t half = len >> 1;
+                            if (__ldg(p + hi + half) <= cmax) { hi += half + 1; len -= half + 1; }
+                            else len = half;
+                        }
+                        s_rng[w][lane] = make_uint2(lo, hi);
+                        n_bytes += 32u * 2u * (33u - __clz(n | 1u));
+                    }
+                    __syncwarp();
+                }
+                if (ok) {
                     for (uint32_t k = o0; k < o1 && ok; ++k) {
                         if (k == o0 + g) continue;
                         const uint4 r = bn[k];
-                        // binary search touches ~log2(len)+1 sectors of each part
-                        n_bytes += 32u * (33u - __clz(r.y | 1u));
-                        if (r.w) n_bytes += 32u * (33u - __clz(r.w | 1u));
-                        ok = list_contains(a.pool, a.dval, r, c);
+                        const uint2 rm = s_rng[w][2 * (k - o0)];
+                        const uint2 rd = s_rng[w][2 * (k - o0) + 1];
+                        n_bytes += 32u * (33u - __clz((rm.y - rm.x) | 1u));
+                        if (rd.y > rd.x) n_bytes += 32u * (33u - __clz((rd.y - rd.x) | 1u));
+                        ok = sorted_has(a.pool + r.x + rm.x, rm.y - rm.x, c) ||
+                             (rd.y > rd.x && sorted_has(a.dval + r.z + rd.x, rd.y - rd.x, c));
                     }
                     ++n_tested;
                 }
@@ -810,7 +851,7 @@ __global__ void __launch_bounds__(kDfsWarps * 32) k_dfs_count(DfsArgs a) {
             if (lane == 0) atomicOr(a.err, 8u);
             break;
         }
-        if (lane == 0) { __threadfence(); atomicAdd((unsigned int*)&a.qctr[3], 1u); }
+        if (lane == 0) add_release((unsigned int*)&a.qctr[3], 1u);
     }
     if (out_of_time && lane == 0) atomicOr(a.err, 8u);
     if (hungry && lane == 0) atomicSub((unsigned int*)&a.qctr[4], 1u);
@@ -1346,7 +1387,9 @@ cgb_status cgb_build_index(cgb_handle* h, const uint64_t* keys, uint64_t n, uint
     cgb_status s;
     if ((s = ensure_dvcap(h, std::max<uint32_t>(dv_count, 1))) != CGB_OK) return s;
     unsigned long long cap = h->cfg.pool_words;
-    if (cap == 0) cap = std::max<unsigned long long>(4ull * n + (16ull << 20), 64ull << 20);
+    // out-of-place merges write every touched run anew, so the pool carries
+    // headroom for many batches between compactions (HBM is plentiful)
+    if (cap == 0) cap = std::max<unsigned long long>(4ull * n + (128ull << 20), 192ull << 20);
     CK(cudaMalloc(&h->pool, cap * sizeof(uint32_t)));
     h->pool_cap = cap;
     h->h_pool_top = 0;
