@@ -3,6 +3,9 @@
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
+#include <fstream>
+#include <numeric>
+#include <random>
 #include <unordered_map>
 
 namespace cgb {
@@ -45,6 +48,40 @@ struct Tok {
         while (p < e && *p >= '0' && *p <= '9') v = v * 10 + (*p++ - '0');
         x = neg ? -v : v;
         return true;
+    }
+};
+
+// The C library's rand() from its default state (seed 1, no srand call):
+// glibc's additive feedback generator of degree 31 and separation 3.  The
+// state r[0..30] comes from the Lehmer sequence r[i] = 16807 r[i-1] mod
+// (2^31 - 1) started at the seed; r[31..33] repeat r[0..2]; afterwards
+// r[i] = r[i-31] + r[i-3] (mod 2^32) and the k-th output is r[k+344] >> 1.
+// Restated from the published description of the generator so the label
+// sequence does not depend on other users of rand() in the process.
+class LibcRand {
+public:
+    LibcRand() {
+        int32_t r[34];
+        r[0] = 1;
+        for (int i = 1; i < 31; ++i) {
+            const int64_t v = (16807LL * r[i - 1]) % 2147483647LL;
+            r[i] = (int32_t)(v < 0 ? v + 2147483647LL : v);
+        }
+        for (int i = 31; i < 34; ++i) r[i] = r[i - 31];
+        for (int i = 0; i < 34; ++i) ring_[i % 34] = (uint32_t)r[i];
+        n_ = 34;
+        for (int i = 34; i < 344; ++i) step();
+    }
+    int next() { return (int)(step() >> 1); }
+
+private:
+    uint32_t ring_[34];
+    uint64_t n_ = 0;  // index of the next value r[n_]
+    uint32_t step() {
+        const uint32_t v = ring_[(n_ - 31) % 34] + ring_[(n_ - 3) % 34];
+        ring_[n_ % 34] = v;
+        ++n_;
+        return v;
     }
 };
 
@@ -181,6 +218,71 @@ std::string CaLiGIndex::load_graph(const std::string& path) {
     for (auto& v : nei_) {
         std::sort(v.begin(), v.end());
         v.erase(std::unique(v.begin(), v.end()), v.end());
+    }
+    li_.assign(n, 0);
+    checked_.assign(n, 0);
+    return "";
+}
+
+std::string CaLiGIndex::load_graph_bin(const std::string& prefix) {
+    std::ifstream meta(prefix + ".meta.txt");
+    if (!meta) return "cannot open " + prefix + ".meta.txt";
+    uint64_t n_edges = 0;
+    uint32_t n = 0, vsize = 0, esize = 0, vlbl = 0, elbl = 0, maxdeg = 0, feat = 0, nvcls = 0, necls = 0;
+    meta >> n >> n_edges >> vsize >> esize >> vlbl >> elbl >> maxdeg >> feat >> nvcls >> necls;
+    if (!meta) return "bad meta file " + prefix + ".meta.txt";
+    if (vsize != 4 || esize != 8) return "unsupported id sizes in meta (expected vertex 4, edge 8)";
+    if (nvcls == 0) return "meta gives zero vertex classes";
+    std::vector<uint64_t> row(n + 1ull, 0);
+    FILE* f = std::fopen((prefix + ".vertex.bin").c_str(), "rb");
+    if (!f) return "cannot open " + prefix + ".vertex.bin";
+    const size_t got_r = std::fread(row.data(), sizeof(uint64_t), row.size(), f);
+    std::fclose(f);
+    if (got_r != row.size()) return "short read of " + prefix + ".vertex.bin";
+    std::vector<uint32_t> adj(n_edges, 0);
+    f = std::fopen((prefix + ".edge.bin").c_str(), "rb");
+    if (!f) return "cannot open " + prefix + ".edge.bin";
+    const size_t got_e = n_edges ? std::fread(adj.data(), sizeof(uint32_t), adj.size(), f) : 0;
+    std::fclose(f);
+    if (got_e != adj.size()) return "short read of " + prefix + ".edge.bin";
+    for (uint32_t v = 0; v < n; ++v)
+        if (row[v] > row[v + 1] || row[v + 1] > n_edges) return "row pointers out of order or range";
+    LibcRand rnd;
+    glabel_.assign(n, -1);
+    for (uint32_t v = 0; v < n; ++v) {
+        const int lb = rnd.next() % (int)nvcls;
+        glabel_[v] = (size_t)lb < label_slot_.size() ? label_slot_[lb] : -1;
+    }
+    // an edge is an update edge iff hash(min, max) % 10 == 0; each such
+    // pair is listed once, from its smaller endpoint's row, as (max, min)
+    auto is_update = [](uint32_t a, uint32_t b) {
+        const uint64_t key = ((uint64_t)std::min(a, b) << 32) | std::max(a, b);
+        return (key * 0x9e3779b97f4a7c15ULL) % 10ULL == 0;
+    };
+    nei_.assign(n, {});
+    std::vector<int> upd;
+    for (uint32_t v = 0; v < n; ++v) {
+        auto& nv = nei_[v];
+        for (uint64_t i = row[v]; i < row[v + 1]; ++i) {
+            const uint32_t u = adj[i];
+            if (is_update(v, u)) {
+                if (v < u) { upd.push_back((int)u); upd.push_back((int)v); }
+            } else {
+                nv.push_back(u);
+            }
+        }
+        std::sort(nv.begin(), nv.end());
+        nv.erase(std::unique(nv.begin(), nv.end()), nv.end());
+    }
+    const size_t pairs = upd.size() / 2;
+    std::vector<int> idx(pairs);
+    std::iota(idx.begin(), idx.end(), 0);
+    std::mt19937 rng(42);
+    std::shuffle(idx.begin(), idx.end(), rng);
+    update_.assign(upd.size(), 0);
+    for (size_t i = 0; i < pairs; ++i) {
+        update_[2 * i] = upd[2 * (size_t)idx[i]];
+        update_[2 * i + 1] = upd[2 * (size_t)idx[i] + 1];
     }
     li_.assign(n, 0);
     checked_.assign(n, 0);

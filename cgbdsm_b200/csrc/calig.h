@@ -27,6 +27,11 @@ public:
     std::string load_query(const std::string& path);
     std::string load_graph(const std::string& path);
     std::string load_updates(const std::string& path);
+    // Binary CSR prefix (calig.cpp:218-323): <prefix>.meta.txt, .vertex.bin
+    // (u64 row pointers), .edge.bin (u32 neighbours).  Labels are drawn with
+    // the C library's rand() sequence from its default seed, the update stream
+    // is the hash-selected 10% of the edges, shuffled with mt19937(42).
+    std::string load_graph_bin(const std::string& prefix);
 
     // constructCand + staticFilter (calig.cpp:325-356, 705-717)
     void construct();

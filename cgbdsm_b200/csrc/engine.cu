@@ -46,9 +46,12 @@ namespace {
 
 constexpr uint32_t kFull = 0xffffffffu;
 constexpr int kDfsWarps = 8;  // warps per DFS block
-constexpr uint32_t kTaskCap = 1u << 20;  // stolen-range queue capacity (64 MiB)
+constexpr uint32_t kTaskCap = 1u << 20;  // stolen-range ring capacity (64 MiB), a power of two
+constexpr uint32_t kTaskSlack = 1u << 13; // tickets kept between the ring's tail and head
 
 __constant__ EdgePlan c_plan[kMaxQE];
+__constant__ cgb::VbPlan c_vb[kMaxQE];
+__constant__ uint8_t c_dir_edge[kMaxDir];
 
 // ---------------------------------------------------------------------------
 // key packing
@@ -298,12 +301,15 @@ struct DfsArgs {
     unsigned long long budget_ns;  // per-launch wall-clock budget (0 = unlimited)
     uint32_t* tasks;             // stolen-range queue [task_cap][16 words]
     uint32_t task_cap;
-    unsigned int* qctr;          // [8]: tail, head, created, completed, hungry, -, seeds issued
+    unsigned int* qctr;          // [8]: tasks reserved, tickets issued, -, completed, -, -, seeds issued
     uint32_t epoch;              // per-launch tag written as a task's ready flag (never 0)
-    uint32_t force_split;        // split every long shallow range, hungry warps or not (tests)
+    uint32_t force_split;        // publish unstarted work at every chunk, waited for or not (tests)
     uint32_t shard, num_shards;  // this engine expands seeds i with i % num_shards == shard
     uint32_t steal;              // share long shallow ranges through the queue
     uint32_t tail_cache;         // count prefix-only tail subsets once per prefix
+    const uint32_t* vb;          // valid bits [qe][qv][vb_stride] or nullptr (no pruning)
+    uint32_t vb_stride;
+    uint32_t qv;
 };
 
 __device__ __forceinline__ unsigned long long global_ns() {
@@ -338,18 +344,19 @@ __device__ __forceinline__ bool list_contains(const uint32_t* __restrict__ pool,
 
 
 // Number of x in the intersection of the resolved lists bn[ids[0..nl)] with x
-// not among the matched core vertices m[0..nc).  Warp-cooperative; the result
-// is warp-uniform.  One list: its length minus the core vertices it holds.
+// not among the matched core vertices m[t], t in the bit set excl (positions
+// whose vertex can lie in these lists).  Warp-cooperative; the result is
+// warp-uniform.  One list: its length minus the excluded vertices it holds.
 // Several: the shortest list is scanned 32 elements at a time and each
 // element probed in the others.
 __device__ unsigned long long isect_count(const uint4* bn, const uint8_t* ids, uint32_t nl, const uint32_t* m,
-                                          uint32_t nc, const uint32_t* __restrict__ pool,
+                                          uint32_t excl, const uint32_t* __restrict__ pool,
                                           const uint32_t* __restrict__ dval, uint32_t lane,
                                           unsigned long long& bytes) {
     if (nl == 1) {
         const uint4 r = bn[ids[0]];
         bool in = false;
-        if (lane < nc) {
+        if (lane < 16 && ((excl >> lane) & 1u)) {
             in = list_contains(pool, dval, r, m[lane]);
             bytes += 32u * (33u - __clz(r.y | 1u));
         }
@@ -368,7 +375,7 @@ __device__ unsigned long long isect_count(const uint4* bn, const uint8_t* ids, u
         if (ok) {
             const uint32_t x = idx < gr.y ? __ldg(pool + gr.x + idx) : __ldg(dval + gr.z + (idx - gr.y));
             bytes += 4;
-            for (uint32_t t = 0; t < nc; ++t) ok &= (x != m[t]);
+            for (uint32_t e = excl; e; e &= e - 1) ok &= (x != m[__ffs(e) - 1]);
             for (uint32_t i = 0; i < nl && ok; ++i) {
                 if (i == g) continue;
                 const uint4 r = bn[ids[i]];
@@ -379,6 +386,15 @@ __device__ unsigned long long isect_count(const uint4* bn, const uint8_t* ids, u
         c += __popc(__ballot_sync(kFull, ok));
     }
     return c;
+}
+
+// Injective assignments of a label group of k <= 3 tail vertices from the
+// sizes sc[mask] of the intersections of its members' candidate sets
+// (inclusion-exclusion over coinciding members).
+__device__ __forceinline__ unsigned long long group_count(const unsigned long long* sc, uint32_t k) {
+    if (k == 1) return sc[1];
+    if (k == 2) return sc[1] * sc[2] - sc[3];
+    return sc[1] * sc[2] * sc[4] - sc[3] * sc[4] - sc[5] * sc[2] - sc[6] * sc[1] + 2 * sc[7];
 }
 
 // Number of injective assignments of the tail vertices given the matched core
@@ -411,13 +427,9 @@ __device__ unsigned long long tail_count_warp(const EdgePlan& P, const uint32_t*
             for (uint32_t i = 0; i < k; ++i)
                 if (mask & (1u << i))
                     for (uint32_t q = P.bn_off[t + i]; q < P.bn_off[t + i + 1]; ++q) ids[nl++] = (uint8_t)q;
-            sc[mask] = isect_count(bn, ids, nl, m, nc, pool, dval, lane, bytes);
+            sc[mask] = isect_count(bn, ids, nl, m, P.excl[t], pool, dval, lane, bytes);
         }
-        unsigned long long g;
-        if (k == 1) g = sc[1];
-        else if (k == 2) g = sc[1] * sc[2] - sc[3];
-        else g = sc[1] * sc[2] * sc[4] - sc[3] * sc[4] - sc[5] * sc[2] - sc[6] * sc[1] + 2 * sc[7];
-        prod *= g;
+        prod *= group_count(sc, k);
         t = e;
     }
     return prod;
@@ -428,7 +440,8 @@ __device__ unsigned long long tail_count_warp(const EdgePlan& P, const uint32_t*
 // hang only off prefix vertices have counts that do not depend on the
 // candidate: tail_prepare computes them once per prefix (excluding the prefix
 // vertices); tail_eval then only subtracts whether the candidate itself lies
-// in the set, and scans only the subsets that involve position j.
+// in the set, and intersects the subsets with lists at position j per
+// candidate.
 constexpr unsigned long long kDynamic = ~0ull;
 
 __device__ void tail_prepare(const EdgePlan& P, const uint32_t* m, uint4* bn, unsigned long long* cache,
@@ -458,7 +471,9 @@ __device__ void tail_prepare(const EdgePlan& P, const uint32_t* m, uint4* bn, un
                         ids[nl++] = (uint8_t)q;
                         dynamic |= P.bn_pos[q] == j;
                     }
-            const unsigned long long v = dynamic ? kDynamic : isect_count(bn, ids, nl, m, j, pool, dval, lane, bytes);
+            const unsigned long long v =
+                dynamic ? kDynamic
+                        : isect_count(bn, ids, nl, m, P.excl[t] & ((1u << j) - 1u), pool, dval, lane, bytes);
             if (lane == 0) cache[t * 8 + mask] = v;
         }
         t = e;
@@ -495,7 +510,9 @@ __device__ unsigned long long tail_eval(const EdgePlan& P, const uint32_t* m, ui
                 if (mask & (1u << i))
                     for (uint32_t q = P.bn_off[t + i]; q < P.bn_off[t + i + 1]; ++q) ids[nl++] = (uint8_t)q;
             const unsigned long long cv = cache[t * 8 + mask];
-            if (cv != kDynamic) {
+            if (cv != kDynamic && !((P.excl[t] >> j) & 1u)) {
+                sc[mask] = cv;  // the candidate cannot lie in these lists (another label)
+            } else if (cv != kDynamic) {
                 bool in = true;
                 if (lane < nl) {
                     const uint4 r = bn[ids[lane]];
@@ -504,14 +521,25 @@ __device__ unsigned long long tail_eval(const EdgePlan& P, const uint32_t* m, ui
                 }
                 sc[mask] = cv - (__all_sync(kFull, in) ? 1ull : 0ull);
             } else {
-                sc[mask] = isect_count(bn, ids, nl, m, nc, pool, dval, lane, bytes);
+                sc[mask] = isect_count(bn, ids, nl, m, P.excl[t], pool, dval, lane, bytes);
             }
         }
-        unsigned long long g;
-        if (k == 1) g = sc[1];
-        else if (k == 2) g = sc[1] * sc[2] - sc[3];
-        else g = sc[1] * sc[2] * sc[4] - sc[3] * sc[4] - sc[5] * sc[2] - sc[6] * sc[1] + 2 * sc[7];
-        prod *= g;
+        prod *= group_count(sc, k);
+        t = e;
+    }
+    return prod;
+}
+
+// Tail count of a plan with tail_const: every subset is prefix-only and no
+// candidate of the last core position can lie in a tail list, so the count
+// is the product of the cached group counts.
+__device__ unsigned long long tail_const_value(const EdgePlan& P, const unsigned long long* cache) {
+    unsigned long long prod = 1;
+    uint32_t t = P.n_core;
+    while (t < P.n && prod) {
+        uint32_t e = t;
+        while (e < P.n && P.tail_gid[e] == P.tail_gid[t]) ++e;
+        prod *= group_count(cache + t * 8, e - t);
         t = e;
     }
     return prod;
@@ -523,13 +551,19 @@ __device__ __forceinline__ unsigned long long warp_sum(unsigned long long x) {
 }
 
 // Work units of the DFS: seeds (delta edges) from a counter, and stolen
-// ranges from a queue.  A task is 16 words: w0 = ei | depth << 8 | generator
-// << 16, w1/w2 = [lo, hi) of the generator list, w3 = ready flag, w4..15 =
-// the matched prefix.  A warp at a shallow depth whose remaining range is long
-// while other warps are hungry publishes the upper half of the range.
-// Termination: a warp leaves when completed == seeds + created (completed
-// read first); a unit's pushes happen before its completion, so equality
-// means no unit is active and none can be created.
+// ranges from a ring of tasks.  A task is 16 words: w0 = ei | depth << 8 |
+// generator << 16, w1/w2 = [lo, hi) of the generator list, w3 = ready tag,
+// w4..15 = the matched prefix.  A warp without a seed takes one ticket
+// (atomicAdd on the ticket counter) and waits for task number `ticket`;
+// tasks are reserved in ticket order, so every task has exactly one
+// consumer and idle warps never contend.  While tickets outnumber reserved
+// tasks, a busy warp publishes all the work it has not started at its
+// shallowest level (top of its stack), so the biggest remaining subtrees
+// move first.  Termination: a warp leaves when completed == seeds + reserved
+// (completed read first); a unit's reservations happen before its
+// completion, so equality means no unit is active and none can be created
+// (and every reserved task was consumed, so the waiting warp's ticket will
+// never be filled).
 // Device-scope acquire load / release increment (cheaper than full fences).
 __device__ __forceinline__ unsigned int ld_acquire(const unsigned int* p) {
     unsigned int v;
@@ -541,8 +575,17 @@ __device__ __forceinline__ void add_release(unsigned int* p, unsigned int v) {
 }
 
 constexpr uint32_t kTaskWords = 16;
-constexpr uint32_t kSplitMaxDepth = 5;
-constexpr uint32_t kSplitMinRemaining = 96;
+constexpr uint32_t kNoTicket = 0xffffffffu;
+// Ready tag of ticket t in launch `epoch`: the epoch's low 20 bits and the
+// ring lap of t, so a slot reused in a later lap or launch never shows a
+// stale tag to the consumer of t.
+__device__ __forceinline__ uint32_t task_tag(uint32_t epoch, uint32_t t) {
+    return ((epoch & 0xfffffu) << 12) | ((t / kTaskCap) & 0xfffu);
+}
+// s_cand entries: vertex id (< 2^27) | offset of the candidate in the
+// generator chunk it came from << 27
+constexpr uint32_t kCandBits = 27;
+constexpr uint32_t kCandMask = (1u << kCandBits) - 1u;
 
 __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
     __shared__ uint32_t s_cand[kDfsWarps][kMaxQV][32];
@@ -564,7 +607,7 @@ __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
     const uint64_t vmask = (1ull << a.B) - 1ull;
     uint32_t* m = s_m[w];
     uint4* bn = s_bn[w];
-    volatile unsigned int* vq = a.qctr;  // [0] tail, [1] head, [2] created, [3] completed, [4] hungry
+    volatile unsigned int* vq = a.qctr;  // [0] tasks reserved, [1] tickets issued, [3] completed, [6] seeds
 
     // per-depth state held by lane == depth
     uint32_t st_ncand = 0, st_pos = 0, st_next = 0, st_len = 0, st_gen = 0;
@@ -574,29 +617,34 @@ __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
     int cur_ei = -1;
     const unsigned long long t_start = global_ns();
     uint32_t steps = 0;
+    uint32_t split_tick = 0;  // waiting warps are checked for every 4th chunk
     bool out_of_time = false;
-    bool hungry = false;
+    uint32_t ticket = kNoTicket;  // lane 0: ticket of the task ring this warp waits on
     bool tail_ready = false;
+    unsigned long long tail_const = 0;  // tail count of the current prefix (plans with tail_const)
     uint32_t idle_spins = 0;
 
     for (;;) {
         // ---- acquire a unit: 1 = seed, 2 = task, 3 = all done, 0 = nothing yet
         uint32_t kind = 0, item = 0;
         if (lane == 0) {
-            if (vq[6] < total) {  // vq[6] mirrors work_next without incrementing it
+            if (ticket == kNoTicket && vq[6] < total) {  // vq[6] mirrors work_next without incrementing it
                 item = atomicAdd(a.work_next, 1u);
                 if (item < total) kind = 1;
                 else atomicMax((unsigned int*)&a.qctr[6], total);
             }
             if (!kind) {
-                const unsigned int h = vq[1];
-                if (h < vq[0] && atomicCAS((unsigned int*)&a.qctr[1], h, h + 1) == h) {
+                // no seed left: hold one ticket of the task ring and wait for its task
+                if (ticket == kNoTicket) ticket = atomicAdd((unsigned int*)&a.qctr[1], 1u);
+                const volatile uint32_t* tk = a.tasks + (size_t)(ticket & (a.task_cap - 1u)) * kTaskWords;
+                if (tk[3] == task_tag(a.epoch, ticket)) {
                     kind = 2;
-                    item = h;
-                } else {
-                    // completed is read with acquire before created (see termination above)
+                    item = ticket;
+                    ticket = kNoTicket;
+                } else if ((idle_spins & 3u) == 3u) {
+                    // completed is read with acquire before reserved (see termination above)
                     const unsigned int done = ld_acquire((const unsigned int*)&a.qctr[3]);
-                    const unsigned int made = ld_acquire((const unsigned int*)&a.qctr[2]);
+                    const unsigned int made = ld_acquire((const unsigned int*)&a.qctr[0]);
                     if (done == total + made && vq[6] >= total) kind = 3;
                 }
             }
@@ -605,19 +653,13 @@ __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
         item = __shfl_sync(kFull, item, 0);
         if (kind == 3) break;
         if (kind == 0) {
-            if (lane == 0 && !hungry) atomicAdd((unsigned int*)&a.qctr[4], 1u);
-            hungry = true;
-            __nanosleep(idle_spins < 64 ? 256u : 2048u);  // back off once the queue stays empty
+            __nanosleep(idle_spins < 64 ? 128u : 1024u);
             ++idle_spins;
             if ((idle_spins & 255u) == 0) {
                 const bool late = a.budget_ns && (global_ns() - t_start) > a.budget_ns;
                 if (__shfl_sync(kFull, late ? 1 : 0, 0)) { out_of_time = true; break; }
             }
             continue;
-        }
-        if (hungry) {
-            if (lane == 0) atomicSub((unsigned int*)&a.qctr[4], 1u);
-            hungry = false;
         }
         idle_spins = 0;
 
@@ -634,20 +676,8 @@ __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
             }
             ++n_seeds;
         } else {
-            // the producer reserved the slot before publishing; wait (bounded) for the data
-            volatile uint32_t* tk = a.tasks + (size_t)item * kTaskWords;
-            uint32_t ready = 0;
-            if (lane == 0) {
-                for (uint32_t it = 0; it < (1u << 22); ++it) {
-                    if (tk[3] == a.epoch) { ready = 1; break; }
-                    __nanosleep(64);
-                }
-            }
-            ready = __shfl_sync(kFull, ready, 0);
-            if (!ready) {  // never published: give up cleanly
-                if (lane == 0) atomicOr(a.err, 16u);
-                break;
-            }
+            // lane 0 saw the ticket's ready tag: the task's words are published
+            volatile uint32_t* tk = a.tasks + (size_t)(item & (a.task_cap - 1u)) * kTaskWords;
             __threadfence();
             const uint32_t wv = lane < kTaskWords ? tk[lane] : 0;
             const uint32_t w0 = __shfl_sync(kFull, wv, 0);
@@ -717,7 +747,7 @@ __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
             const uint32_t pos = __shfl_sync(kFull, st_pos, j);
             if (pos < ncand) {
                 if (lane == j) st_pos = pos + 1;
-                if (lane == 0) m[j] = s_cand[w][j][pos];
+                if (lane == 0) m[j] = s_cand[w][j][pos] & kCandMask;
                 __syncwarp();
                 ++j;
                 setup(j);
@@ -727,31 +757,63 @@ __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
             uint32_t glen = __shfl_sync(kFull, st_len, j);
             if (gnext < glen) {
                 const uint32_t g = __shfl_sync(kFull, st_gen, j);
-                // share the rest of a long shallow range with hungry warps
-                if (a.steal && j <= kSplitMaxDepth && glen - gnext >= kSplitMinRemaining) {
-                    uint32_t slot = 0xffffffffu;
-                    if (lane == 0 && (vq[4] > 0 || a.force_split)) {
-                        const unsigned int t = vq[0];
-                        if (t < a.task_cap && atomicCAS((unsigned int*)&a.qctr[0], t, t + 1) == t) {
-                            atomicAdd((unsigned int*)&a.qctr[2], 1u);
-                            slot = t;
+                // While warps wait for tasks, hand the work not yet started at the
+                // shallowest level of this unit to the queue: at a depth d < j
+                // the buffered survivors not yet descended plus the unscanned
+                // generator range, at d = j the range after this chunk.  The
+                // survivors are a contiguous stretch of the generator (their
+                // offsets in their chunk ride in the top bits of s_cand), so
+                // one range [lo, hi) of depth d's generator describes it all.
+                if (a.steal && (a.force_split || ((++split_tick & 3u) == 0))) {
+                    uint32_t want = 0;  // some warp holds a ticket no task has been reserved for
+                    if (lane == 0) want = (a.force_split || (int)(vq[1] - vq[0]) > 0) ? 1u : 0u;
+                    if (__shfl_sync(kFull, want, 0)) {
+                        bool has = false;
+                        if (lane >= jbase && lane < j) has = st_next < st_len || st_pos < st_ncand;
+                        if (lane == j) has = glen > gnext + 32u;
+                        const uint32_t hb = __ballot_sync(kFull, has);
+                        uint32_t slot = 0xffffffffu;
+                        if (hb && lane == 0) {
+                            // reserve the next ticket while it is (or, under force_split, soon
+                            // may be) waited for; the ring never laps its head
+                            const unsigned int t = vq[0], hd = vq[1];
+                            if ((a.force_split || (int)(hd - t) > 0) && (int)(t - hd) < (int)(a.task_cap - kTaskSlack) &&
+                                atomicCAS((unsigned int*)&a.qctr[0], t, t + 1) == t)
+                                slot = t;
                         }
-                    }
-                    slot = __shfl_sync(kFull, slot, 0);
-                    if (slot != 0xffffffffu) {
-                        const uint32_t mid = gnext + 32u + (((glen - gnext - 32u) / 2u) & ~31u);
-                        uint32_t* tk = a.tasks + (size_t)slot * kTaskWords;
-                        uint32_t v = 0;
-                        if (lane == 0) v = (uint32_t)ei | (j << 8) | (g << 16);
-                        else if (lane == 1) v = mid;
-                        else if (lane == 2) v = glen;
-                        else if (lane >= 4 && lane < 4 + kMaxQV) v = (lane - 4 < j) ? m[lane - 4] : 0u;
-                        if (lane < kTaskWords && lane != 3) tk[lane] = v;
-                        __threadfence();
-                        __syncwarp();
-                        if (lane == 0) *(volatile uint32_t*)(tk + 3) = a.epoch;
-                        if (lane == j) st_len = mid;
-                        glen = mid;
+                        slot = __shfl_sync(kFull, slot, 0);
+                        if (slot != 0xffffffffu) {
+                            const uint32_t d = __ffs(hb) - 1;
+                            uint32_t lo = 0, hi = 0;
+                            if (lane == d) {
+                                if (d == j) {
+                                    lo = gnext + 32u;
+                                    hi = glen;
+                                } else {
+                                    lo = st_pos < st_ncand ? st_next - 32u + (s_cand[w][d][st_pos] >> kCandBits)
+                                                           : st_next;
+                                    hi = st_len;
+                                }
+                            }
+                            lo = __shfl_sync(kFull, lo, d);
+                            hi = __shfl_sync(kFull, hi, d);
+                            const uint32_t gd = __shfl_sync(kFull, st_gen, d);
+                            uint32_t* tk = a.tasks + (size_t)(slot & (a.task_cap - 1u)) * kTaskWords;
+                            uint32_t v = 0;
+                            if (lane == 0) v = (uint32_t)ei | (d << 8) | (gd << 16);
+                            else if (lane == 1) v = lo;
+                            else if (lane == 2) v = hi;
+                            else if (lane >= 4 && lane < 4 + kMaxQV) v = (lane - 4 < d) ? m[lane - 4] : 0u;
+                            if (lane < kTaskWords && lane != 3) tk[lane] = v;
+                            __threadfence();
+                            __syncwarp();
+                            if (lane == 0) *(volatile uint32_t*)(tk + 3) = task_tag(a.epoch, slot);
+                            if (lane == d) {
+                                if (d == j) st_len = gnext + 32u;
+                                else { st_len = st_next; st_ncand = st_pos; }
+                            }
+                            if (d == j) glen = gnext + 32u;
+                        }
                     }
                 }
                 const uint32_t o0 = P.bn_off[j], o1 = P.bn_off[j + 1];
@@ -763,6 +825,8 @@ __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
                     c = idx < gr.y ? __ldg(a.pool + gr.x + idx) : __ldg(a.dval + gr.z + (idx - gr.y));
                     n_bytes += 4;
                     for (uint32_t t = 0; t < j; ++t) ok &= (c != m[t]);
+                    if (ok && a.vb)  // the valid bits are a sound superset: a clear bit cannot match
+                        ok = (__ldg(a.vb + ((size_t)ei * a.qv + P.vs[j]) * a.vb_stride + (c >> 5)) >> (c & 31)) & 1u;
                 }
                 if (o1 - o0 > 1) {
                     // Narrow every other backward list to the chunk's value range
@@ -812,7 +876,18 @@ __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
                 }
                 ++n_chunks;
                 if (j == nc - 1) {
-                    if (has_tail) {
+                    if (has_tail && P.tail_const && a.tail_cache) {
+                        // the tail count depends on the prefix only: one value per prefix
+                        const uint32_t bal = __ballot_sync(kFull, ok);
+                        if (bal) {
+                            if (!tail_ready) {
+                                tail_prepare(P, m, bn, s_tc[w], a.rec, a.dvcap, a.pool, a.dval, lane, n_bytes);
+                                tail_const = tail_const_value(P, s_tc[w]);
+                                tail_ready = true;
+                            }
+                            if (lane == 0) { cnt += (unsigned long long)__popc(bal) * tail_const; n_tail += __popc(bal); }
+                        }
+                    } else if (has_tail) {
                         // every surviving candidate completes a core embedding: count its tail
                         uint32_t bal = __ballot_sync(kFull, ok);
                         while (bal) {
@@ -838,7 +913,7 @@ __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
                     }
                 } else {
                     const uint32_t bal = __ballot_sync(kFull, ok);
-                    if (ok) s_cand[w][j][__popc(bal & ((1u << lane) - 1u))] = c;
+                    if (ok) s_cand[w][j][__popc(bal & ((1u << lane) - 1u))] = c | (lane << kCandBits);
                     if (lane == j) { st_ncand = __popc(bal); st_pos = 0; }
                 }
                 if (lane == j) st_next = gnext + 32;
@@ -854,7 +929,6 @@ __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
         if (lane == 0) add_release((unsigned int*)&a.qctr[3], 1u);
     }
     if (out_of_time && lane == 0) atomicOr(a.err, 8u);
-    if (hungry && lane == 0) atomicSub((unsigned int*)&a.qctr[4], 1u);
     const unsigned long long c = warp_sum(cnt);
     if (cur_ei >= 0 && lane == 0 && c) atomicAdd(a.counts + cur_ei, c);
     const unsigned long long tested = warp_sum(n_tested), tails = warp_sum(n_tail), bytes = warp_sum(n_bytes);
@@ -865,6 +939,76 @@ __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
         atomicAdd(a.stats + 3, tails);
         atomicAdd(a.stats + 4, bytes);
         atomicAdd(a.stats + 7, n_tasks);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// valid bits (BuildLocalIndexBitAll with 1-bit masks, graph_gpu.cu:803-869,
+// indexing.cu:2295-2379): vb[ei][u][w] holds bit (dv & 31) of word dv >> 5
+// for query vertex u under query edge ei.  A sound superset of the vertices
+// that some embedding mapping ei to a delta edge can place at u.
+// ---------------------------------------------------------------------------
+// Rebuilt (ei, u) start empty, the others all ones (graph_gpu.cu:818-828).
+__global__ void k_vb_fill(uint32_t* vb, uint32_t qe, uint32_t qv, uint32_t stride) {
+    const size_t n = (size_t)qe * qv * stride;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const uint32_t ei = (uint32_t)(i / ((size_t)qv * stride));
+        const uint32_t u = (uint32_t)((i / stride) % qv);
+        vb[i] = ((c_vb[ei].rebuild >> u) & 1u) ? 0u : 0xffffffffu;
+    }
+}
+
+// Endpoints of ei: vertices with a delta list in ei's own direction
+// (setInitialValidBitsAll1Bit, indexing.cu:2295-2317), set from the sorted
+// packed delta keys (d << 2B | u << B | v): one bit per key, no full sweep.
+__global__ void k_vb_seed(const uint64_t* __restrict__ dkeys, uint64_t n, uint32_t B, uint32_t* vb, uint32_t qv,
+                          uint32_t stride) {
+    const uint64_t m = (1ull << B) - 1ull;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t k = dkeys[i];
+        const uint32_t d = (uint32_t)(k >> (2 * B)), u = (uint32_t)((k >> B) & m);
+        const uint32_t ei = c_dir_edge[d];
+        const cgb::VbPlan& P = c_vb[ei];
+        const uint32_t qu = d == P.d01 ? P.vs[0] : P.vs[1];
+        atomicOr(vb + ((size_t)ei * qv + qu) * stride + (u >> 5), 1u << (u & 31));
+    }
+}
+
+// Position `depth` of every query edge's indexing order (grid.y = ei): a
+// vertex is valid if, for every backward neighbour, its list towards that
+// neighbour (old run, plus the delta run when visible) holds a vertex whose
+// bit is set (checkAllConstraintsAndSetBitsAll1Bit, indexing.cu:2319-2377).
+// One warp per mask word, one lane per vertex.
+__global__ void k_vb_depth(const uint4* __restrict__ rec, uint32_t dvcap, const uint32_t* __restrict__ pool,
+                           const uint32_t* __restrict__ dval, uint32_t dv, uint32_t* vb, uint32_t qv,
+                           uint32_t stride, uint32_t depth) {
+    const uint32_t ei = blockIdx.y;
+    const cgb::VbPlan& P = c_vb[ei];
+    const uint32_t u = P.vs[depth];
+    if (!((P.rebuild >> u) & 1u)) return;
+    uint32_t* out = vb + ((size_t)ei * qv + u) * stride;
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t wi = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; wi < stride; wi += nw) {
+        const uint32_t x = wi * 32u + lane;
+        bool valid = x < dv;
+        for (uint32_t b = P.off[depth]; b < P.off[depth + 1] && valid; ++b) {
+            const uint32_t* m1 = vb + ((size_t)ei * qv + P.vs[P.bpos[b]]) * stride;
+            const uint4 r = rec[(size_t)P.bdir[b] * dvcap + x];
+            bool sat = false;
+            for (uint32_t t = 0; t < r.y && !sat; ++t) {
+                const uint32_t nb = __ldg(pool + r.x + t);
+                sat = (m1[nb >> 5] >> (nb & 31)) & 1u;
+            }
+            if (P.bvis[b])
+                for (uint32_t t = 0; t < r.w && !sat; ++t) {
+                    const uint32_t nb = __ldg(dval + r.z + t);
+                    sat = (m1[nb >> 5] >> (nb & 31)) & 1u;
+                }
+            valid = sat;
+        }
+        const uint32_t word = __ballot_sync(kFull, valid);
+        if (lane == 0) out[wi] = word;
     }
 }
 
@@ -991,9 +1135,16 @@ struct cgb_handle {
     unsigned long long last_stats[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     void* d_temp = nullptr; size_t temp_cap = 0;
 
+    // valid bits
+    uint32_t vb_start[2] = {0, 0};   // starting edge (SelectStartingEdge)
+    std::string vb_plan_error;       // set when the pattern has no consistent rebuild flags
+    uint32_t* d_vb = nullptr; size_t vb_cap = 0;
+    uint32_t vb_stride = 0;          // words per (ei, u) of the last matched batch; 0 = none
+    float last_vb_ms = 0;
+
     uint64_t last_counts[kMaxQE] = {0};
     float last_t[4] = {0, 0, 0, 0};
-    cudaEvent_t ev[6] = {};
+    cudaEvent_t ev[7] = {};  // phases 0-3, caller-stream order 4, end 5, valid bits 6
 };
 
 namespace {
@@ -1382,6 +1533,17 @@ cgb_status cgb_build_index(cgb_handle* h, const uint64_t* keys, uint64_t n, uint
     cgb::plan_edges(h->q, avg, h->plans, !(h->cfg.flags & CGB_FLAG_ENUMERATE_TAIL),
                     !(h->cfg.flags & CGB_FLAG_PLAIN_CORE_ORDER));
     CK(cudaMemcpyToSymbol(c_plan, h->plans, sizeof(EdgePlan) * kMaxQE));
+    {
+        // valid-bit plans from the reference's starting edge
+        cgb::select_starting_edge(h->q, card.data(), avg, h->vb_start);
+        cgb::VbPlan vbp[kMaxQE];
+        std::memset(vbp, 0, sizeof(vbp));
+        h->vb_plan_error = cgb::plan_valid_bits(h->q, h->vb_start, vbp);
+        if (!h->vb_plan_error.empty() && (h->cfg.flags & (CGB_FLAG_VALID_BITS | CGB_FLAG_MASK_PRUNE)))
+            return fail(h, CGB_ERR_ARG, "valid bits: %s", h->vb_plan_error.c_str());
+        CK(cudaMemcpyToSymbol(c_vb, vbp, sizeof(vbp)));
+        CK(cudaMemcpyToSymbol(c_dir_edge, h->q.dir_to_edge, sizeof(h->q.dir_to_edge)));
+    }
 
     h->dv = dv_count;
     cgb_status s;
@@ -1460,6 +1622,29 @@ cgb_status cgb_apply_batch_device(cgb_handle* h, uint32_t dv_count, const uint64
                                                edge_ok ? 1 : 0, h->d_seed, h->d_seed + kMaxQE);
         LAUNCHED();
         CK(cudaGetLastError());
+        const bool vb_on = (h->cfg.flags & (CGB_FLAG_VALID_BITS | CGB_FLAG_MASK_PRUNE)) != 0;
+        h->vb_stride = 0;
+        if (vb_on) {
+            // 2b. valid bits: fill, endpoints from the delta keys, then one
+            // launch per indexing-order position (all query edges at once)
+            const uint32_t stride = (dv_count + 31) / 32, qv = h->q.qv, qe = h->q.qe;
+            if ((s = grow(h, h->d_vb, h->vb_cap, (size_t)qe * qv * stride)) != CGB_OK) return s;
+            CK(cudaEventRecord(h->ev[6], h->stream));
+            const size_t words = (size_t)qe * qv * stride;
+            k_vb_fill<<<(unsigned)std::min<size_t>((words + 255) / 256, (size_t)h->num_sms * 16), 256, 0,
+                        h->stream>>>(h->d_vb, qe, qv, stride);
+            LAUNCHED();
+            k_vb_seed<<<grid_for(h, n_delta), 256, 0, h->stream>>>(h->d_dkeys, n_delta, B, h->d_vb, qv, stride);
+            LAUNCHED();
+            const dim3 g((unsigned)std::min<uint32_t>((stride + 7) / 8, (uint32_t)h->num_sms * 8), qe);
+            for (uint32_t d = 2; d < qv; ++d) {
+                k_vb_depth<<<g, 256, 0, h->stream>>>(h->rec, h->dvcap, h->pool, h->d_dval, dv_count, h->d_vb, qv,
+                                                     stride, d);
+                LAUNCHED();
+            }
+            CK(cudaGetLastError());
+            h->vb_stride = stride;
+        }
         CK(cudaEventRecord(h->ev[2], h->stream));
 
         // 3. matching
@@ -1480,12 +1665,18 @@ cgb_status cgb_apply_batch_device(cgb_handle* h, uint32_t dv_count, const uint64
         da.tasks = h->d_tasks;
         da.task_cap = kTaskCap;
         da.qctr = h->d_qctr;
-        da.epoch = ++h->dfs_epoch ? h->dfs_epoch : ++h->dfs_epoch;
+        do {  // the tag's epoch field must never be 0 (the ring starts zeroed)
+            ++h->dfs_epoch;
+        } while ((h->dfs_epoch & 0xfffffu) == 0);
+        da.epoch = h->dfs_epoch;
         da.force_split = (h->cfg.flags & CGB_FLAG_FORCE_SPLIT) ? 1u : 0u;
         da.num_shards = h->cfg.num_shards ? h->cfg.num_shards : 1u;
         da.steal = (h->cfg.flags & CGB_FLAG_NO_STEAL) ? 0u : 1u;
         da.tail_cache = (h->cfg.flags & CGB_FLAG_NO_TAIL_CACHE) ? 0u : 1u;
         da.shard = h->cfg.shard_index < da.num_shards ? h->cfg.shard_index : 0u;
+        da.vb = (h->cfg.flags & CGB_FLAG_MASK_PRUNE) ? h->d_vb : nullptr;
+        da.vb_stride = h->vb_stride;
+        da.qv = h->q.qv;
         da.budget_ns = h->cfg.dfs_budget_ms ? (unsigned long long)h->cfg.dfs_budget_ms * 1000000ull
                                             : 600ull * 1000000000ull;
         // persistent grid: exactly the blocks that can be resident at once
@@ -1519,6 +1710,8 @@ cgb_status cgb_apply_batch_device(cgb_handle* h, uint32_t dv_count, const uint64
     cudaEventElapsedTime(&t12, h->ev[1], h->ev[2]);
     cudaEventElapsedTime(&t23, h->ev[2], h->ev[3]);
     cudaEventElapsedTime(&t03, h->ev[0], h->ev[5]);
+    h->last_vb_ms = 0;
+    if (h->vb_stride) cudaEventElapsedTime(&h->last_vb_ms, h->ev[6], h->ev[2]);
     h->last_t[0] = t01; h->last_t[1] = t12; h->last_t[2] = t23; h->last_t[3] = t03;
     for (int i = 0; i < 8; ++i) h->last_stats[i] = h->h_scal[4 + kMaxQE + i];
     if (h->h_scal[2]) {
@@ -1577,6 +1770,30 @@ cgb_status cgb_last_stats(const cgb_handle* h, uint64_t* out8) {
 }
 
 void* cgb_stream(const cgb_handle* h) { return h ? (void*)h->stream : nullptr; }
+
+cgb_status cgb_starting_edge(const cgb_handle* h, uint32_t* out2) {
+    if (!h || !out2) return CGB_ERR_ARG;
+    if (!h->have_index) return CGB_ERR_STATE;
+    out2[0] = h->vb_start[0];
+    out2[1] = h->vb_start[1];
+    return CGB_OK;
+}
+
+cgb_status cgb_valid_bits(cgb_handle* h, uint32_t* out, uint64_t cap, uint64_t* n_words, float* ms) {
+    if (!h || !n_words) return CGB_ERR_ARG;
+    *n_words = 0;
+    if (!h->vb_stride) return fail(h, CGB_ERR_STATE, "no valid bits: enable CGB_FLAG_VALID_BITS and match a batch");
+    const uint64_t n = (uint64_t)h->q.qe * h->q.qv * h->vb_stride;
+    *n_words = n;
+    if (ms) *ms = h->last_vb_ms;
+    if (!out) return CGB_OK;
+    if (cap < n) return fail(h, CGB_ERR_ARG, "buffer holds %llu of %llu words", (unsigned long long)cap,
+                             (unsigned long long)n);
+    CK(cudaSetDevice(h->device));
+    CK(cudaMemcpyAsync(out, h->d_vb, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return CGB_OK;
+}
 
 cgb_status cgb_read_index(cgb_handle* h, uint64_t* out, uint64_t cap, uint64_t* n_out) {
     if (!h || !n_out) return CGB_ERR_ARG;

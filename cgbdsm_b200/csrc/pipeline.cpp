@@ -60,15 +60,13 @@ cgb_status cgb_producer_open(const char* query_path, const char* data_path, cons
     *out = p;
     p->batch_size = batch_size_ints ? batch_size_ints : UINT32_MAX;
     std::string e = p->idx.load_query(query_path);
-    if (e.empty()) {
-        std::string dp = data_path;
-        if (dp.size() < 6 || dp.compare(dp.size() - 6, 6, ".graph") != 0) {
-            p->err = "binary CSR input (calig.cpp:218-323) is not supported; use a .graph text file";
-            return CGB_ERR_ARG;
-        }
-        e = p->idx.load_graph(data_path);
-    }
-    if (e.empty() && update_path) e = p->idx.load_updates(update_path);
+    // main_calig.cpp:93-101: a data path ending in ".graph" is text and takes
+    // the update file; anything else is a binary CSR prefix whose update
+    // stream is derived from the graph (the update path is ignored)
+    const std::string dp = data_path;
+    const bool text = dp.size() >= 6 && dp.compare(dp.size() - 6, 6, ".graph") == 0;
+    if (e.empty()) e = text ? p->idx.load_graph(data_path) : p->idx.load_graph_bin(dp);
+    if (e.empty() && text && update_path) e = p->idx.load_updates(update_path);
     if (!e.empty()) {
         p->err = e;
         return CGB_ERR_IO;

@@ -1,5 +1,7 @@
 #include "query.h"
 
+#include <limits>
+
 #include <algorithm>
 #include <cstring>
 #include <fstream>
@@ -249,7 +251,158 @@ void plan_edges(const QueryMeta& q, const float* avg_deg, EdgePlan* plans, bool 
             }
         }
         p.bn_off[q.qv] = (uint8_t)k;
+        const bool known = !q.labels.empty();
+        for (uint32_t t = n_core; t < q.qv; ++t)
+            for (uint32_t c = 0; c < n_core; ++c)
+                if (!known || lab(p.vs[c]) == lab(p.vs[t])) p.excl[t] |= (uint16_t)(1u << c);
+        if (known && n_core > 2 && n_core < q.qv) {
+            bool cst = true;
+            const uint32_t jl = n_core - 1;
+            for (uint32_t t = n_core; t < q.qv; ++t) {
+                cst &= lab(p.vs[t]) != lab(p.vs[jl]);
+                for (uint32_t b = p.bn_off[t]; b < p.bn_off[t + 1]; ++b) cst &= p.bn_pos[b] != jl;
+            }
+            p.tail_const = cst ? 1 : 0;
+        }
     }
+}
+
+void select_starting_edge(const QueryMeta& q, const uint64_t* card, const float* avg, uint32_t out[2]) {
+    std::vector<uint32_t> sel, nxt;
+    // 1. largest endpoint degree sum
+    size_t best = 0;
+    for (uint32_t e = 0; e < q.qe; ++e) {
+        const size_t sd = q.nbrs[q.qe_u[e]].size() + q.nbrs[q.qe_v[e]].size();
+        if (sd > best) { best = sd; sel.assign(1, e); }
+        else if (sd == best) sel.push_back(e);
+    }
+    // 2. most triangles
+    if (sel.size() > 1) {
+        uint32_t bt = 0;
+        nxt.clear();
+        for (uint32_t e : sel) {
+            const uint32_t a = q.qe_u[e], b = q.qe_v[e];
+            uint32_t t = 0;
+            for (uint32_t x = 0; x < q.qv; ++x)
+                t += (q.eidx[x * kMaxQV + a] != 255 && q.eidx[x * kMaxQV + b] != 255) ? 1u : 0u;
+            if (t > bt) { bt = t; nxt.assign(1, e); }
+            else if (t == bt) nxt.push_back(e);
+        }
+        sel.swap(nxt);
+    }
+    // 3. fewest index entries on (a -> b)
+    if (sel.size() > 1) {
+        uint64_t bc = UINT32_MAX;
+        nxt.clear();
+        for (uint32_t e : sel) {
+            const uint64_t c = card[q.eidx[q.qe_u[e] * kMaxQV + q.qe_v[e]]];
+            if (c < bc) { bc = c; nxt.assign(1, e); }
+            else if (c == bc) nxt.push_back(e);
+        }
+        sel.swap(nxt);
+    }
+    // 4. smallest sum of the other incident directions' mean list lengths
+    //    (float, summed in neighbour order as the reference does)
+    if (sel.size() > 1) {
+        float bs = std::numeric_limits<float>::max();
+        nxt.clear();
+        for (uint32_t e : sel) {
+            const uint32_t a = q.qe_u[e], b = q.qe_v[e];
+            float sum = 0.0f;
+            for (uint32_t w : q.nbrs[a])
+                if (w != b) sum += avg[q.eidx[a * kMaxQV + w]];
+            for (uint32_t w : q.nbrs[b])
+                if (w != a) sum += avg[q.eidx[b * kMaxQV + w]];
+            if (sum < bs) { bs = sum; nxt.assign(1, e); }
+            else if (sum == bs) nxt.push_back(e);
+        }
+        sel.swap(nxt);
+    }
+    out[0] = q.qe_u[sel[0]];
+    out[1] = q.qe_v[sel[0]];
+}
+
+std::string plan_valid_bits(const QueryMeta& q, const uint32_t start[2], VbPlan* plans) {
+    const uint32_t qv = q.qv;
+    auto adj = [&](uint32_t a, uint32_t b) { return q.eidx[a * kMaxQV + b] != 255; };
+    for (uint32_t ei = 0; ei < q.qe; ++ei) {
+        VbPlan& P = plans[ei];
+        std::memset(&P, 0, sizeof(P));
+        const uint32_t u0 = q.qe_u[ei], u1 = q.qe_v[ei];
+        // indexing order: BFS by levels, neighbours ascending
+        std::vector<uint32_t> order{u0, u1};
+        std::vector<char> vis(qv, 0);
+        vis[u0] = vis[u1] = 1;
+        for (size_t lo = 0; lo < order.size();) {
+            const size_t hi = order.size();
+            for (size_t i = lo; i < hi; ++i)
+                for (uint32_t w : q.nbrs[order[i]])
+                    if (!vis[w]) { vis[w] = 1; order.push_back(w); }
+            lo = hi;
+        }
+        if (order.size() != qv) return "query is not connected";
+        uint32_t k = 0;
+        for (uint32_t j = 0; j < qv; ++j) {
+            P.vs[j] = (uint8_t)order[j];
+            P.off[j] = (uint8_t)k;
+            for (uint32_t t = 0; t < j; ++t)
+                if (adj(order[j], order[t])) {
+                    const uint8_t d = q.eidx[order[j] * kMaxQV + order[t]];
+                    P.bpos[k] = (uint8_t)t;
+                    P.bdir[k] = d;
+                    P.bvis[k] = q.dir_to_edge[d] <= ei ? 1 : 0;
+                    ++k;
+                }
+        }
+        P.off[qv] = (uint8_t)k;
+        P.d01 = q.eidx[u0 * kMaxQV + u1];
+        P.d10 = q.eidx[u1 * kMaxQV + u0];
+        // rebuild edges: every simple path from a starting vertex to u0 or u1
+        std::vector<char> f((size_t)qv * qv, 0);
+        f[u0 * qv + u1] = f[u1 * qv + u0] = 1;
+        for (int si = 0; si < 2; ++si) {
+            std::vector<uint32_t> path(qv + 1, 0), ci(qv + 1, 0);
+            std::vector<char> on(qv, 0);
+            on[start[si]] = 1;
+            path[0] = start[si];
+            uint32_t depth = 1;
+            for (;;) {
+                const auto& nb = q.nbrs[path[depth - 1]];
+                bool pushed = false;
+                while (ci[depth] < nb.size()) {
+                    const uint32_t nv = nb[ci[depth]];
+                    if (on[nv]) { ++ci[depth]; continue; }
+                    if (nv == u0 || nv == u1) {
+                        path[depth] = nv;
+                        for (uint32_t i = 0; i < depth; ++i)
+                            f[path[i] * qv + path[i + 1]] = f[path[i + 1] * qv + path[i]] = 1;
+                        ++ci[depth];
+                        continue;
+                    }
+                    on[nv] = 1;
+                    path[depth] = nv;
+                    ++depth;
+                    pushed = true;
+                    break;
+                }
+                if (pushed) continue;
+                ci[depth] = 0;
+                if (--depth == 0) break;
+                on[path[depth]] = 0;
+                ++ci[depth];
+            }
+        }
+        // rebuilt vertices: all or none of a vertex's backward edges rebuilt
+        for (uint32_t i = 0; i < qv; ++i) {
+            const uint32_t u = P.vs[i];
+            if (i == 0) { P.rebuild |= (uint16_t)(1u << u); continue; }
+            uint32_t sum = 0;
+            for (uint32_t b = P.off[i]; b < P.off[i + 1]; ++b) sum += f[P.vs[P.bpos[b]] * qv + u] ? 1u : 0u;
+            if (sum == P.off[i + 1] - P.off[i]) P.rebuild |= (uint16_t)(1u << u);
+            else if (sum != 0) return "rebuild flags are inconsistent for this pattern (plan.cpp:1361-1366)";
+        }
+    }
+    return "";
 }
 
 }  // namespace cgb

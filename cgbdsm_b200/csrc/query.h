@@ -47,8 +47,41 @@ struct EdgePlan {
     uint8_t bn_dir[kMaxBN];
     uint8_t bn_dvis[kMaxBN];
     uint8_t tail_gid[kMaxQV];
-    uint8_t pad[2];
+    // tail_const: the last core vertex has no tail neighbour and its label
+    // differs from every tail label, so the tail count is the same for every
+    // candidate of the last core position (labels must be known).
+    uint8_t tail_const;
+    uint8_t pad;
+    // excl[t] (tail position t): core positions whose matched vertex can lie
+    // in t's candidate sets (same label; every core position when labels are
+    // unknown); only those are excluded from t's counts.
+    uint16_t excl[kMaxQV];
 };
+
+// Valid-bit plan of one query edge ei (the reference's 1-bit support masks,
+// BuildLocalIndexBitAll, graph_gpu.cu:803-869): its indexing order (BFS from
+// ei's endpoints, plan.cpp:1180-1230), each position's backward neighbours
+// with the direction vs[d] -> neighbour and whether that direction's delta
+// part is visible while building (dir_to_edge <= ei, indexing.cu:2345), and
+// the rebuilt vertices (plan.cpp:1277-1370); other vertices' masks are all
+// ones.
+struct VbPlan {
+    uint8_t vs[kMaxQV];
+    uint8_t off[kMaxQV + 1];
+    uint8_t bpos[kMaxBN];
+    uint8_t bdir[kMaxBN];
+    uint8_t bvis[kMaxBN];
+    uint16_t rebuild;
+    uint8_t d01, d10;  // directions vs[0] -> vs[1] and back
+};
+
+// SelectStartingEdge (plan.cpp:428-533): the first two vertices of the
+// reference's global order from the query and the initial index's
+// per-direction entry counts and mean list lengths.
+void select_starting_edge(const QueryMeta& q, const uint64_t* card, const float* avg, uint32_t out[2]);
+// Valid-bit plans for every query edge; "" or the reference's order error
+// (plan.cpp:1361-1366).
+std::string plan_valid_bits(const QueryMeta& q, const uint32_t start[2], VbPlan* plans);
 
 // Returns "" on success, else an error message.
 std::string build_query_meta(uint32_t qv, uint32_t qe, const uint32_t* edges, const uint32_t* labels,

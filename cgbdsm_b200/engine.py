@@ -27,7 +27,7 @@ EXPORTS = [
     "cgb_apply_batch_device", "cgb_last_edge_counts", "cgb_read_index", "cgb_last_timings",
     "cgb_kernel_launches", "cgb_last_stats", "cgb_stream", "cgb_producer_open", "cgb_producer_close", "cgb_producer_last_error",
     "cgb_producer_num_batches", "cgb_producer_initial", "cgb_producer_next", "cgb_producer_vertex_map",
-    "cgb_merge_keys_noalloc",
+    "cgb_merge_keys_noalloc", "cgb_valid_bits", "cgb_starting_edge",
 ]
 
 # Edits one cgb_merge_keys_noalloc call accepts (CGB_NOALLOC_MAX_EDITS).
@@ -51,6 +51,8 @@ FLAG_FORCE_SPLIT = 0x4
 FLAG_NO_STEAL = 0x8
 FLAG_NO_TAIL_CACHE = 0x10
 FLAG_PLAIN_CORE_ORDER = 0x20
+FLAG_VALID_BITS = 0x40
+FLAG_MASK_PRUNE = 0x80
 
 
 class BatchKeys(ctypes.Structure):
@@ -104,6 +106,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.cgb_producer_next.argtypes = [_vp, ctypes.POINTER(BatchKeys)]
     lib.cgb_producer_vertex_map.argtypes = [_vp, ctypes.POINTER(ctypes.POINTER(_u32)), ctypes.POINTER(_u32)]
     lib.cgb_merge_keys_noalloc.argtypes = [_vp, _u64, _vp, _u64, _vp, _u64, _u32, _vp, _vp, _vp]
+    lib.cgb_valid_bits.argtypes = [_vp, _vp, _u64, ctypes.POINTER(_u64), ctypes.POINTER(ctypes.c_float)]
+    lib.cgb_starting_edge.argtypes = [_vp, _vp]
     for name in EXPORTS:
         getattr(lib, name)
     _lib_handle = lib
@@ -217,6 +221,20 @@ class Engine:
         return {"seeds": int(out[0]), "chunks": int(out[1]), "tested": int(out[2]), "tails": int(out[3]),
                 "match_bytes": int(out[4]), "update_bytes": int(out[5]), "touched_runs": int(out[6]),
                 "stolen_tasks": int(out[7])}
+
+    def valid_bits(self) -> tuple[np.ndarray, float]:
+        """Valid bits of the last matched batch, words [ei][u][(dv+31)//32], and the pass's device ms."""
+        n = _u64(0)
+        ms = ctypes.c_float(0)
+        self._check(self.lib.cgb_valid_bits(self.h, None, 0, ctypes.byref(n), ctypes.byref(ms)))
+        out = np.zeros(max(n.value, 1), dtype=np.uint32)
+        self._check(self.lib.cgb_valid_bits(self.h, out.ctypes.data, n.value, ctypes.byref(n), None))
+        return out[: n.value], float(ms.value)
+
+    def starting_edge(self) -> tuple[int, int]:
+        out = np.zeros(2, dtype=np.uint32)
+        self._check(self.lib.cgb_starting_edge(self.h, out.ctypes.data))
+        return int(out[0]), int(out[1])
 
     def stream(self) -> int:
         return int(self.lib.cgb_stream(self.h) or 0)

@@ -131,3 +131,38 @@ def read_query(path: str) -> tuple[list[int], list[tuple[int, int]]]:
         elif t[0] == "e":
             edges.append((int(t[1]), int(t[2])))
     return [labels[i] for i in range(len(labels))], edges
+
+
+def write_binary_csr(spec: WorkloadSpec, directory: str, nvcls: int) -> dict[str, str]:
+    """Writes the full graph of spec (initial edges plus the held-out stream)
+    as the reference's binary CSR prefix (calig.cpp:218-323): <prefix>.meta.txt
+    ("n m 4 8 0 0 maxdeg 0 nvcls 0"), <prefix>.vertex.bin (u64 row pointers),
+    <prefix>.edge.bin (u32 neighbours, both directions, rows sorted).  Labels
+    and the update stream are not stored: the reader draws them.  Returns
+    {"data": prefix, "query": path of spec's query}."""
+    import numpy as np
+
+    p = materialize(spec, directory)
+    n = 0
+    edges = []
+    for path in (p["data"], p["update"]):
+        for line in open(path):
+            t = line.split()
+            if not t:
+                continue
+            if t[0] == "v":
+                n = max(n, int(t[1]) + 1)
+            elif len(t) >= 3:
+                edges.append((int(t[1]), int(t[2])))
+    e = np.array(edges, dtype=np.int64).reshape(-1, 2)
+    both = np.concatenate([e, e[:, ::-1]])
+    both = np.unique(both, axis=0)  # sorted by (row, neighbour), duplicates dropped
+    deg = np.bincount(both[:, 0], minlength=n)
+    row = np.zeros(n + 1, dtype=np.uint64)
+    np.cumsum(deg, out=row[1:])
+    prefix = os.path.join(directory, spec.name, f"{spec.name}_csr")
+    with open(prefix + ".meta.txt", "w") as f:
+        f.write(f"{n} {len(both)} 4 8 0 0 {int(deg.max()) if n else 0} 0 {nvcls} 0\n")
+    row.tofile(prefix + ".vertex.bin")
+    both[:, 1].astype(np.uint32).tofile(prefix + ".edge.bin")
+    return {"data": prefix, "query": p["query"]}

@@ -60,6 +60,8 @@ typedef struct {
 #define CGB_FLAG_NO_STEAL 0x8u            /* never share DFS ranges (one warp per seed)                 */
 #define CGB_FLAG_NO_TAIL_CACHE 0x10u      /* recount every tail subset for every core embedding        */
 #define CGB_FLAG_PLAIN_CORE_ORDER 0x20u   /* greedy core order only (no choice of the last core vertex) */
+#define CGB_FLAG_VALID_BITS 0x40u         /* compute the reference's valid bits every matched batch     */
+#define CGB_FLAG_MASK_PRUNE 0x80u         /* valid bits, and skip core candidates whose bit is clear    */
 
 /* Limits (reference: utils/config.h:5-6; key layout calig_helper_gamma.cu:228-229). */
 #define CGB_MAX_QV 12
@@ -188,7 +190,11 @@ typedef struct {
 } cgb_batch_keys;
 
 /* batch_size_ints counts ints, two per edge, as the reference CLI does
- * (main_calig.cpp:65-69, 103-104); UINT32_MAX = one batch. */
+ * (main_calig.cpp:65-69, 103-104); UINT32_MAX = one batch.  A data_path
+ * ending in ".graph" is a text graph and update_path its update stream;
+ * any other data_path is a binary CSR prefix (.meta.txt, .vertex.bin,
+ * .edge.bin; calig.cpp:218-323) whose update stream is derived from the
+ * graph, and update_path is ignored (main_calig.cpp:93-101). */
 cgb_status cgb_producer_open(const char* query_path, const char* data_path, const char* update_path,
                              uint32_t batch_size_ints, uint32_t threads, cgb_producer** out);
 void cgb_producer_close(cgb_producer* p);
@@ -230,6 +236,23 @@ cgb_status cgb_merge_keys_noalloc(const uint64_t* old_keys_device, uint64_t n_ol
                                   const uint64_t* ins_device, uint64_t n_ins,
                                   const uint64_t* del_device, uint64_t n_del, uint32_t dv_count,
                                   uint64_t* out_device, uint64_t* out_n_device, void* stream);
+
+/* Valid bits (the reference's 1-bit support masks, BuildLocalIndexBitAll,
+ * graph_gpu.cu:803-869; indexing.cu:2295-2379), computed for every matched
+ * batch when CGB_FLAG_VALID_BITS or CGB_FLAG_MASK_PRUNE is set, after the
+ * delta lists and before matching.  Layout: words [ei][u][(dv_count+31)/32],
+ * bit (x & 31) of word x >> 5 set when vertex x may take query vertex u in
+ * an embedding that maps query edge ei to a delta edge.  Orders, rebuilt
+ * vertices and the starting edge follow plan.cpp:428-533, 1180-1370; a
+ * pattern whose rebuild flags are inconsistent (the reference exits,
+ * plan.cpp:1361-1366) makes cgb_build_index fail with CGB_ERR_ARG when the
+ * flag is set.  Pass out = NULL to get *n_words only; *ms (optional) gets
+ * the pass's device time.  CGB_ERR_STATE if no batch has computed them. */
+cgb_status cgb_valid_bits(cgb_handle* h, uint32_t* out, uint64_t cap, uint64_t* n_words, float* ms);
+/* The starting edge (SelectStartingEdge, plan.cpp:428-533) the valid bits
+ * use: out2[0], out2[1] = the first two vertices of the reference's global
+ * order.  Available after cgb_build_index. */
+cgb_status cgb_starting_edge(const cgb_handle* h, uint32_t* out2);
 
 #ifdef __cplusplus
 }

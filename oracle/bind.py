@@ -72,6 +72,14 @@ class RefPipeline:
         L.cgbref_last_edge_ok.argtypes = [_vp]
         L.cgbref_last_edge_ok.restype = _u8p
         L.cgbref_global_order.argtypes = [_vp, _vp]
+        L.cgbref_cardinalities.argtypes = [_vp]
+        L.cgbref_cardinalities.restype = ctypes.POINTER(_u32)
+        L.cgbref_avg_degrees.argtypes = [_vp]
+        L.cgbref_avg_degrees.restype = ctypes.POINTER(ctypes.c_float)
+        L.cgbref_indexing_order.argtypes = [_vp, _u32, _vp, _vp, _vp]
+        L.cgbref_indexing_order.restype = _u32
+        L.cgbref_rebuild_vertices.argtypes = [_vp, _u32]
+        L.cgbref_rebuild_vertices.restype = _u32
         L.cgbref_new2old.argtypes = [_vp]
         L.cgbref_new2old.restype = ctypes.POINTER(_u32)
         L.cgbref_dump_main.argtypes = [_vp, _vp, _u64]
@@ -107,6 +115,10 @@ class RefPipeline:
     def qv(self) -> int:
         return self.L.cgbref_qv(self.h)
 
+    @property
+    def num_dir(self) -> int:
+        return self.L.cgbref_num_dir(self.h)
+
     def set_count(self, on: bool) -> None:
         self.L.cgbref_set_count(self.h, 1 if on else 0)
 
@@ -130,6 +142,24 @@ class RefPipeline:
         o = (ctypes.c_uint8 * 12)()
         self.L.cgbref_global_order(self.h, o)
         return np.array(list(o)[: self.qv], dtype=np.uint8)
+
+    def cardinalities(self) -> np.ndarray:
+        p = self.L.cgbref_cardinalities(self.h)
+        return np.array([p[i] for i in range(self.num_dir)], dtype=np.uint32)
+
+    def avg_degrees(self) -> np.ndarray:
+        p = self.L.cgbref_avg_degrees(self.h)
+        return np.array([p[i] for i in range(self.num_dir)], dtype=np.float32)
+
+    def indexing_order(self, ei: int):
+        vs = np.zeros(12, np.uint8)
+        offs = np.zeros(13, np.uint8)
+        bni = np.zeros(160, np.uint8)
+        n = self.L.cgbref_indexing_order(self.h, ei, vs.ctypes.data, offs.ctypes.data, bni.ctypes.data)
+        return vs[: self.qv].copy(), offs[: self.qv + 1].copy(), bni[:n].copy()
+
+    def rebuild_vertices(self, ei: int) -> int:
+        return int(self.L.cgbref_rebuild_vertices(self.h, ei))
 
     def new2old(self) -> np.ndarray:
         n = self.dv_count
@@ -191,6 +221,12 @@ class Oracle:
         L.orc_num_edges.restype = _u32
         L.orc_dir.argtypes = [_vp, _u32, _u32]
         L.orc_dir.restype = _u32
+        L.orc_starting_edge.argtypes = [_vp, _vp, _vp, _vp]
+        L.orc_set_valid_bits.argtypes = [_vp, ctypes.c_int, _u32, _u32]
+        L.orc_valid_bits.argtypes = [_vp, _vp, _u64]
+        L.orc_valid_bits.restype = _u64
+        L.orc_indexing_order.argtypes = [_vp, _u32, _u32, _u32, _vp, _vp, _vp, _vp]
+        L.orc_indexing_order.restype = _u32
         L.orc_bruteforce.restype = _u64
         L.orc_bruteforce.argtypes = [_u32, _vp, _vp, _vp, _u32, _vp, _u32, _vp]
         self.L = L
@@ -237,6 +273,35 @@ class Oracle:
         n = self.L.orc_dump(self.h, None, 0)
         out = np.zeros(max(n, 1), dtype=np.uint64)
         self.L.orc_dump(self.h, out.ctypes.data, n)
+        return out[:n]
+
+    def starting_edge(self, card: np.ndarray, avg: np.ndarray) -> tuple[int, int]:
+        c = np.ascontiguousarray(card, dtype=np.uint32)
+        a = np.ascontiguousarray(avg, dtype=np.float32)
+        out = np.zeros(2, np.uint32)
+        self.L.orc_starting_edge(self.h, c.ctypes.data, a.ctypes.data, out.ctypes.data)
+        return int(out[0]), int(out[1])
+
+    def indexing_order(self, ei: int, start: tuple[int, int]):
+        """(vs, offsets, bni, rebuild-vertex mask or ~0) of query edge ei."""
+        vs = np.zeros(12, np.uint8)
+        offs = np.zeros(13, np.uint8)
+        bni = np.zeros(160, np.uint8)
+        vf = _u32(0)
+        n = self.L.orc_indexing_order(self.h, ei, start[0], start[1], vs.ctypes.data, offs.ctypes.data,
+                                      bni.ctypes.data, ctypes.byref(vf))
+        return vs, offs, bni[:n].copy(), int(vf.value)
+
+    def set_valid_bits(self, mode: int, start: tuple[int, int]) -> None:
+        """mode 0 = off, 1 = compute per matched batch, 2 = compute and prune the count."""
+        self.L.orc_set_valid_bits(self.h, mode, start[0], start[1])
+
+    def valid_bits(self) -> np.ndarray:
+        n = self.L.orc_valid_bits(self.h, None, 0)
+        if n == 2**64 - 1:
+            raise ValueError("rebuild flags inconsistent (the reference stops here)")
+        out = np.zeros(max(n, 1), np.uint32)
+        self.L.orc_valid_bits(self.h, out.ctypes.data, n)
         return out[:n]
 
     def asymmetry(self) -> int:

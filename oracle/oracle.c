@@ -37,7 +37,10 @@
  *               are symmetric ((a->b) contains y at x iff (b->a) contains x
  *               at y), which tests/ check as a property.
  * Plus an independent brute-force embedding counter for the incremental
- * identity  sum(batch counts) = |Emb(Q, G_after)| - |Emb(Q, G_before)|.
+ * identity  sum(batch counts) = |Emb(Q, G_after)| - |Emb(Q, G_before)|,
+ * and the valid bits of BuildLocalIndexBitAll (graph_gpu.cu:803-869,
+ * indexing.cu:2295-2379, orders and rebuild flags plan.cpp:428-533,
+ * 1180-1370) with the starting edge of SelectStartingEdge.
  */
 #include <stdint.h>
 #include <stdlib.h>
@@ -65,6 +68,12 @@ typedef struct {
     uint64_t* pending;  /* delta keys of the last matched batch (merged before the next) */
     uint64_t n_pending;
     uint64_t last_edge_counts[ORC_MAXQE];
+    /* valid bits (BuildLocalIndexBitAll) of the last matched batch */
+    int vb_on;
+    uint32_t vb_start[2];
+    uint32_t* vb;        /* [qe][qv][stride] */
+    uint64_t vb_words;
+    int vb_error;        /* the reference's "Error in order generation" case */
 } Orc;
 
 static int cmp_u64(const void* a, const void* b) {
@@ -196,6 +205,7 @@ void orc_destroy(void* h) {
     free(o->main);
     free(o->delta);
     free(o->pending);
+    free(o->vb);
     free(o);
 }
 
@@ -216,6 +226,8 @@ int orc_build(void* h, const uint64_t* keys, uint64_t n, uint32_t dv) {
     free(s);
     return 0;
 }
+
+static int test_bit(const uint32_t* m, uint32_t x) { return (m[x >> 5] >> (x & 31)) & 1u; }
 
 /* ---- matching ---- */
 typedef struct {
@@ -250,6 +262,10 @@ static uint64_t dfs(Run* r, uint32_t j) {
             uint32_t c = L->v[t];
             int ok = 1;
             for (uint32_t k = 0; k < j && ok; ++k) ok = (r->m[k] != c);
+            if (ok && o->vb_on == 2) {  /* prune by the valid bits (a sound superset) */
+                const uint32_t stride = (o->dv + 31) / 32;
+                ok = test_bit(o->vb + ((uint64_t)r->ei * o->qv + r->vs[j]) * stride, c);
+            }
             for (uint32_t k = b0 + 1; k < b1 && ok; ++k) {
                 const List *xb, *xa;
                 resolve(r, r->bn_dir[k], r->m[r->bn_pos[k]], &xb, &xa);
@@ -349,6 +365,256 @@ static uint64_t count_batch(Orc* o, const uint8_t* edge_ok, int mode, const uint
     return total;
 }
 
+/* ---- valid bits: BuildLocalIndexBitAll with SUPPORT_MASK_WIDTH 1
+ * (graph_gpu.cu:803-869; indexing.cu:2295-2379), orders and rebuild flags
+ * from plan.cpp:1180-1370 ---- */
+typedef struct {
+    uint8_t vs[ORC_MAXQV];
+    uint8_t off[ORC_MAXQV + 1];
+    uint8_t bni[ORC_MAXQV * ORC_MAXQV];
+} IdxOrder;
+
+static int adj(const Orc* o, uint32_t a, uint32_t b) { return o->eidx[a * ORC_MAXQV + b] != 255; }
+
+/* BuildIndexingOrder (plan.cpp:1180-1230): BFS from (u0, u1), neighbours in
+ * ascending order; backward neighbours of position j = earlier positions
+ * adjacent to vs[j], in position order. */
+static void indexing_order(const Orc* o, uint32_t u0, uint32_t u1, IdxOrder* io) {
+    uint8_t order[ORC_MAXQV], vis[ORC_MAXQV] = {0};
+    uint32_t n = 0, lo = 0;
+    order[n++] = (uint8_t)u0;
+    order[n++] = (uint8_t)u1;
+    vis[u0] = vis[u1] = 1;
+    while (lo < n) {
+        uint32_t hi = n;
+        for (uint32_t i = lo; i < hi; ++i)
+            for (uint32_t w = 0; w < o->qv; ++w)
+                if (adj(o, order[i], w) && !vis[w]) { vis[w] = 1; order[n++] = (uint8_t)w; }
+        lo = hi;
+    }
+    uint32_t k = 0;
+    io->off[0] = 0;
+    io->bni[k++] = 1; /* bni_[0] = 1 (plan.cpp:1213-1215); position 0 has none in use */
+    io->off[1] = 1;
+    io->vs[0] = order[0];
+    for (uint32_t j = 1; j < o->qv; ++j) {
+        io->vs[j] = order[j];
+        for (uint32_t t = 0; t < j; ++t)
+            if (adj(o, order[j], io->vs[t])) io->bni[k++] = (uint8_t)t;
+        io->off[j + 1] = (uint8_t)k;
+    }
+}
+
+/* GenerateRebuildFlagsWithOrder (plan.cpp:1277-1332): every edge on a simple
+ * path from a starting vertex to u0 or u1 (stopping there), plus (u0,u1). */
+static void rebuild_edges(const Orc* o, uint32_t u0, uint32_t u1, const uint32_t* starts, uint8_t* f) {
+    const uint32_t qv = o->qv;
+    memset(f, 0, ORC_MAXQV * ORC_MAXQV);
+    f[u0 * ORC_MAXQV + u1] = f[u1 * ORC_MAXQV + u0] = 1;
+    for (int s = 0; s < 2; ++s) {
+        uint8_t path[ORC_MAXQV + 1], vis[ORC_MAXQV] = {0};
+        uint32_t ci[ORC_MAXQV + 1] = {0};
+        vis[starts[s]] = 1;
+        path[0] = (uint8_t)starts[s];
+        uint32_t depth = 1;
+        for (;;) {
+            /* next neighbour (ascending) of path[depth-1] from index ci[depth] */
+            int advanced = 0;
+            while (1) {
+                uint32_t cnt = 0, nv = 255;
+                for (uint32_t w = 0; w < qv; ++w)
+                    if (adj(o, path[depth - 1], w)) {
+                        if (cnt == ci[depth]) { nv = w; break; }
+                        ++cnt;
+                    }
+                if (nv == 255) break;
+                if (vis[nv]) { ci[depth]++; continue; }
+                if (nv == u0 || nv == u1) {
+                    path[depth] = (uint8_t)nv;
+                    for (uint32_t i = 0; i < depth; ++i) {
+                        f[path[i] * ORC_MAXQV + path[i + 1]] = 1;
+                        f[path[i + 1] * ORC_MAXQV + path[i]] = 1;
+                    }
+                    ci[depth]++;
+                    continue;
+                }
+                vis[nv] = 1;
+                path[depth] = (uint8_t)nv;
+                depth++;
+                advanced = 1;
+                break;
+            }
+            if (advanced) continue;
+            ci[depth] = 0;
+            depth--;
+            if (depth == 0) break;
+            vis[path[depth]] = 0;
+            ci[depth]++;
+        }
+    }
+}
+
+/* GenerateRebuildVFlagsWithOrder (plan.cpp:1334-1370); -1 where the
+ * reference stops with "Error in order generation!". */
+static int rebuild_vertices(const Orc* o, const IdxOrder* io, const uint8_t* f, uint8_t* vf) {
+    memset(vf, 0, ORC_MAXQV);
+    for (uint32_t i = 0; i < o->qv; ++i) {
+        uint32_t u = io->vs[i];
+        if (i == 0) { vf[u] = 1; continue; }
+        uint32_t sum = 0, nb = io->off[i + 1] - io->off[i];
+        for (uint32_t b = io->off[i]; b < io->off[i + 1]; ++b) sum += f[io->vs[io->bni[b]] * ORC_MAXQV + u] ? 1 : 0;
+        if (sum == 0) vf[u] = 0;
+        else if (sum == nb) vf[u] = 1;
+        else return -1;
+    }
+    return 0;
+}
+
+/* SelectStartingEdge (plan.cpp:428-533) from per-direction cardinalities and
+ * average list lengths of the initial index. */
+void orc_starting_edge(void* h, const uint32_t* card, const float* avg, uint32_t* out2) {
+    Orc* o = (Orc*)h;
+    uint32_t sel[ORC_MAXQE], ns = 0, nxt[ORC_MAXQE], nn;
+    uint32_t deg[ORC_MAXQV] = {0};
+    for (uint32_t u = 0; u < o->qv; ++u)
+        for (uint32_t w = 0; w < o->qv; ++w) deg[u] += adj(o, u, w);
+    uint32_t best = 0;
+    for (uint32_t e = 0; e < o->qe; ++e) {
+        uint32_t sd = deg[o->qe_u[e]] + deg[o->qe_v[e]];
+        if (sd > best) { best = sd; ns = 0; sel[ns++] = e; }
+        else if (sd == best) sel[ns++] = e;
+    }
+    if (ns > 1) {
+        uint32_t bt = 0;
+        nn = 0;
+        for (uint32_t i = 0; i < ns; ++i) {
+            uint32_t a = o->qe_u[sel[i]], b = o->qe_v[sel[i]], t = 0;
+            for (uint32_t x = 0; x < o->qv; ++x) t += adj(o, x, a) && adj(o, x, b);
+            if (t > bt) { bt = t; nn = 0; nxt[nn++] = sel[i]; }
+            else if (t == bt) nxt[nn++] = sel[i];
+        }
+        memcpy(sel, nxt, sizeof(sel));
+        ns = nn;
+    }
+    if (ns > 1) {
+        uint32_t bc = UINT32_MAX;
+        nn = 0;
+        for (uint32_t i = 0; i < ns; ++i) {
+            uint32_t c = card[o->eidx[o->qe_u[sel[i]] * ORC_MAXQV + o->qe_v[sel[i]]]];
+            if (c < bc) { bc = c; nn = 0; nxt[nn++] = sel[i]; }
+            else if (c == bc) nxt[nn++] = sel[i];
+        }
+        memcpy(sel, nxt, sizeof(sel));
+        ns = nn;
+    }
+    if (ns > 1) {
+        float bs = 3.402823466e+38f;
+        nn = 0;
+        for (uint32_t i = 0; i < ns; ++i) {
+            uint32_t a = o->qe_u[sel[i]], b = o->qe_v[sel[i]];
+            float sum = 0.0f;
+            for (uint32_t w = 0; w < o->qv; ++w)
+                if (adj(o, a, w) && w != b) sum += avg[o->eidx[a * ORC_MAXQV + w]];
+            for (uint32_t w = 0; w < o->qv; ++w)
+                if (adj(o, b, w) && w != a) sum += avg[o->eidx[b * ORC_MAXQV + w]];
+            if (sum < bs) { bs = sum; nn = 0; nxt[nn++] = sel[i]; }
+            else if (sum == bs) nxt[nn++] = sel[i];
+        }
+        memcpy(sel, nxt, sizeof(sel));
+        ns = nn;
+    }
+    out2[0] = o->qe_u[sel[0]];
+    out2[1] = o->qe_v[sel[0]];
+}
+
+
+static int list_hits(const List* l, const uint32_t* m) {
+    for (uint32_t t = 0; t < l->n; ++t)
+        if (test_bit(m, l->v[t])) return 1;
+    return 0;
+}
+
+static void compute_valid_bits(Orc* o) {
+    const uint32_t stride = (o->dv + 31) / 32, qv = o->qv;
+    o->vb_words = (uint64_t)o->qe * qv * stride;
+    o->vb = (uint32_t*)realloc(o->vb, (o->vb_words ? o->vb_words : 1) * 4);
+    o->vb_error = 0;
+    for (uint32_t ei = 0; ei < o->qe; ++ei) {
+        IdxOrder io;
+        uint8_t f[ORC_MAXQV * ORC_MAXQV], vf[ORC_MAXQV];
+        indexing_order(o, o->qe_u[ei], o->qe_v[ei], &io);
+        rebuild_edges(o, o->qe_u[ei], o->qe_v[ei], o->vb_start, f);
+        if (rebuild_vertices(o, &io, f, vf) < 0) { o->vb_error = 1; return; }
+        uint32_t* M = o->vb + (uint64_t)ei * qv * stride;
+        for (uint32_t u = 0; u < qv; ++u) memset(M + (uint64_t)u * stride, vf[u] ? 0x00 : 0xFF, stride * 4);
+        uint32_t a = io.vs[0], b = io.vs[1];
+        uint32_t i01 = o->eidx[a * ORC_MAXQV + b], i10 = o->eidx[b * ORC_MAXQV + a];
+        for (uint32_t x = 0; x < o->dv; ++x) {
+            if (o->delta[(size_t)i01 * o->dvcap + x].n) M[(uint64_t)a * stride + (x >> 5)] |= 1u << (x & 31);
+            if (o->delta[(size_t)i10 * o->dvcap + x].n) M[(uint64_t)b * stride + (x >> 5)] |= 1u << (x & 31);
+        }
+        for (uint32_t d = 2; d < qv; ++d) {
+            uint32_t u = io.vs[d];
+            if (!vf[u]) continue;
+            uint32_t* out = M + (uint64_t)u * stride;
+            memset(out, 0, stride * 4);
+            for (uint32_t x = 0; x < o->dv; ++x) {
+                int valid = 1;
+                for (uint32_t bp = io.off[d]; bp < io.off[d + 1] && valid; ++bp) {
+                    uint32_t u1 = io.vs[io.bni[bp]];
+                    uint32_t bwd = o->eidx[u * ORC_MAXQV + u1];
+                    const uint32_t* m1 = M + (uint64_t)u1 * stride;
+                    int sat = list_hits(&o->main[(size_t)bwd * o->dvcap + x], m1);
+                    if (!sat && o->dir_to_edge[bwd] <= ei) sat = list_hits(&o->delta[(size_t)bwd * o->dvcap + x], m1);
+                    valid = sat;
+                }
+                if (valid) out[x >> 5] |= 1u << (x & 31);
+            }
+        }
+    }
+}
+
+/* The indexing order and rebuild-vertex flags of query edge ei for the
+ * starting edge (s0, s1), for pinning against the reference planner.
+ * Returns the number of bni entries; *vflags = bit mask, or ~0u on the
+ * reference's "Error in order generation" case. */
+uint32_t orc_indexing_order(void* h, uint32_t ei, uint32_t s0, uint32_t s1, uint8_t* vs, uint8_t* offs,
+                            uint8_t* bni, uint32_t* vflags) {
+    Orc* o = (Orc*)h;
+    IdxOrder io;
+    uint8_t f[ORC_MAXQV * ORC_MAXQV], vf[ORC_MAXQV];
+    uint32_t st[2] = {s0, s1};
+    indexing_order(o, o->qe_u[ei], o->qe_v[ei], &io);
+    rebuild_edges(o, o->qe_u[ei], o->qe_v[ei], st, f);
+    *vflags = 0;
+    if (rebuild_vertices(o, &io, f, vf) < 0) *vflags = ~0u;
+    else
+        for (uint32_t u = 0; u < o->qv; ++u) *vflags |= (uint32_t)vf[u] << u;
+    memcpy(vs, io.vs, o->qv);
+    memcpy(offs, io.off, o->qv + 1);
+    memcpy(bni, io.bni, io.off[o->qv]);
+    return io.off[o->qv];
+}
+
+/* Valid bits are computed for every later matched batch (after its delta
+ * lists, before matching) from the starting edge (s0, s1); on = 0 stops,
+ * on = 2 also prunes the count's candidates by them (soundness check). */
+void orc_set_valid_bits(void* h, int on, uint32_t s0, uint32_t s1) {
+    Orc* o = (Orc*)h;
+    o->vb_on = on;
+    o->vb_start[0] = s0;
+    o->vb_start[1] = s1;
+}
+
+/* Copies the last batch's valid bits ([qe][qv][(dv+31)/32] words) and returns
+ * the word count; UINT64_MAX if the reference would have stopped. */
+uint64_t orc_valid_bits(void* h, uint32_t* out, uint64_t cap) {
+    Orc* o = (Orc*)h;
+    if (o->vb_error) return UINT64_MAX;
+    if (out) memcpy(out, o->vb, (cap < o->vb_words ? cap : o->vb_words) * 4);
+    return o->vb_words;
+}
+
 static void flush_pending(Orc* o) {
     if (!o->n_pending) return;
     uint64_t m;
@@ -399,6 +665,7 @@ uint64_t orc_batch(void* h, uint32_t dv, const uint64_t* ins, uint64_t n_ins, co
             ok[e] = dcount[o->eidx[o->qe_u[e] * ORC_MAXQV + o->qe_v[e]]] &&
                     dcount[o->eidx[o->qe_v[e] * ORC_MAXQV + o->qe_u[e]]];
     }
+    if (o->vb_on) compute_valid_bits(o);
     uint64_t c = count_batch(o, ok, mode, global_order);
     o->pending = (uint64_t*)realloc(o->pending, n_delta * 8);
     memcpy(o->pending, delta, n_delta * 8);

@@ -394,6 +394,26 @@ void cgbref_global_order(void* h, uint8_t* vs) {
     auto* p = (RefPipeline*)h;
     for (uint32_t i = 0; i < p->query.vcount_; ++i) vs[i] = p->plan->global_order_.vs_[i];
 }
+// Indexing order of query edge ei (plan.cpp:1180-1230): vertices, backward
+// neighbour offsets and positions; returns the number of bni_ entries.
+uint32_t cgbref_indexing_order(void* h, uint32_t ei, uint8_t* vs, uint8_t* offs, uint8_t* bni) {
+    auto* p = (RefPipeline*)h;
+    const auto& io = p->plan->indexing_orders_[ei];
+    const uint32_t qv = p->query.vcount_;
+    for (uint32_t i = 0; i < qv; ++i) vs[i] = io.vs_[i];
+    for (uint32_t i = 0; i <= qv; ++i) offs[i] = io.bni_offs_[i];
+    const uint32_t n = io.bni_offs_[qv];
+    for (uint32_t i = 0; i < n; ++i) bni[i] = io.bni_[i];
+    return n;
+}
+// Rebuild vertex flags of query edge ei (plan.cpp:1334-1370) as a bit mask.
+uint32_t cgbref_rebuild_vertices(void* h, uint32_t ei) {
+    auto* p = (RefPipeline*)h;
+    uint32_t m = 0;
+    for (uint32_t u = 0; u < p->query.vcount_; ++u)
+        if (p->plan->rebuild_v_flags_[ei][u]) m |= 1u << u;
+    return m;
+}
 int cgbref_step(void* h) {
     auto* p = (RefPipeline*)h;
     std::streambuf* old = nullptr;

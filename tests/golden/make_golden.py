@@ -16,7 +16,9 @@ synthetic input (cgbdsm_b200/workloads.py):
 
 t_tiny is stored in full as well (inputs, keys in the reference's own
 compressed ids, new->old mapping, final index) so the restatement can be
-replayed from the fixture alone.
+replayed from the fixture alone.  <name>_csr.json holds the same digests for
+the reference's binary CSR input path (labels drawn from rand(), hash-selected
+update stream) on the full graph of <name>.
 """
 from __future__ import annotations
 
@@ -32,11 +34,13 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 
-from cgbdsm_b200.workloads import SPECS, materialize  # noqa: E402
+from cgbdsm_b200.workloads import SPECS, materialize, write_binary_csr  # noqa: E402
 from oracle import bind  # noqa: E402
 
 FULL = ["t_tiny"]
 HASHED = ["t_tiny", "t_er5", "t_er_tree", "t_er_sparse", "t_rmat"]
+# binary CSR inputs (calig.cpp:218-323): workload -> number of vertex classes
+BINARY = {"t_er5": 4, "t_rmat": 10}
 
 
 def to_original(keys: np.ndarray, new2old: np.ndarray) -> np.ndarray:
@@ -103,6 +107,24 @@ def make(name: str, workdir: str) -> None:
     print(name, rec["num_batches"], "batches, counts", [b["count"] for b in rec["batches"]])
 
 
+def make_binary(name: str, nvcls: int, workdir: str) -> None:
+    """The reference reads the CSR prefix and draws labels from rand(), so it
+    runs in a fresh process (oracle/refdigest.py)."""
+    import subprocess
+
+    spec = SPECS[name]
+    p = write_binary_csr(spec, workdir, nvcls)
+    r = subprocess.run([sys.executable, "-m", "oracle.refdigest", p["query"], p["data"], "-",
+                        str(spec.cli_batch_size)], capture_output=True, text=True, check=True, cwd=ROOT)
+    rec = json.loads(r.stdout.strip().splitlines()[-1])
+    rec = {"workload": name, "spec": repr(spec), "nvcls": nvcls,
+           "inputs": {s: file_digest(p["data"] + s) for s in (".meta.txt", ".vertex.bin", ".edge.bin")}, **rec}
+    with open(os.path.join(HERE, f"{name}_csr.json"), "w") as f:
+        json.dump(rec, f, indent=1)
+        f.write("\n")
+    print(name, "binary CSR,", rec["num_batches"], "batches, counts", [b["count"] for b in rec["batches"]])
+
+
 def main() -> None:
     bind.build(ref=True)
     if not bind.have_ref():
@@ -110,6 +132,8 @@ def main() -> None:
     with tempfile.TemporaryDirectory() as d:
         for name in HASHED:
             make(name, d)
+        for name, nvcls in BINARY.items():
+            make_binary(name, nvcls, d)
 
 
 if __name__ == "__main__":

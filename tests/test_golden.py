@@ -5,7 +5,9 @@ reference's own CPU path) replayed without the reference tree:
   * the restatement (oracle/oracle.c) replays t_tiny from the stored keys,
   * the product's producer emits the reference's key multisets, and the
     restatement on those keys gives the reference's counts and final index,
-  * (GPU) the engine on the producer's keys gives the same counts and index.
+  * (GPU) the engine on the producer's keys gives the same counts and index,
+
+for the text inputs and for the reference's binary CSR input path (<name>_csr).
 """
 import hashlib
 import json
@@ -15,11 +17,12 @@ import numpy as np
 import pytest
 
 from cgbdsm_b200 import Producer
-from cgbdsm_b200.workloads import SPECS, materialize, read_query
+from cgbdsm_b200.workloads import SPECS, materialize, read_query, write_binary_csr
 from oracle import bind
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 NAMES = ["t_tiny", "t_er5", "t_er_tree", "t_er_sparse", "t_rmat"]
+BINARY = ["t_er5_csr", "t_rmat_csr"]
 
 
 def load(name):
@@ -49,6 +52,25 @@ def test_generator_reproduces_golden_inputs(name, workdir):
         assert hashlib.sha256(open(p[k], "rb").read()).hexdigest() == h, f"{name}: {k} input differs"
 
 
+@pytest.mark.parametrize("name", BINARY)
+def test_csr_writer_reproduces_golden_inputs(name, workdir):
+    g = load(name)
+    p = write_binary_csr(SPECS[g["workload"]], workdir, g["nvcls"])
+    for suffix, h in g["inputs"].items():
+        assert hashlib.sha256(open(p["data"] + suffix, "rb").read()).hexdigest() == h, f"{name}: {suffix} differs"
+
+
+def _inputs(name, workdir):
+    """(fixture, query, data, update) of a text or binary golden workload."""
+    g = load(name)
+    spec = SPECS[g["workload"]]
+    if "nvcls" in g:
+        p = write_binary_csr(spec, workdir, g["nvcls"])
+        return g, spec, p["query"], p["data"], "-"
+    p = materialize(spec, workdir)
+    return g, spec, p["query"], p["data"], p["update"]
+
+
 def test_restatement_replays_full_fixture():
     z = np.load(os.path.join(GOLDEN, "t_tiny_full.npz"))
     q = z["file_query"].tobytes().decode()
@@ -74,11 +96,9 @@ def test_restatement_replays_full_fixture():
 
 def _producer_batches(name, workdir):
     """Runs the product's producer over the workload and checks every key
-    multiset against the fixture; yields the batches for replay."""
-    g = load(name)
-    spec = SPECS[name]
-    p = materialize(spec, workdir)
-    prod = Producer(p["query"], p["data"], p["update"], spec.cli_batch_size)
+    multiset against the fixture; returns the batches for replay."""
+    g, spec, query, data, update = _inputs(name, workdir)
+    prod = Producer(query, data, update, spec.cli_batch_size)
     assert prod.num_batches == g["num_batches"]
     init, dv0 = prod.initial()
     assert dv0 == g["dv_initial"]
@@ -95,11 +115,11 @@ def _producer_batches(name, workdir):
         batches.append(r)
     n2o = prod.new2old()
     prod.close()
-    ql, qe = read_query(p["query"])
+    ql, qe = read_query(query)
     return g, (init, dv0), batches, n2o, (ql, qe)
 
 
-@pytest.mark.parametrize("name", NAMES)
+@pytest.mark.parametrize("name", NAMES + BINARY)
 def test_producer_and_restatement_match_golden(name, workdir):
     g, (init, dv0), batches, n2o, (ql, qe) = _producer_batches(name, workdir)
     o = bind.Oracle(len(ql), qe)
@@ -111,7 +131,7 @@ def test_producer_and_restatement_match_golden(name, workdir):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("name", NAMES)
+@pytest.mark.parametrize("name", NAMES + BINARY)
 def test_engine_matches_golden(name, workdir):
     from cgbdsm_b200 import Engine
 

@@ -10,7 +10,8 @@ import numpy as np
 import pytest
 
 from cgbdsm_b200 import CgbError, Engine
-from cgbdsm_b200.engine import FLAG_ENUMERATE_TAIL, FLAG_FORCE_SPLIT
+from cgbdsm_b200.engine import (FLAG_ENUMERATE_TAIL, FLAG_FORCE_SPLIT, FLAG_MASK_PRUNE, FLAG_NO_TAIL_CACHE,
+                                FLAG_VALID_BITS)
 from cgbdsm_b200.workloads import SPECS, materialize, read_query
 from oracle import bind
 
@@ -23,8 +24,10 @@ def _key(d, u, v):
     return (np.uint64(d) << np.uint64(59)) | (np.uint64(u) << np.uint64(32)) | np.uint64(v)
 
 
-@pytest.mark.parametrize("flags", [0, FLAG_ENUMERATE_TAIL, FLAG_FORCE_SPLIT | FLAG_ENUMERATE_TAIL, FLAG_FORCE_SPLIT],
-                         ids=["counted_tail", "enumerated_tail", "stolen_enumerated", "stolen_counted"])
+@pytest.mark.parametrize("flags", [0, FLAG_ENUMERATE_TAIL, FLAG_FORCE_SPLIT | FLAG_ENUMERATE_TAIL, FLAG_FORCE_SPLIT,
+                                   FLAG_NO_TAIL_CACHE],
+                         ids=["counted_tail", "enumerated_tail", "stolen_enumerated", "stolen_counted",
+                              "counted_no_prefix_cache"])
 @pytest.mark.parametrize("name", PIPELINE_CASES)
 def test_engine_matches_reference_cpu_path(name, flags, workdir):
     if not bind.have_ref():
@@ -215,4 +218,45 @@ def test_seed_shards_sum_to_full_count(name, workdir):
         assert np.array_equal(e.read_index(), idx)
         e.close()
     full.close()
+    ref.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["t_tiny", "t_er5", "t_er_sparse", "t_er_tree", "t_rmat"])
+def test_valid_bits_match_restatement(name, workdir):
+    """Valid bits (BuildLocalIndexBitAll) equal the restatement's word for word
+    after every matched batch; the starting edge equals the reference
+    planner's; pruning the matcher by them leaves every count unchanged."""
+    if not bind.have_ref():
+        pytest.skip("oracle/_ref/libcgbref.so not built")
+    spec = SPECS[name]
+    p = materialize(spec, workdir)
+    ref = bind.RefPipeline(p["query"], p["data"], p["update"], spec.cli_batch_size)
+    ql, qe = read_query(p["query"])
+    o = bind.Oracle(len(ql), qe)
+    go = ref.global_order()
+    start = o.starting_edge(ref.cardinalities(), ref.avg_degrees())
+    o.set_valid_bits(1, start)
+    init = ref.init_keys()
+    o.build(init, ref.dv_count)
+    engs = []
+    for flags in (FLAG_VALID_BITS, FLAG_MASK_PRUNE):
+        e = Engine(flags=flags)
+        e.load_query(len(ql), qe, ql)
+        e.build_index(init, ref.dv_count)
+        assert e.starting_edge() == start == (int(go[0]), int(go[1]))
+        engs.append(e)
+    matched = 0
+    while ref.step() >= 0:
+        r = ref.last()
+        co = o.batch(r["dv"], r["ins"], r["del"], r["delta"], None, bind.PER_EDGE)
+        for e in engs:
+            assert e.apply_batch(r["dv"], r["ins"], r["del"], r["delta"], r["edge_ok"]) == r["count"] == co
+        if len(r["delta"]):
+            matched += 1
+            want = o.valid_bits()
+            for e in engs:
+                got, ms = e.valid_bits()
+                assert np.array_equal(got, want), f"{name}: valid bits differ"
+    assert matched > 0
     ref.close()
