@@ -443,9 +443,15 @@ __device__ unsigned long long tail_count_warp(const EdgePlan& P, const uint32_t*
 // in the set, and intersects the subsets with lists at position j per
 // candidate.
 constexpr unsigned long long kDynamic = ~0ull;
+constexpr uint32_t kClean = 0xffu;  // tail cache up to date
 
+// Recounts only the entries that depend on a position >= dirty (the shallowest
+// position whose vertex changed since the last call): an entry's count
+// depends on the positions of its lists' backward neighbours and of the
+// excluded core vertices, so e.g. a subset hanging off positions 0 and 1
+// is counted once per (m[0], m[1]), not once per prefix.
 __device__ void tail_prepare(const EdgePlan& P, const uint32_t* m, uint4* bn, unsigned long long* cache,
-                             const uint4* rec, uint32_t dvcap, const uint32_t* __restrict__ pool,
+                             uint32_t dirty, const uint4* rec, uint32_t dvcap, const uint32_t* __restrict__ pool,
                              const uint32_t* __restrict__ dval, uint32_t lane, unsigned long long& bytes) {
     const uint32_t nc = P.n_core, n = P.n, j = nc - 1;
     for (uint32_t k = P.bn_off[nc] + lane; k < P.bn_off[n]; k += 32) {
@@ -463,17 +469,19 @@ __device__ void tail_prepare(const EdgePlan& P, const uint32_t* m, uint4* bn, un
         const uint32_t k = e - t;
         for (uint32_t mask = 1; mask < (1u << k); ++mask) {
             uint8_t ids[kMaxBN];
-            uint32_t nl = 0;
+            uint32_t nl = 0, dep = 0;
             bool dynamic = false;
             for (uint32_t i = 0; i < k; ++i)
                 if (mask & (1u << i))
                     for (uint32_t q = P.bn_off[t + i]; q < P.bn_off[t + i + 1]; ++q) {
                         ids[nl++] = (uint8_t)q;
                         dynamic |= P.bn_pos[q] == j;
+                        dep = max(dep, (uint32_t)P.bn_pos[q]);
                     }
-            const unsigned long long v =
-                dynamic ? kDynamic
-                        : isect_count(bn, ids, nl, m, P.excl[t] & ((1u << j) - 1u), pool, dval, lane, bytes);
+            const uint32_t ex = P.excl[t] & ((1u << j) - 1u);
+            if (ex) dep = max(dep, 31u - __clz(ex));
+            if (!dynamic && dep < dirty) continue;  // still valid
+            const unsigned long long v = dynamic ? kDynamic : isect_count(bn, ids, nl, m, ex, pool, dval, lane, bytes);
             if (lane == 0) cache[t * 8 + mask] = v;
         }
         t = e;
@@ -620,7 +628,7 @@ __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
     uint32_t split_tick = 0;  // waiting warps are checked for every 4th chunk
     bool out_of_time = false;
     uint32_t ticket = kNoTicket;  // lane 0: ticket of the task ring this warp waits on
-    bool tail_ready = false;
+    uint32_t dirty = 0;  // shallowest position changed since the tail cache was filled (kClean: none)
     unsigned long long tail_const = 0;  // tail count of the current prefix (plans with tail_const)
     uint32_t idle_spins = 0;
 
@@ -729,9 +737,9 @@ __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
             }
             if (lane == j) { st_ncand = 0; st_pos = 0; st_next = 0; st_len = nb ? best : 0; st_gen = bl; }
             __syncwarp();
-            if (j == nc - 1) tail_ready = false;  // prefix changed: cached tail counts are stale
         };
 
+        dirty = 0;  // new unit: every cached tail count is stale
         setup(jbase);
         if (kind == 2 && lane == jbase) { st_gen = tgen; st_next = tlo; st_len = thi; }
         __syncwarp();
@@ -749,6 +757,7 @@ __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
                 if (lane == j) st_pos = pos + 1;
                 if (lane == 0) m[j] = s_cand[w][j][pos] & kCandMask;
                 __syncwarp();
+                dirty = min(dirty, j);
                 ++j;
                 setup(j);
                 continue;
@@ -880,10 +889,10 @@ __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
                         // the tail count depends on the prefix only: one value per prefix
                         const uint32_t bal = __ballot_sync(kFull, ok);
                         if (bal) {
-                            if (!tail_ready) {
-                                tail_prepare(P, m, bn, s_tc[w], a.rec, a.dvcap, a.pool, a.dval, lane, n_bytes);
+                            if (dirty != kClean) {
+                                tail_prepare(P, m, bn, s_tc[w], dirty, a.rec, a.dvcap, a.pool, a.dval, lane, n_bytes);
                                 tail_const = tail_const_value(P, s_tc[w]);
-                                tail_ready = true;
+                                dirty = kClean;
                             }
                             if (lane == 0) { cnt += (unsigned long long)__popc(bal) * tail_const; n_tail += __popc(bal); }
                         }
@@ -894,10 +903,10 @@ __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
                             const int l = __ffs(bal) - 1;
                             bal &= bal - 1;
                             const uint32_t cl = __shfl_sync(kFull, c, l);
-                            if (!tail_ready && a.tail_cache) {
-                                // first embedding of this prefix: count the prefix-only subsets once
-                                tail_prepare(P, m, bn, s_tc[w], a.rec, a.dvcap, a.pool, a.dval, lane, n_bytes);
-                                tail_ready = true;
+                            if (dirty != kClean && a.tail_cache) {
+                                // first embedding since the prefix changed: recount the stale prefix-only subsets
+                                tail_prepare(P, m, bn, s_tc[w], dirty, a.rec, a.dvcap, a.pool, a.dval, lane, n_bytes);
+                                dirty = kClean;
                             }
                             if (lane == 0) m[j] = cl;
                             __syncwarp();
