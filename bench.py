@@ -48,6 +48,20 @@ def _peaks():
         return 6650.0, "fallback"
 
 
+def _profiled_traffic(kernel: str):
+    """DRAM bytes (read + write) of one launch of `kernel` on this workload, from
+    the committed ncu summary (profiles/<kernel>_rmat1m10m.md, a line
+    "traffic_bytes_per_launch: N"); None when there is no such capture."""
+    import re
+
+    path = os.path.join(ROOT, "profiles", f"{kernel}_rmat1m10m.md")
+    try:
+        m = re.search(r"traffic_bytes_per_launch:\s*(\d+)", open(path).read())
+        return (int(m.group(1)), os.path.relpath(path, ROOT)) if m else (None, None)
+    except OSError:
+        return None, None
+
+
 class ClockSampler:
     """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
 
@@ -225,6 +239,7 @@ def run_ours(args) -> None:
         kname, kbytes, kms = "k_dfs_count (matching)", match_bytes, match_ms
     else:
         kname, kbytes, kms = "k_merge_runs (index update)", upd_bytes, upd_ms
+    traffic, traffic_src = _profiled_traffic(kname.split()[0])
     achieved = (kbytes / 1e9) / (kms / 1e3) if kms > 0 else 0.0
     upd_achieved = (upd_bytes / 1e9) / (upd_ms / 1e3) if upd_ms > 0 else 0.0
     lat = sorted(step_ms)
@@ -259,7 +274,8 @@ def run_ours(args) -> None:
         "gpu_launches": launches,
         "roofline": {"kernel": kname, "bound": "hbm", "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak if peak else None, "peak_source": peak_kind,
-                     "algorithmic_bytes_per_step": kbytes / len(recs), "traffic": None,
+                     "algorithmic_bytes_per_step": kbytes / len(recs), "traffic": traffic,
+                     "traffic_source": traffic_src,
                      "index_update_achieved_gbs": upd_achieved},
         "clocks": clk.summary(),
         "stage1_setup_s": round(s1_s, 2),

@@ -77,13 +77,17 @@ __device__ __forceinline__ uint64_t pack_duv(uint32_t d, uint32_t u, uint32_t v,
 // Edits: ((d,u,v) << 1) | op, op 0 = add, 1 = remove.  Keys whose direction
 // or vertex ids are out of range raise error bit 1 and become the all-ones
 // marker, which sorts last and is skipped by the merge.
+// Added keys with u == v (a self-loop in the data graph) set the sticky
+// self_seen flag: until one appears no vertex lies in its own lists, which
+// lets the matcher skip those exclusion tests.
 __global__ void k_pack_edits(const uint64_t* __restrict__ in, uint64_t n, uint32_t op, PackInfo pi,
-                             uint64_t* __restrict__ out, unsigned int* err) {
+                             uint64_t* __restrict__ out, unsigned int* err, unsigned int* self_seen) {
     uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
     for (; i < n; i += stride) {
         uint32_t d, u, v;
         if (decode_ext(in[i], pi, d, u, v)) {
+            if (op == 0 && u == v) atomicOr(self_seen, 1u);
             out[i] = (pack_duv(d, u, v, pi.B) << 1) | op;
         } else {
             out[i] = ~0ull;
@@ -93,12 +97,13 @@ __global__ void k_pack_edits(const uint64_t* __restrict__ in, uint64_t n, uint32
 }
 
 __global__ void k_pack_delta(const uint64_t* __restrict__ in, uint64_t n, PackInfo pi,
-                             uint64_t* __restrict__ out, unsigned int* err) {
+                             uint64_t* __restrict__ out, unsigned int* err, unsigned int* self_seen) {
     uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
     for (; i < n; i += stride) {
         uint32_t d, u, v;
         if (decode_ext(in[i], pi, d, u, v)) {
+            if (u == v) atomicOr(self_seen, 1u);
             out[i] = pack_duv(d, u, v, pi.B);
         } else {
             out[i] = ~0ull;
@@ -307,6 +312,7 @@ struct DfsArgs {
     uint32_t shard, num_shards;  // this engine expands seeds i with i % num_shards == shard
     uint32_t steal;              // share long shallow ranges through the queue
     uint32_t tail_cache;         // count prefix-only tail subsets once per prefix
+    const unsigned int* self_seen;  // sticky self-loop flag (see k_pack_edits)
     const uint32_t* vb;          // valid bits [qe][qv][vb_stride] or nullptr (no pruning)
     uint32_t vb_stride;
     uint32_t qv;
@@ -357,7 +363,10 @@ __device__ unsigned long long isect_count(const uint4* bn, const uint8_t* ids, u
         const uint4 r = bn[ids[0]];
         bool in = false;
         if (lane < 16 && ((excl >> lane) & 1u)) {
-            in = list_contains(pool, dval, r, m[lane]);
+            // a vertex held by two positions (a self-loop seed edge) is excluded once
+            bool dup = false;
+            for (uint32_t e = excl & ((1u << lane) - 1u); e; e &= e - 1) dup |= m[__ffs(e) - 1] == m[lane];
+            if (!dup) in = list_contains(pool, dval, r, m[lane]);
             bytes += 32u * (33u - __clz(r.y | 1u));
         }
         return (unsigned long long)(r.y + r.w) - __popc(__ballot_sync(kFull, in));
@@ -388,6 +397,14 @@ __device__ unsigned long long isect_count(const uint4* bn, const uint8_t* ids, u
     return c;
 }
 
+// Positions owning the lists bn[ids[0..nl)]: without self-loops a matched
+// vertex never lies in its own lists, so excluding it needs no test.
+__device__ __forceinline__ uint32_t owner_mask(const EdgePlan& P, const uint8_t* ids, uint32_t nl) {
+    uint32_t o = 0;
+    for (uint32_t i = 0; i < nl; ++i) o |= 1u << P.bn_pos[ids[i]];
+    return o;
+}
+
 // Injective assignments of a label group of k <= 3 tail vertices from the
 // sizes sc[mask] of the intersections of its members' candidate sets
 // (inclusion-exclusion over coinciding members).
@@ -403,7 +420,7 @@ __device__ __forceinline__ unsigned long long group_count(const unsigned long lo
 // excluded); groups multiply.  Warp-cooperative, warp-uniform result.
 __device__ unsigned long long tail_count_warp(const EdgePlan& P, const uint32_t* m, uint4* bn, const uint4* rec,
                                               uint32_t dvcap, const uint32_t* __restrict__ pool,
-                                              const uint32_t* __restrict__ dval, uint32_t lane,
+                                              const uint32_t* __restrict__ dval, bool self_loops, uint32_t lane,
                                               unsigned long long& bytes) {
     const uint32_t nc = P.n_core, n = P.n;
     // resolve every tail BN record once
@@ -427,7 +444,8 @@ __device__ unsigned long long tail_count_warp(const EdgePlan& P, const uint32_t*
             for (uint32_t i = 0; i < k; ++i)
                 if (mask & (1u << i))
                     for (uint32_t q = P.bn_off[t + i]; q < P.bn_off[t + i + 1]; ++q) ids[nl++] = (uint8_t)q;
-            sc[mask] = isect_count(bn, ids, nl, m, P.excl[t], pool, dval, lane, bytes);
+            const uint32_t ex = P.excl[t] & ~(self_loops ? 0u : owner_mask(P, ids, nl));
+            sc[mask] = isect_count(bn, ids, nl, m, ex, pool, dval, lane, bytes);
         }
         prod *= group_count(sc, k);
         t = e;
@@ -452,7 +470,8 @@ constexpr uint32_t kClean = 0xffu;  // tail cache up to date
 // is counted once per (m[0], m[1]), not once per prefix.
 __device__ void tail_prepare(const EdgePlan& P, const uint32_t* m, uint4* bn, unsigned long long* cache,
                              uint32_t dirty, const uint4* rec, uint32_t dvcap, const uint32_t* __restrict__ pool,
-                             const uint32_t* __restrict__ dval, uint32_t lane, unsigned long long& bytes) {
+                             const uint32_t* __restrict__ dval, bool self_loops, uint32_t lane,
+                             unsigned long long& bytes) {
     const uint32_t nc = P.n_core, n = P.n, j = nc - 1;
     for (uint32_t k = P.bn_off[nc] + lane; k < P.bn_off[n]; k += 32) {
         if (P.bn_pos[k] >= j) continue;
@@ -478,7 +497,7 @@ __device__ void tail_prepare(const EdgePlan& P, const uint32_t* m, uint4* bn, un
                         dynamic |= P.bn_pos[q] == j;
                         dep = max(dep, (uint32_t)P.bn_pos[q]);
                     }
-            const uint32_t ex = P.excl[t] & ((1u << j) - 1u);
+            const uint32_t ex = P.excl[t] & ((1u << j) - 1u) & ~(self_loops ? 0u : owner_mask(P, ids, nl));
             if (ex) dep = max(dep, 31u - __clz(ex));
             if (!dynamic && dep < dirty) continue;  // still valid
             const unsigned long long v = dynamic ? kDynamic : isect_count(bn, ids, nl, m, ex, pool, dval, lane, bytes);
@@ -493,7 +512,7 @@ __device__ void tail_prepare(const EdgePlan& P, const uint32_t* m, uint4* bn, un
 __device__ unsigned long long tail_eval(const EdgePlan& P, const uint32_t* m, uint4* bn,
                                         const unsigned long long* cache, const uint4* rec, uint32_t dvcap,
                                         const uint32_t* __restrict__ pool, const uint32_t* __restrict__ dval,
-                                        uint32_t lane, unsigned long long& bytes) {
+                                        bool self_loops, uint32_t lane, unsigned long long& bytes) {
     const uint32_t nc = P.n_core, n = P.n, j = nc - 1;
     const uint32_t c = m[j];
     for (uint32_t k = P.bn_off[nc] + lane; k < P.bn_off[n]; k += 32) {
@@ -529,7 +548,8 @@ __device__ unsigned long long tail_eval(const EdgePlan& P, const uint32_t* m, ui
                 }
                 sc[mask] = cv - (__all_sync(kFull, in) ? 1ull : 0ull);
             } else {
-                sc[mask] = isect_count(bn, ids, nl, m, P.excl[t], pool, dval, lane, bytes);
+                const uint32_t ex = P.excl[t] & ~(self_loops ? 0u : owner_mask(P, ids, nl));
+                sc[mask] = isect_count(bn, ids, nl, m, ex, pool, dval, lane, bytes);
             }
         }
         prod *= group_count(sc, k);
@@ -563,8 +583,8 @@ __device__ __forceinline__ unsigned long long warp_sum(unsigned long long x) {
 // generator << 16, w1/w2 = [lo, hi) of the generator list, w3 = ready tag,
 // w4..15 = the matched prefix.  A warp without a seed takes one ticket
 // (atomicAdd on the ticket counter) and waits for task number `ticket`;
-// tasks are reserved in ticket order, so every task has exactly one
-// consumer and idle warps never contend.  While tickets outnumber reserved
+// tasks are numbered by an atomicAdd in the same order, so every task has
+// exactly one consumer and neither side contends on a CAS.  While tickets outnumber reserved
 // tasks, a busy warp publishes all the work it has not started at its
 // shallowest level (top of its stack), so the biggest remaining subtrees
 // move first.  Termination: a warp leaves when completed == seeds + reserved
@@ -606,6 +626,7 @@ __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
 
     const uint32_t lane = threadIdx.x & 31;
     const uint32_t w = threadIdx.x >> 5;
+    const bool self_loops = *(const volatile unsigned int*)a.self_seen != 0;
     if (threadIdx.x <= a.qe) s_pre[threadIdx.x] = a.seed_pre[threadIdx.x];
     if (threadIdx.x < a.qe) s_lo[threadIdx.x] = a.seed_lo[threadIdx.x];
     __syncthreads();
@@ -709,7 +730,7 @@ __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
         const bool has_tail = nc < P.n;
         if (kind == 1 && nc == 2) {  // the seed edge alone is the core: only the tail remains
             const unsigned long long tc =
-                (P.n == 2) ? 1ull : tail_count_warp(P, m, bn, a.rec, a.dvcap, a.pool, a.dval, lane, n_bytes);
+                (P.n == 2) ? 1ull : tail_count_warp(P, m, bn, a.rec, a.dvcap, a.pool, a.dval, self_loops, lane, n_bytes);
             if (lane == 0) { cnt += tc; ++n_tail; }
             __syncwarp();
             if (lane == 0) add_release((unsigned int*)&a.qctr[3], 1u);
@@ -783,12 +804,13 @@ __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
                         const uint32_t hb = __ballot_sync(kFull, has);
                         uint32_t slot = 0xffffffffu;
                         if (hb && lane == 0) {
-                            // reserve the next ticket while it is (or, under force_split, soon
-                            // may be) waited for; the ring never laps its head
+                            // reserve the next task number while tickets wait for one (always, under
+                            // force_split).  atomicAdd never fails, so concurrent producers may
+                            // overshoot the demand by a few tasks; those wait in the ring for the
+                            // next idle warps, and the slack keeps the ring from lapping its head.
                             const unsigned int t = vq[0], hd = vq[1];
-                            if ((a.force_split || (int)(hd - t) > 0) && (int)(t - hd) < (int)(a.task_cap - kTaskSlack) &&
-                                atomicCAS((unsigned int*)&a.qctr[0], t, t + 1) == t)
-                                slot = t;
+                            if ((a.force_split || (int)(hd - t) > 0) && (int)(t - hd) < (int)(a.task_cap - kTaskSlack))
+                                slot = atomicAdd((unsigned int*)&a.qctr[0], 1u);
                         }
                         slot = __shfl_sync(kFull, slot, 0);
                         if (slot != 0xffffffffu) {
@@ -890,7 +912,7 @@ __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
                         const uint32_t bal = __ballot_sync(kFull, ok);
                         if (bal) {
                             if (dirty != kClean) {
-                                tail_prepare(P, m, bn, s_tc[w], dirty, a.rec, a.dvcap, a.pool, a.dval, lane, n_bytes);
+                                tail_prepare(P, m, bn, s_tc[w], dirty, a.rec, a.dvcap, a.pool, a.dval, self_loops, lane, n_bytes);
                                 tail_const = tail_const_value(P, s_tc[w]);
                                 dirty = kClean;
                             }
@@ -905,15 +927,17 @@ __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
                             const uint32_t cl = __shfl_sync(kFull, c, l);
                             if (dirty != kClean && a.tail_cache) {
                                 // first embedding since the prefix changed: recount the stale prefix-only subsets
-                                tail_prepare(P, m, bn, s_tc[w], dirty, a.rec, a.dvcap, a.pool, a.dval, lane, n_bytes);
+                                tail_prepare(P, m, bn, s_tc[w], dirty, a.rec, a.dvcap, a.pool, a.dval, self_loops, lane, n_bytes);
                                 dirty = kClean;
                             }
                             if (lane == 0) m[j] = cl;
                             __syncwarp();
                             const unsigned long long tc =
                                 a.tail_cache
-                                    ? tail_eval(P, m, bn, s_tc[w], a.rec, a.dvcap, a.pool, a.dval, lane, n_bytes)
-                                    : tail_count_warp(P, m, bn, a.rec, a.dvcap, a.pool, a.dval, lane, n_bytes);
+                                    ? tail_eval(P, m, bn, s_tc[w], a.rec, a.dvcap, a.pool, a.dval, self_loops, lane,
+                                                n_bytes)
+                                    : tail_count_warp(P, m, bn, a.rec, a.dvcap, a.pool, a.dval, self_loops, lane,
+                                                      n_bytes);
                             if (lane == 0) { cnt += tc; ++n_tail; }
                             __syncwarp();
                         }
@@ -1120,6 +1144,7 @@ struct cgb_handle {
     unsigned long long pool_cap = 0;
     // device scalars: [0] pool_top, [1] live_words, [2] err, [3] work_next
     unsigned long long* d_scal = nullptr;
+    unsigned int* d_self = nullptr;  // sticky: some added key was a self-loop (u == v)
     unsigned long long* h_scal = nullptr;  // pinned mirror (4 scalars + counts)
     unsigned long long h_pool_top = 0;
     long long h_live = 0;
@@ -1370,9 +1395,9 @@ cgb_status apply_edits(cgb_handle* h, const uint64_t* adds0, uint64_t n0, const 
     if ((s = ensure_edit_buffers(h, n)) != CGB_OK) return s;
     PackInfo pi{bits_for(h->dv), h->nd, h->dv};
     unsigned int* d_err = (unsigned int*)(h->d_scal + 2);
-    if (n0) { k_pack_edits<<<grid_for(h, n0), 256, 0, h->stream>>>(adds0, n0, 0, pi, h->d_edits, d_err); LAUNCHED(); }
-    if (n1) { k_pack_edits<<<grid_for(h, n1), 256, 0, h->stream>>>(adds1, n1, 0, pi, h->d_edits + n0, d_err); LAUNCHED(); }
-    if (n2) { k_pack_edits<<<grid_for(h, n2), 256, 0, h->stream>>>(rems, n2, 1, pi, h->d_edits + n0 + n1, d_err); LAUNCHED(); }
+    if (n0) { k_pack_edits<<<grid_for(h, n0), 256, 0, h->stream>>>(adds0, n0, 0, pi, h->d_edits, d_err, h->d_self); LAUNCHED(); }
+    if (n1) { k_pack_edits<<<grid_for(h, n1), 256, 0, h->stream>>>(adds1, n1, 0, pi, h->d_edits + n0, d_err, h->d_self); LAUNCHED(); }
+    if (n2) { k_pack_edits<<<grid_for(h, n2), 256, 0, h->stream>>>(rems, n2, 1, pi, h->d_edits + n0 + n1, d_err, h->d_self); LAUNCHED(); }
     CK(cudaGetLastError());
     // valid keys use 2B+6 bits; one more bit makes the all-ones invalid marker sort last
     if ((s = radix_sort(h, h->d_edits, h->d_edits_alt, n, 2 * (int)pi.B + 7)) != CGB_OK) return s;
@@ -1451,6 +1476,8 @@ cgb_status cgb_create(const cgb_config* cfg, cgb_handle** out) {
     h->own_stream = true;
     CKC(cudaMalloc(&h->d_scal, 4 * sizeof(unsigned long long)));
     CKC(cudaMemset(h->d_scal, 0, 4 * sizeof(unsigned long long)));
+    CKC(cudaMalloc(&h->d_self, sizeof(unsigned int)));
+    CKC(cudaMemset(h->d_self, 0, sizeof(unsigned int)));
     CKC(cudaMallocHost(&h->h_scal, (12 + kMaxQE) * sizeof(unsigned long long)));
     CKC(cudaMalloc(&h->d_num_runs, 2 * sizeof(int)));
     CKC(cudaMalloc(&h->d_seed, (3 * kMaxQE + 2) * sizeof(uint32_t)));
@@ -1471,10 +1498,11 @@ void cgb_destroy(cgb_handle* h) {
     if (!h) return;
     cudaSetDevice(h->device);
     if (h->stream) cudaStreamSynchronize(h->stream);
-    void* ptrs[] = {h->rec, h->pool, h->pool_alt, h->d_scal, h->d_keys_in, h->d_pending, h->d_edits,
+    void* ptrs[] = {h->rec, h->pool, h->pool_alt, h->d_scal, h->d_self, h->d_keys_in, h->d_pending, h->d_edits,
                     h->d_edits_alt, h->d_du, h->d_run_du, h->d_run_len, h->d_run_off, h->d_num_runs,
                     h->d_dkeys, h->d_dkeys_alt, h->d_dval, h->d_ddu, h->d_drun_du, h->d_drun_len, h->d_drun_off,
-                    h->d_seed, h->d_counts, h->d_stats, h->d_tasks, h->d_qctr, h->d_temp, h->d_qe_dirs, h->d_edge_ok};
+                    h->d_seed, h->d_counts, h->d_stats, h->d_tasks, h->d_qctr, h->d_temp, h->d_qe_dirs, h->d_edge_ok,
+                    h->d_vb};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (h->h_scal) cudaFreeHost(h->h_scal);
@@ -1614,7 +1642,7 @@ cgb_status cgb_apply_batch_device(cgb_handle* h, uint32_t dv_count, const uint64
     if (match) {
         if ((s = ensure_delta_buffers(h, n_delta)) != CGB_OK) return s;
         uint32_t* du = h->d_ddu;
-        k_pack_delta<<<grid_for(h, n_delta), 256, 0, h->stream>>>(delta, n_delta, pi, h->d_dkeys, d_err);
+        k_pack_delta<<<grid_for(h, n_delta), 256, 0, h->stream>>>(delta, n_delta, pi, h->d_dkeys, d_err, h->d_self);
         LAUNCHED();
         if ((s = radix_sort(h, h->d_dkeys, h->d_dkeys_alt, n_delta, 2 * (int)B + 6)) != CGB_OK) return s;
         k_delta_values<<<grid_for(h, n_delta), 256, 0, h->stream>>>(h->d_dkeys, n_delta, (1ull << B) - 1, h->d_dval);
@@ -1683,6 +1711,7 @@ cgb_status cgb_apply_batch_device(cgb_handle* h, uint32_t dv_count, const uint64
         da.steal = (h->cfg.flags & CGB_FLAG_NO_STEAL) ? 0u : 1u;
         da.tail_cache = (h->cfg.flags & CGB_FLAG_NO_TAIL_CACHE) ? 0u : 1u;
         da.shard = h->cfg.shard_index < da.num_shards ? h->cfg.shard_index : 0u;
+        da.self_seen = h->d_self;
         da.vb = (h->cfg.flags & CGB_FLAG_MASK_PRUNE) ? h->d_vb : nullptr;
         da.vb_stride = h->vb_stride;
         da.qv = h->q.qv;

@@ -79,6 +79,18 @@ def _sym_keys(orc, pairs_by_edge):
 
 @pytest.mark.parametrize("seed", range(8))
 def test_random_symmetric_streams(seed):
+    _random_stream(seed, 0.0)
+
+
+@pytest.mark.parametrize("seed", range(4))
+def test_random_streams_with_self_loops(seed):
+    """Self-loop keys (x, x) never complete an embedding (injectivity) but do
+    change the counted tails: a matched vertex then lies in its own list and
+    must be excluded from it."""
+    _random_stream(100 + seed, 0.15)
+
+
+def _random_stream(seed, self_loop_rate):
     rng = np.random.default_rng(1000 + seed)
     qv = int(rng.integers(3, 7))
     qedges = _random_query(rng, qv, int(rng.integers(0, 4)))
@@ -98,6 +110,8 @@ def test_random_symmetric_streams(seed):
                 x = int(rng.integers(0, 2))
                 if y == x:
                     y = 2
+            if rng.random() < self_loop_rate:
+                y = x
             out.append((a, b, int(x), int(y)))
         return out
 
