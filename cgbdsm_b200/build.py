@@ -23,7 +23,7 @@ NVCC = os.environ.get("CGB_NVCC", shutil.which("nvcc") or "/usr/local/cuda/bin/n
 CXX = "/usr/bin/g++"  # system compiler: dynamic libstdc++ (safe to load into Python)
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
-ENGINE_CU = ["engine.cu", "noalloc.cu"]
+ENGINE_CU = ["engine.cu", "noalloc.cu", "gpma.cu"]
 ENGINE_CPP = ["query.cpp", "calig.cpp", "pipeline.cpp"]
 GEN_CPP = ["gen.cpp"]
 

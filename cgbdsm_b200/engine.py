@@ -28,6 +28,8 @@ EXPORTS = [
     "cgb_kernel_launches", "cgb_last_stats", "cgb_stream", "cgb_producer_open", "cgb_producer_close", "cgb_producer_last_error",
     "cgb_producer_num_batches", "cgb_producer_initial", "cgb_producer_next", "cgb_producer_vertex_map",
     "cgb_merge_keys_noalloc", "cgb_valid_bits", "cgb_starting_edge",
+    "cgb_gpma_create", "cgb_gpma_destroy", "cgb_gpma_last_error", "cgb_gpma_bulk_load", "cgb_gpma_batch_update",
+    "cgb_gpma_extract", "cgb_gpma_stats",
 ]
 
 # Edits one cgb_merge_keys_noalloc call accepts (CGB_NOALLOC_MAX_EDITS).
@@ -108,6 +110,14 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.cgb_merge_keys_noalloc.argtypes = [_vp, _u64, _vp, _u64, _vp, _u64, _u32, _vp, _vp, _vp]
     lib.cgb_valid_bits.argtypes = [_vp, _vp, _u64, ctypes.POINTER(_u64), ctypes.POINTER(ctypes.c_float)]
     lib.cgb_starting_edge.argtypes = [_vp, _vp]
+    lib.cgb_gpma_create.argtypes = [ctypes.c_int, _u32, ctypes.POINTER(_vp)]
+    lib.cgb_gpma_destroy.argtypes = [_vp]
+    lib.cgb_gpma_last_error.argtypes = [_vp]
+    lib.cgb_gpma_last_error.restype = ctypes.c_char_p
+    lib.cgb_gpma_bulk_load.argtypes = [_vp, _vp, _u64]
+    lib.cgb_gpma_batch_update.argtypes = [_vp, _vp, _u64, _vp, _u64]
+    lib.cgb_gpma_extract.argtypes = [_vp, _u32, _vp, _u64, ctypes.POINTER(_u64)]
+    lib.cgb_gpma_stats.argtypes = [_vp, _vp]
     for name in EXPORTS:
         getattr(lib, name)
     _lib_handle = lib
@@ -303,3 +313,66 @@ class Producer:
         n = _u32(0)
         self.lib.cgb_producer_vertex_map(self.h, ctypes.byref(p), ctypes.byref(n))
         return _copy(p, n.value, np.uint32)
+
+
+class Gpma:
+    """Packed-memory-array index layout (cgb_gpma_*); key arrays live on the
+    device (torch tensors of int64 holding the u64 keys)."""
+
+    def __init__(self, num_dirs: int, device: int = 0):
+        self.lib = load_library()
+        h = _vp()
+        st = self.lib.cgb_gpma_create(device, num_dirs, ctypes.byref(h))
+        self.h = h.value
+        self.device = device
+        if st != 0:
+            msg = self.lib.cgb_gpma_last_error(self.h).decode() if self.h else ""
+            self.close()
+            raise CgbError(st, msg)
+
+    def _check(self, st: int) -> None:
+        if st != 0:
+            raise CgbError(st, self.lib.cgb_gpma_last_error(self.h).decode())
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.lib.cgb_gpma_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _dev(self, keys: np.ndarray):
+        import torch
+
+        a = np.ascontiguousarray(keys, dtype=np.uint64).view(np.int64)
+        return torch.from_numpy(a).to(f"cuda:{self.device}")
+
+    def bulk_load(self, keys: np.ndarray) -> None:
+        t = self._dev(keys)
+        self._check(self.lib.cgb_gpma_bulk_load(self.h, t.data_ptr() if len(t) else None, len(t)))
+
+    def batch_update(self, ins: np.ndarray, dele: np.ndarray) -> None:
+        ti, td = self._dev(ins), self._dev(dele)
+        self._check(self.lib.cgb_gpma_batch_update(self.h, ti.data_ptr() if len(ti) else None, len(ti),
+                                                   td.data_ptr() if len(td) else None, len(td)))
+
+    def extract(self, d: int) -> np.ndarray:
+        """Keys of direction d, ascending, as (u << 32 | v)."""
+        import torch
+
+        n = _u64(0)
+        self._check(self.lib.cgb_gpma_extract(self.h, d, None, 0, ctypes.byref(n)))
+        out = torch.empty(max(n.value, 1), dtype=torch.int64, device=f"cuda:{self.device}")
+        self._check(self.lib.cgb_gpma_extract(self.h, d, out.data_ptr(), n.value, ctypes.byref(n)))
+        return out[: n.value].cpu().numpy().view(np.uint64)
+
+    def stats(self) -> dict:
+        out = np.zeros(6, dtype=np.uint64)
+        self._check(self.lib.cgb_gpma_stats(self.h, out.ctypes.data))
+        return {"slots": int(out[0]), "windows": int(out[1]), "rewritten": int(out[2]), "rebuilt": int(out[3]),
+                "device_us": int(out[4]), "keys": int(out[5])}
+

@@ -237,6 +237,31 @@ cgb_status cgb_merge_keys_noalloc(const uint64_t* old_keys_device, uint64_t n_ol
                                   const uint64_t* del_device, uint64_t n_del, uint32_t dv_count,
                                   uint64_t* out_device, uint64_t* out_n_device, void* stream);
 
+/* ---- Packed-memory-array index layout (the reference's GPMA: Multi_GPMA
+ * gpma/gpma.cuh:36-111, CGCSM_GPMA index/gpma_wrapper.cuh:10-40) ----
+ * One PMA per query direction over the same 64-bit keys, batch-updated with
+ * the engine's set semantics (index + ins) - del, rebalanced within windows
+ * chosen by the reference's density bounds (0.92 at the leaves to 0.84 at
+ * the root, gpma.cuh:55-58), without device-side launches.  All key arrays
+ * are device pointers. */
+typedef struct cgb_gpma cgb_gpma;
+/* CGCSM_GPMA::Init (gpma_wrapper.cu:20-25). */
+cgb_status cgb_gpma_create(int device, uint32_t num_dirs, cgb_gpma** out);
+void cgb_gpma_destroy(cgb_gpma* g);
+const char* cgb_gpma_last_error(const cgb_gpma* g);
+/* CGCSM_GPMA::BulkLoad (gpma_wrapper.cu:27-58): any order, duplicates allowed;
+ * replaces the contents. */
+cgb_status cgb_gpma_bulk_load(cgb_gpma* g, const uint64_t* keys_device, uint64_t n);
+/* CGCSM_GPMA::BatchUpdate (gpma_wrapper.cu:60-116). */
+cgb_status cgb_gpma_batch_update(cgb_gpma* g, const uint64_t* ins_device, uint64_t n_ins,
+                                 const uint64_t* del_device, uint64_t n_del);
+/* CGCSM_GPMA::ExtractEdges (gpma_wrapper.cuh:35-37): the keys of direction
+ * dir, ascending, as (u << 32 | v); out_device NULL = count only. */
+cgb_status cgb_gpma_extract(cgb_gpma* g, uint32_t dir, uint64_t* out_device, uint64_t cap, uint64_t* n_out);
+/* Last batch update: [0] slots, [1] windows rewritten, [2] keys rewritten,
+ * [3] 1 if it rebuilt the structure, [4] device microseconds, [5] keys held. */
+cgb_status cgb_gpma_stats(const cgb_gpma* g, uint64_t* out6);
+
 /* Valid bits (the reference's 1-bit support masks, BuildLocalIndexBitAll,
  * graph_gpu.cu:803-869; indexing.cu:2295-2379), computed for every matched
  * batch when CGB_FLAG_VALID_BITS or CGB_FLAG_MASK_PRUNE is set, after the
