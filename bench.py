@@ -281,8 +281,13 @@ def run_ours(args) -> None:
         "stage1_setup_s": round(s1_s, 2),
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        log("cpu baseline: reference CPU path on batch 0")
-        line["cpu_baseline"] = reference_sample(paths, spec, args.cpu_budget_s, batches)
+        from oracle import bind
+
+        if bind.have_ref():
+            log("cpu baseline: reference CPU path on batch 0")
+            line["cpu_baseline"] = reference_sample(paths, spec, args.cpu_budget_s, batches)
+        else:
+            line["cpu_baseline"] = {"unavailable": "oracle/_ref/libcgbref.so was not built (no reference tree)"}
     if rank == 0:
         print(json.dumps(line), flush=True)
     state["eng"].close()
@@ -347,7 +352,7 @@ def run_reference(args) -> None:
         "impl": "reference",
         "metric": "edge updates/sec (and incremental matches/sec, p50/p99 batch latency) on 1 B200",
         "value": v, "unit": "edge updates/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": (spec.batch_edges / v * 1e3) if v else None, "higher_is_better": True, "scaling": "weak",
+        "ms_per_step": (spec.batch_edges / v * 1e3) if v else None, "higher_is_better": True, "scaling": "strong",
         "vs_baseline": None, "dtype": "u32/u64 integer", "data": "synthetic (seeded R-MAT)",
         "config": {"workload": "R-MAT 1,000,000 vertices / 10,000,000 edges, 16 labels Zipf(1.2), "
                                "1,000,000 insertions in batches of 100,000, 9-vertex dense pattern"},
