@@ -646,7 +646,6 @@ __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
     int cur_ei = -1;
     const unsigned long long t_start = global_ns();
     uint32_t steps = 0;
-    uint32_t split_tick = 0;  // waiting warps are checked for every 4th chunk
     bool out_of_time = false;
     uint32_t ticket = kNoTicket;  // lane 0: ticket of the task ring this warp waits on
     uint32_t dirty = 0;  // shallowest position changed since the tail cache was filled (kClean: none)
@@ -794,7 +793,7 @@ __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
                 // survivors are a contiguous stretch of the generator (their
                 // offsets in their chunk ride in the top bits of s_cand), so
                 // one range [lo, hi) of depth d's generator describes it all.
-                if (a.steal && (a.force_split || ((++split_tick & 3u) == 0))) {
+                if (a.steal) {  // checked at every chunk: a waiting warp is served within one chunk's time
                     uint32_t want = 0;  // some warp holds a ticket no task has been reserved for
                     if (lane == 0) want = (a.force_split || (int)(vq[1] - vq[0]) > 0) ? 1u : 0u;
                     if (__shfl_sync(kFull, want, 0)) {
