@@ -6,6 +6,7 @@
 #include <fstream>
 #include <numeric>
 #include <random>
+#include <thread>
 #include <unordered_map>
 
 namespace cgb {
@@ -91,6 +92,16 @@ inline bool sorted_insert(std::vector<uint32_t>& v, uint32_t x) {
     v.insert(it, x);
     return true;
 }
+// Runs fn(0..n-1), each on its own thread (inline when n == 1).
+template <class Fn>
+void run_threads(uint32_t n, Fn fn) {
+    if (n <= 1) { fn(0u); return; }
+    std::vector<std::thread> pool;
+    pool.reserve(n);
+    for (uint32_t k = 0; k < n; ++k) pool.emplace_back(fn, k);
+    for (auto& t : pool) t.join();
+}
+
 inline bool sorted_erase(std::vector<uint32_t>& v, uint32_t x) {
     auto it = std::lower_bound(v.begin(), v.end(), x);
     if (it == v.end() || *it != x) return false;
@@ -312,6 +323,11 @@ const std::vector<uint32_t>* CaLiGIndex::cand(uint32_t v, uint32_t ui, uint32_t 
     return &lists_[cbase_[v] + block_off_[ui] + (uint32_t)p];
 }
 
+void CaLiGIndex::set_threads(uint32_t n) {
+    if (n == 0) n = std::max(1u, std::thread::hardware_concurrency());
+    threads_ = std::min<uint32_t>(n, 64);
+}
+
 // calig.cpp:325-356 constructCand, then 705-717 staticFilter.
 void CaLiGIndex::construct() {
     const uint32_t n = (uint32_t)glabel_.size();
@@ -423,17 +439,77 @@ void CaLiGIndex::add_and_check(std::vector<Task>& add, std::vector<Task>& add_de
     dedupe(add);
     std::vector<Tmp> tmp;
     std::vector<Task> check;
-    for (auto& t : add)
-        for (uint32_t uj : qnei_[t.u])
-            for (uint32_t vj : C(t.v, t.u, uj)) {
-                tmp.push_back({t.u, uj, t.v, vj});
-                if (!lit(vj, uj)) {
-                    check.push_back({uj, vj});
-                    checked_[vj] &= ~(1u << uj);
+    // The work list, in add order: slices of `add` on threads, concatenated
+    // in slice order (checked_ bits are cleared atomically: clearing commutes).
+    const uint32_t TB = add.size() >= 4096 ? threads_ : 1u;
+    std::vector<std::vector<Tmp>> ptmp(TB);
+    std::vector<std::vector<Task>> pchk(TB);
+    run_threads(TB, [&](uint32_t k) {
+        const size_t a0 = add.size() * k / TB, a1 = add.size() * (k + 1) / TB;
+        auto& lt = TB == 1 ? tmp : ptmp[k];
+        auto& lc = TB == 1 ? check : pchk[k];
+        for (size_t i = a0; i < a1; ++i) {
+            const Task& t = add[i];
+            for (uint32_t uj : qnei_[t.u])
+                for (uint32_t vj : C(t.v, t.u, uj)) {
+                    lt.push_back({t.u, uj, t.v, vj});
+                    if (!lit(vj, uj)) {
+                        lc.push_back({uj, vj});
+                        __atomic_fetch_and(&checked_[vj], ~(1u << uj), __ATOMIC_RELAXED);
+                    }
                 }
+        }
+    });
+    if (TB > 1)
+        for (uint32_t k = 0; k < TB; ++k) {
+            tmp.insert(tmp.end(), ptmp[k].begin(), ptmp[k].end());
+            check.insert(check.end(), pchk[k].begin(), pchk[k].end());
+        }
+    // Insert each vi into its candidate list.  Most of these inserts find the
+    // value present already, and each is a cache-missing search in a long
+    // list, so large rounds run on threads_ threads, each owning the lists
+    // with index % threads_ == its id: every list still sees its inserts in
+    // tmp order, and the inserted (new) entries are the same multiset.
+    const uint32_t T = tmp.size() >= (1u << 16) ? threads_ : 1u;
+    if (T <= 1) {
+        for (auto& t : tmp)
+            if (sorted_insert(C(t.vj, t.uj, t.ui), t.vi)) delta_ins.push_back({t.vj, t.vi, t.uj, t.ui});
+    } else {
+        // counting sort of the items by owner (list % T), stable, then one
+        // thread per owner
+        const size_t n = tmp.size();
+        std::vector<uint64_t> L(n);
+        std::vector<size_t> off((size_t)T * T, 0);  // [chunk][owner]
+        run_threads(T, [&](uint32_t c) {
+            for (size_t i = n * c / T; i < n * (c + 1) / T; ++i) {
+                L[i] = list_index(tmp[i].vj, tmp[i].uj, tmp[i].ui);
+                ++off[(size_t)c * T + L[i] % T];
             }
-    for (auto& t : tmp)
-        if (sorted_insert(C(t.vj, t.uj, t.ui), t.vi)) delta_ins.push_back({t.vj, t.vi, t.uj, t.ui});
+        });
+        std::vector<size_t> start(T + 1, 0);
+        size_t acc = 0;
+        for (uint32_t k = 0; k < T; ++k) {
+            start[k] = acc;
+            for (uint32_t c = 0; c < T; ++c) {
+                const size_t x = off[(size_t)c * T + k];
+                off[(size_t)c * T + k] = acc;
+                acc += x;
+            }
+        }
+        start[T] = acc;
+        std::vector<uint32_t> order(n);
+        run_threads(T, [&](uint32_t c) {
+            for (size_t i = n * c / T; i < n * (c + 1) / T; ++i) order[off[(size_t)c * T + L[i] % T]++] = (uint32_t)i;
+        });
+        std::vector<std::vector<DeltaOp>> part(T);
+        run_threads(T, [&](uint32_t k) {
+            for (size_t q = start[k]; q < start[k + 1]; ++q) {
+                const Tmp& t = tmp[order[q]];
+                if (sorted_insert(lists_[L[order[q]]], t.vi)) part[k].push_back({t.vj, t.vi, t.uj, t.ui});
+            }
+        });
+        for (auto& q : part) delta_ins.insert(delta_ins.end(), q.begin(), q.end());
+    }
     std::vector<Task> next;
     for (auto& c : check) {
         if ((checked_[c.v] >> c.u) & 1u) continue;

@@ -36,6 +36,9 @@ public:
     // constructCand + staticFilter (calig.cpp:325-356, 705-717)
     void construct();
 
+    // Host threads for the list-parallel phases (0 = all hardware threads).
+    void set_threads(uint32_t n);
+
     // One batch over update[start, start+count) (ints; two per edge).
     void update_index(uint32_t start, uint32_t count);
     void construct_update(uint32_t start, uint32_t count);
@@ -73,10 +76,12 @@ private:
     std::vector<std::vector<uint32_t>> lists_;
     std::vector<uint32_t> li_, checked_;
     std::vector<int> update_;
+    uint32_t threads_ = 1;
 
-    inline std::vector<uint32_t>& C(uint32_t v, uint32_t ui, uint32_t uj) {
-        return lists_[cbase_[v] + block_off_[ui] + (uint32_t)npos_[ui * qn_ + uj]];
+    inline uint64_t list_index(uint32_t v, uint32_t ui, uint32_t uj) const {
+        return cbase_[v] + block_off_[ui] + (uint32_t)npos_[ui * qn_ + uj];
     }
+    inline std::vector<uint32_t>& C(uint32_t v, uint32_t ui, uint32_t uj) { return lists_[list_index(v, ui, uj)]; }
     inline bool lit(uint32_t v, uint32_t u) const { return (li_[v] >> u) & 1u; }
     bool has_slot(uint32_t v, uint32_t u) const {
         return glabel_[v] >= 0 && glabel_[v] == label_slot_[qlabel_[u]];

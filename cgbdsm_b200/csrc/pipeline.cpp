@@ -54,10 +54,10 @@ extern "C" {
 
 cgb_status cgb_producer_open(const char* query_path, const char* data_path, const char* update_path,
                              uint32_t batch_size_ints, uint32_t threads, cgb_producer** out) {
-    (void)threads;
     if (!out || !query_path || !data_path) return CGB_ERR_ARG;
     auto* p = new cgb_producer();
     *out = p;
+    p->idx.set_threads(threads);
     p->batch_size = batch_size_ints ? batch_size_ints : UINT32_MAX;
     std::string e = p->idx.load_query(query_path);
     // main_calig.cpp:93-101: a data path ending in ".graph" is text and takes

@@ -194,7 +194,9 @@ typedef struct {
  * ending in ".graph" is a text graph and update_path its update stream;
  * any other data_path is a binary CSR prefix (.meta.txt, .vertex.bin,
  * .edge.bin; calig.cpp:218-323) whose update stream is derived from the
- * graph, and update_path is ignored (main_calig.cpp:93-101). */
+ * graph, and update_path is ignored (main_calig.cpp:93-101).  threads: host
+ * threads for Stage 1's list-parallel phases (0 = all hardware threads; the
+ * emitted key multisets do not depend on it). */
 cgb_status cgb_producer_open(const char* query_path, const char* data_path, const char* update_path,
                              uint32_t batch_size_ints, uint32_t threads, cgb_producer** out);
 void cgb_producer_close(cgb_producer* p);

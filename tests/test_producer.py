@@ -46,3 +46,34 @@ def test_producer_keys_match_reference(name, workdir):
                               np.unique(to_original(r["ins"], ref.new2old()))), f"batch {b}: ins keys differ"
     ref.close()
     prod.close()
+
+
+def test_parallel_producer_matches_reference_on_rmat_1m(workdir):
+    """The R-MAT 1M/10M stream is large enough for the producer's
+    list-parallel phases (all host threads); its first two batches' keys
+    still equal the reference's Stage 1 output (the reference's count is
+    switched off: only Stage 1 and staging run)."""
+    import os
+
+    if not bind.have_ref():
+        pytest.skip("oracle/_ref/libcgbref.so not built")
+    spec = SPECS["c2"]
+    p = materialize(spec, workdir)
+    ref = bind.RefPipeline(p["query"], p["data"], p["update"], spec.cli_batch_size, threads=os.cpu_count() or 1)
+    ref.set_count(False)
+    prod = Producer(p["query"], p["data"], p["update"], spec.cli_batch_size, threads=0)
+    init, dv = prod.initial()
+    assert dv == ref.dv_count
+    assert np.array_equal(to_original(init, prod.new2old()), to_original(ref.init_keys(), ref.new2old()))
+    for b in range(2):
+        mine = prod.next()
+        assert ref.step() == b
+        r = ref.last()
+        assert mine["dv"] == r["dv"]
+        assert np.array_equal(mine["edge_ok"], r["edge_ok"])
+        for k in ("delta", "del"):
+            assert np.array_equal(to_original(mine[k], prod.new2old()), to_original(r[k], ref.new2old())), k
+        assert np.array_equal(np.unique(to_original(mine["ins"], prod.new2old())),
+                              np.unique(to_original(r["ins"], ref.new2old())))
+    ref.close()
+    prod.close()
