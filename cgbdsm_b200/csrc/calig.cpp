@@ -2,6 +2,7 @@
 
 #include <algorithm>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <fstream>
 #include <numeric>
@@ -110,6 +111,46 @@ inline bool sorted_erase(std::vector<uint32_t>& v, uint32_t x) {
 }
 inline bool sorted_has(const std::vector<uint32_t>& v, uint32_t x) {
     return std::binary_search(v.begin(), v.end(), x);
+}
+
+// Adds the ascending values x[0..k) to the sorted set L with one merge pass
+// (a hub's list takes many values per batch; one memmove each would be
+// quadratic).  The result is the set union, as k sorted_insert calls give.
+void insert_run(std::vector<uint32_t>& L, const uint32_t* x, size_t k) {
+    if (k == 1) { sorted_insert(L, x[0]); return; }
+    const size_t old = L.size();
+    L.insert(L.end(), x, x + k);
+    std::inplace_merge(L.begin(), L.begin() + (std::ptrdiff_t)old, L.end());
+    L.erase(std::unique(L.begin(), L.end()), L.end());
+}
+
+// Removes the ascending distinct values x[0..k) from the sorted set L in one
+// pass; hit[i] = 1 when x[i] was present (what sorted_erase would return).
+void erase_run(std::vector<uint32_t>& L, const uint32_t* x, size_t k, uint8_t* hit) {
+    if (k == 1) { hit[0] = sorted_erase(L, x[0]); return; }
+    size_t w = 0, j = 0;
+    for (size_t i = 0; i < L.size(); ++i) {
+        while (j < k && x[j] < L[i]) hit[j++] = 0;
+        if (j < k && x[j] == L[i]) { hit[j++] = 1; continue; }
+        L[w++] = L[i];
+    }
+    while (j < k) hit[j++] = 0;
+    L.resize(w);
+}
+
+// Thread that owns data vertex v among T: a multiplicative hash, since
+// R-MAT-like ids concentrate degree on ids with many zero bits (v % T would
+// hand most of the work to thread 0).
+inline uint32_t owner(uint32_t v, uint32_t T) {
+    return (uint32_t)(((uint64_t)(v * 0x9E3779B1u) * T) >> 32);
+}
+
+template <typename T>
+void concat(std::vector<T>& dst, std::vector<std::vector<T>>& parts) {
+    size_t n = dst.size();
+    for (auto& p : parts) n += p.size();
+    dst.reserve(n);
+    for (auto& p : parts) dst.insert(dst.end(), p.begin(), p.end());
 }
 
 // Sorts and deduplicates a task queue.  Repeated tasks in the reference's
@@ -326,6 +367,9 @@ const std::vector<uint32_t>* CaLiGIndex::cand(uint32_t v, uint32_t ui, uint32_t 
 void CaLiGIndex::set_threads(uint32_t n) {
     if (n == 0) n = std::max(1u, std::thread::hardware_concurrency());
     threads_ = std::min<uint32_t>(n, 64);
+    // CGB_PRODUCER_MIN_PARALLEL: the smallest phase (items, pairs or tasks)
+    // that runs on threads; smaller ones run inline.  Default 4096.
+    if (const char* e = std::getenv("CGB_PRODUCER_MIN_PARALLEL")) par_min_ = std::strtoull(e, nullptr, 10);
 }
 
 // calig.cpp:325-356 constructCand, then 705-717 staticFilter.
@@ -396,133 +440,175 @@ bool CaLiGIndex::check_nei(uint32_t v, uint32_t u) {
     return true;
 }
 
+// Both fix-points below run on threads_ threads (large rounds), thread k
+// owning every data vertex v with owner(v, T) == k: the candidate lists of v, its
+// LI and checked bits.  A round first scans the task lists read-only (every
+// thread scans all of them and keeps the items whose target vertex it owns,
+// so each thread sees its items in the reference's queue order), then each
+// thread edits only the lists it owns.  The sequential round reads the
+// pre-round lists and LI while building its work list, and its set results
+// (list contents, deltas, the next queue) do not depend on the order of the
+// edits; the one order-dependent step — which same-label group a checked
+// (u, v) is tested against — depends on the order of v's own items only,
+// which the owner keeps.
+
 // calig.cpp:410-475 delAndCheck (one round; `del` becomes the next round).
 void CaLiGIndex::del_and_check(std::vector<Task>& del) {
     dedupe(del);
-    std::vector<Tmp> tmp;
+    size_t work = 0;
     for (auto& t : del)
-        for (uint32_t uj : qnei_[t.u])
-            for (uint32_t vj : C(t.v, t.u, uj))
-                if (lit(vj, uj)) tmp.push_back({t.u, uj, t.v, vj});
-    std::vector<Task> next;
+        for (uint32_t uj : qnei_[t.u]) work += C(t.v, t.u, uj).size();
+    const uint32_t T = work >= par_min_ ? threads_ : 1u;
+    struct Item { uint64_t list; uint32_t vi, vj, ui, uj; };
+    std::vector<std::vector<Item>> items(T);
+    run_threads(T, [&](uint32_t k) {
+        for (auto& t : del)
+            for (uint32_t uj : qnei_[t.u])
+                for (uint32_t vj : C(t.v, t.u, uj))
+                    if (owner(vj, T) == k && lit(vj, uj)) items[k].push_back({list_index(vj, uj, t.u), t.v, vj, t.u, uj});
+    });
     struct Chk { uint32_t u, v; int group; };
-    std::vector<Chk> chk;
-    for (auto& t : tmp) {
-        auto& L = C(t.vj, t.uj, t.ui);
-        if (sorted_erase(L, t.vi)) delta_del.push_back({t.vj, t.vi, t.uj, t.ui});
-        if (L.empty()) {
-            li_[t.vj] &= ~(1u << t.uj);
-            next.push_back({t.uj, t.vj});
-        } else {
-            const int g = rep_of_label_[t.uj][label_slot_[qlabel_[t.ui]]];
-            if (g >= 0) {
-                chk.push_back({t.uj, t.vj, g});
-                checked_[t.vj] &= ~(1u << t.uj);
+    std::vector<std::vector<Task>> next(T);
+    std::vector<std::vector<DeltaOp>> erased(T);
+    run_threads(T, [&](uint32_t k) {
+        const auto& it = items[k];
+        // erase each list's values in one pass; a list that ends empty turns
+        // its (uj, vj) off (the sequential round sees it empty at its last
+        // item; earlier items' group checks of a vertex that ends off change
+        // nothing)
+        // (list, vi << 32 | item) keys: grouped by list, values ascending
+        std::vector<std::pair<uint64_t, uint64_t>> ord(it.size());
+        for (size_t i = 0; i < it.size(); ++i) ord[i] = {it[i].list, (uint64_t)it[i].vi << 32 | i};
+        std::sort(ord.begin(), ord.end());
+        std::vector<uint8_t> ends_empty(it.size()), hit;
+        std::vector<uint32_t> vals;
+        for (size_t g0 = 0; g0 < ord.size();) {
+            size_t g1 = g0 + 1;
+            while (g1 < ord.size() && ord[g1].first == ord[g0].first) ++g1;
+            vals.clear();
+            for (size_t q = g0; q < g1; ++q) vals.push_back((uint32_t)(ord[q].second >> 32));
+            hit.assign(vals.size(), 0);
+            auto& L = lists_[ord[g0].first];
+            erase_run(L, vals.data(), vals.size(), hit.data());
+            for (size_t q = g0; q < g1; ++q) {
+                const uint32_t i = (uint32_t)ord[q].second;
+                const Item& e = it[i];
+                if (hit[q - g0]) erased[k].push_back({e.vj, e.vi, e.uj, e.ui});
+                ends_empty[i] = L.empty();
+            }
+            g0 = g1;
+        }
+        std::vector<Chk> chk;
+        for (size_t i = 0; i < it.size(); ++i) {
+            const Item& e = it[i];
+            if (ends_empty[i]) {
+                li_[e.vj] &= ~(1u << e.uj);
+                next[k].push_back({e.uj, e.vj});
+            } else {
+                const int g = rep_of_label_[e.uj][label_slot_[qlabel_[e.ui]]];
+                if (g >= 0) {
+                    chk.push_back({e.uj, e.vj, g});
+                    checked_[e.vj] &= ~(1u << e.uj);
+                }
             }
         }
-    }
-    for (auto& c : chk) {
-        if ((checked_[c.v] >> c.u) & 1u) continue;
-        checked_[c.v] |= 1u << c.u;
-        std::vector<uint32_t> used;
-        if (!try_nei(c.v, c.u, rep_[c.u][c.group], 0, used)) {
-            li_[c.v] &= ~(1u << c.u);
-            next.push_back({c.u, c.v});
+        for (auto& c : chk) {
+            if ((checked_[c.v] >> c.u) & 1u) continue;
+            checked_[c.v] |= 1u << c.u;
+            std::vector<uint32_t> used;
+            if (!try_nei(c.v, c.u, rep_[c.u][c.group], 0, used)) {
+                li_[c.v] &= ~(1u << c.u);
+                next[k].push_back({c.u, c.v});
+            }
         }
-    }
-    del.swap(next);
+    });
+    concat(delta_del, erased);
+    del.clear();
+    concat(del, next);
 }
 
 // calig.cpp:536-638 addAndCheck (one round; `add` becomes the next round).
-void CaLiGIndex::add_and_check(std::vector<Task>& add, std::vector<Task>& add_del,
-                               std::vector<Task>& activated) {
+//
+// Each item of a task (ui, vi) inserts vi into (vj, uj -> ui)'s list for
+// every vj in vi's (ui -> uj) list.  `settled` holds tasks whose (ui, vi)
+// was lit before the batch: their inserts all find vi present, so only
+// their unlit neighbours are collected.  Why: call vj in C(vi, ui, uj) with
+// vi missing from C(vj, uj, ui) an asymmetry of (ui, vi).  The lists start
+// symmetric (both hold the data edge); new edges insert both orientations;
+// an insert of vj into C(vi, ui, uj) by a task (uj, vj) comes from vi in
+// C(vj, uj, ui); erasing vj from vi's lists removes entries only.  The one
+// step that creates an asymmetry of (ui, vi) is the erasure of vi by its
+// own deletion, which turns (ui, vi) off; it comes back on only by an
+// activation, whose task re-inserts vi into every list its own lists name.
+// So a pair that stayed lit has none.  Tasks in `add` (activations) are
+// looked up item by item, and the misses are inserted; a (list, value) pair
+// occurs once per round (tasks are distinct), so each is inserted once.
+void CaLiGIndex::add_and_check(std::vector<Task>& add, std::vector<Task>& settled,
+                               std::vector<Task>& add_del, std::vector<Task>& activated) {
     dedupe(add);
-    std::vector<Tmp> tmp;
-    std::vector<Task> check;
-    // The work list, in add order: slices of `add` on threads, concatenated
-    // in slice order (checked_ bits are cleared atomically: clearing commutes).
-    const uint32_t TB = add.size() >= 4096 ? threads_ : 1u;
-    std::vector<std::vector<Tmp>> ptmp(TB);
-    std::vector<std::vector<Task>> pchk(TB);
-    run_threads(TB, [&](uint32_t k) {
-        const size_t a0 = add.size() * k / TB, a1 = add.size() * (k + 1) / TB;
-        auto& lt = TB == 1 ? tmp : ptmp[k];
-        auto& lc = TB == 1 ? check : pchk[k];
-        for (size_t i = a0; i < a1; ++i) {
-            const Task& t = add[i];
-            for (uint32_t uj : qnei_[t.u])
-                for (uint32_t vj : C(t.v, t.u, uj)) {
-                    lt.push_back({t.u, uj, t.v, vj});
-                    if (!lit(vj, uj)) {
-                        lc.push_back({uj, vj});
-                        __atomic_fetch_and(&checked_[vj], ~(1u << uj), __ATOMIC_RELAXED);
+    dedupe(settled);
+    size_t work = 0;
+    for (auto* q : {&add, &settled})
+        for (auto& t : *q)
+            for (uint32_t uj : qnei_[t.u]) work += C(t.v, t.u, uj).size();
+    const uint32_t T = work >= par_min_ ? threads_ : 1u;
+    struct Ins { uint64_t list; uint32_t vi, vj, ui, uj; };
+    std::vector<std::vector<Ins>> ins(T);
+    std::vector<std::vector<Task>> check(T);
+    run_threads(T, [&](uint32_t k) {
+        for (int pass = 0; pass < 2; ++pass)
+            for (auto& t : pass ? settled : add)
+                for (uint32_t uj : qnei_[t.u])
+                    for (uint32_t vj : C(t.v, t.u, uj)) {
+                        if (owner(vj, T) != k) continue;
+                        if (!pass) {
+                            const uint64_t L = list_index(vj, uj, t.u);
+                            if (!sorted_has(lists_[L], t.v)) ins[k].push_back({L, t.v, vj, t.u, uj});
+                        }
+                        if (!lit(vj, uj)) {
+                            check[k].push_back({uj, vj});
+                            checked_[vj] &= ~(1u << uj);
+                        }
                     }
-                }
+    });
+    settled.clear();
+    std::vector<std::vector<Task>> next(T), act(T), drop(T);
+    std::vector<std::vector<DeltaOp>> added(T);
+    run_threads(T, [&](uint32_t k) {
+        auto& it = ins[k];
+        std::sort(it.begin(), it.end(), [](const Ins& a, const Ins& b) {
+            return a.list != b.list ? a.list < b.list : a.vi < b.vi;
+        });
+        std::vector<uint32_t> vals;
+        for (size_t g0 = 0; g0 < it.size();) {
+            size_t g1 = g0 + 1;
+            while (g1 < it.size() && it[g1].list == it[g0].list) ++g1;
+            vals.clear();
+            for (size_t q = g0; q < g1; ++q) {
+                vals.push_back(it[q].vi);
+                added[k].push_back({it[q].vj, it[q].vi, it[q].uj, it[q].ui});
+            }
+            insert_run(lists_[it[g0].list], vals.data(), vals.size());
+            g0 = g1;
+        }
+        // check_nei(v, u) reads v's own lists only, all final for this round
+        for (auto& c : check[k]) {
+            if ((checked_[c.v] >> c.u) & 1u) continue;
+            checked_[c.v] |= 1u << c.u;
+            if (check_nei(c.v, c.u)) {
+                li_[c.v] |= 1u << c.u;
+                next[k].push_back(c);
+                act[k].push_back(c);
+            } else {
+                drop[k].push_back(c);
+            }
         }
     });
-    if (TB > 1)
-        for (uint32_t k = 0; k < TB; ++k) {
-            tmp.insert(tmp.end(), ptmp[k].begin(), ptmp[k].end());
-            check.insert(check.end(), pchk[k].begin(), pchk[k].end());
-        }
-    // Insert each vi into its candidate list.  Most of these inserts find the
-    // value present already, and each is a cache-missing search in a long
-    // list, so large rounds run on threads_ threads, each owning the lists
-    // with index % threads_ == its id: every list still sees its inserts in
-    // tmp order, and the inserted (new) entries are the same multiset.
-    const uint32_t T = tmp.size() >= (1u << 16) ? threads_ : 1u;
-    if (T <= 1) {
-        for (auto& t : tmp)
-            if (sorted_insert(C(t.vj, t.uj, t.ui), t.vi)) delta_ins.push_back({t.vj, t.vi, t.uj, t.ui});
-    } else {
-        // counting sort of the items by owner (list % T), stable, then one
-        // thread per owner
-        const size_t n = tmp.size();
-        std::vector<uint64_t> L(n);
-        std::vector<size_t> off((size_t)T * T, 0);  // [chunk][owner]
-        run_threads(T, [&](uint32_t c) {
-            for (size_t i = n * c / T; i < n * (c + 1) / T; ++i) {
-                L[i] = list_index(tmp[i].vj, tmp[i].uj, tmp[i].ui);
-                ++off[(size_t)c * T + L[i] % T];
-            }
-        });
-        std::vector<size_t> start(T + 1, 0);
-        size_t acc = 0;
-        for (uint32_t k = 0; k < T; ++k) {
-            start[k] = acc;
-            for (uint32_t c = 0; c < T; ++c) {
-                const size_t x = off[(size_t)c * T + k];
-                off[(size_t)c * T + k] = acc;
-                acc += x;
-            }
-        }
-        start[T] = acc;
-        std::vector<uint32_t> order(n);
-        run_threads(T, [&](uint32_t c) {
-            for (size_t i = n * c / T; i < n * (c + 1) / T; ++i) order[off[(size_t)c * T + L[i] % T]++] = (uint32_t)i;
-        });
-        std::vector<std::vector<DeltaOp>> part(T);
-        run_threads(T, [&](uint32_t k) {
-            for (size_t q = start[k]; q < start[k + 1]; ++q) {
-                const Tmp& t = tmp[order[q]];
-                if (sorted_insert(lists_[L[order[q]]], t.vi)) part[k].push_back({t.vj, t.vi, t.uj, t.ui});
-            }
-        });
-        for (auto& q : part) delta_ins.insert(delta_ins.end(), q.begin(), q.end());
-    }
-    std::vector<Task> next;
-    for (auto& c : check) {
-        if ((checked_[c.v] >> c.u) & 1u) continue;
-        checked_[c.v] |= 1u << c.u;
-        if (check_nei(c.v, c.u)) {
-            li_[c.v] |= 1u << c.u;
-            next.push_back(c);
-            activated.push_back(c);
-        } else {
-            add_del.push_back(c);
-        }
-    }
-    add.swap(next);
+    concat(delta_ins, added);
+    concat(activated, act);
+    concat(add_del, drop);
+    add.clear();
+    concat(add, next);
 }
 
 // calig.cpp:950-1069 for an insertion batch.  Deletions (negative ids) are
@@ -535,83 +621,127 @@ void CaLiGIndex::update_index(uint32_t start, uint32_t count) {
     delta_update.clear();
     const uint32_t end = std::min<uint32_t>(start + count, (uint32_t)update_.size());
     const uint32_t n = (uint32_t)glabel_.size();
-    std::vector<std::pair<uint32_t, uint32_t>> ups;
-    std::vector<Tmp> tmp;
-    for (uint32_t t = start; t + 1 < end; t += 2) {
-        const int a = update_[t], b = update_[t + 1];
-        if (a < 0 || b < 0 || (uint32_t)a >= n || (uint32_t)b >= n) continue;
-        const uint32_t v1 = (uint32_t)a, v2 = (uint32_t)b;
-        if (glabel_[v1] < 0 || glabel_[v2] < 0) continue;
-        if (sorted_has(nei_[v1], v2)) continue;  // edge exists before this batch
-        ups.emplace_back(v1, v2);
-        // turnOnCond (calig.cpp:640-655), both orientations
-        for (int o = 0; o < 2; ++o) {
-            const uint32_t x = o ? v2 : v1, y = o ? v1 : v2;
-            for (uint32_t ui : qlist_[glabel_[x]])
-                for (uint32_t uj : qnei_[ui])
-                    if (label_slot_[qlabel_[uj]] == glabel_[y]) tmp.push_back({ui, uj, x, y});
+    const uint32_t npairs = end > start ? (end - start) / 2 : 0;
+    const uint32_t T = npairs >= par_min_ ? threads_ : 1u;
+    // turnOnCond (calig.cpp:640-655) on slices of the batch, against the
+    // adjacency before the batch (a pair listed twice is new both times)
+    std::vector<std::vector<std::pair<uint32_t, uint32_t>>> ups(T);
+    std::vector<std::vector<Tmp>> tmp(T);
+    run_threads(T, [&](uint32_t s) {
+        for (uint32_t p = (uint32_t)((uint64_t)npairs * s / T); p < (uint32_t)((uint64_t)npairs * (s + 1) / T); ++p) {
+            const int a = update_[start + 2 * p], b = update_[start + 2 * p + 1];
+            if (a < 0 || b < 0 || (uint32_t)a >= n || (uint32_t)b >= n) continue;
+            const uint32_t v1 = (uint32_t)a, v2 = (uint32_t)b;
+            if (glabel_[v1] < 0 || glabel_[v2] < 0) continue;
+            if (sorted_has(nei_[v1], v2)) continue;  // edge exists before this batch
+            ups[s].emplace_back(v1, v2);
+            for (int o = 0; o < 2; ++o) {
+                const uint32_t x = o ? v2 : v1, y = o ? v1 : v2;
+                for (uint32_t ui : qlist_[glabel_[x]])
+                    for (uint32_t uj : qnei_[ui])
+                        if (label_slot_[qlabel_[uj]] == glabel_[y]) tmp[s].push_back({ui, uj, x, y});
+            }
         }
-    }
-    for (auto& [x, y] : ups) {
-        sorted_insert(nei_[x], y);
-        sorted_insert(nei_[y], x);
-    }
-    // turnOnCheck (calig.cpp:657-693)
-    std::vector<Task> add, check, activated, add_del;
-    for (auto& t : tmp) {
-        sorted_insert(C(t.vi, t.ui, t.uj), t.vj);
-        if (lit(t.vi, t.ui)) add.push_back({t.ui, t.vi});
-        else {
-            check.push_back({t.ui, t.vi});
-            checked_[t.vi] &= ~(1u << t.ui);
+    });
+    // Adjacency and candidate-list inserts, then turnOnCheck (calig.cpp:657-693),
+    // by owner of the first vertex: its lists, LI and checked bits.
+    std::vector<std::vector<Task>> addp(T), setp(T), actp(T);
+    run_threads(T, [&](uint32_t k) {
+        std::vector<std::pair<uint64_t, uint32_t>> ins;
+        for (auto& part : ups)
+            for (auto& [x, y] : part) {
+                if (owner(x, T) == k) ins.emplace_back(x, y);
+                if (owner(y, T) == k) ins.emplace_back(y, x);
+            }
+        std::vector<uint32_t> vals;
+        auto apply = [&](auto&& list_of) {
+            std::sort(ins.begin(), ins.end());
+            for (size_t g0 = 0; g0 < ins.size();) {
+                size_t g1 = g0 + 1;
+                while (g1 < ins.size() && ins[g1].first == ins[g0].first) ++g1;
+                vals.clear();
+                for (size_t q = g0; q < g1; ++q) vals.push_back(ins[q].second);
+                insert_run(list_of(ins[g0].first), vals.data(), vals.size());
+                g0 = g1;
+            }
+        };
+        apply([&](uint64_t x) -> std::vector<uint32_t>& { return nei_[x]; });
+        ins.clear();
+        std::vector<Task> check;
+        for (auto& part : tmp)
+            for (auto& t : part) {
+                if (owner(t.vi, T) != k) continue;
+                ins.emplace_back(list_index(t.vi, t.ui, t.uj), t.vj);
+                if (lit(t.vi, t.ui)) setp[k].push_back({t.ui, t.vi});
+                else {
+                    check.push_back({t.ui, t.vi});
+                    checked_[t.vi] &= ~(1u << t.ui);
+                }
+            }
+        apply([&](uint64_t l) -> std::vector<uint32_t>& { return lists_[l]; });
+        for (auto& c : check) {
+            if ((checked_[c.v] >> c.u) & 1u) continue;
+            checked_[c.v] |= 1u << c.u;
+            if (lit(c.v, c.u)) continue;
+            if (check_nei(c.v, c.u)) {
+                li_[c.v] |= 1u << c.u;
+                addp[k].push_back(c);
+                actp[k].push_back(c);
+            }
         }
-    }
-    for (auto& c : check) {
-        if ((checked_[c.v] >> c.u) & 1u) continue;
-        checked_[c.v] |= 1u << c.u;
-        if (lit(c.v, c.u)) continue;
-        if (check_nei(c.v, c.u)) {
-            li_[c.v] |= 1u << c.u;
-            add.push_back(c);
-            activated.push_back(c);
-        }
-    }
+    });
+    std::vector<Task> add, settled, activated, add_del;
+    concat(add, addp);
+    concat(settled, setp);
+    concat(activated, actp);
     // addAndCheck to the fix-point, then addAndCheckDelete (calig.cpp:695-703)
-    while (!add.empty()) add_and_check(add, add_del, activated);
+    while (!add.empty() || !settled.empty()) add_and_check(add, settled, add_del, activated);
     std::vector<Task> del;
     for (auto& c : add_del)
         if (!lit(c.v, c.u)) del.push_back(c);
     while (!del.empty()) del_and_check(del);
     // newly lit vertices contribute their whole candidate lists (calig.cpp:1048-1068)
-    for (auto& a : activated) {
-        if (!lit(a.v, a.u)) continue;
-        for (uint32_t uj : qnei_[a.u])
-            for (uint32_t vj : C(a.v, a.u, uj)) delta_ins.push_back({a.v, vj, a.u, uj});
-    }
+    const uint32_t TA = activated.size() >= par_min_ ? threads_ : 1u;
+    std::vector<std::vector<DeltaOp>> whole(TA);
+    run_threads(TA, [&](uint32_t s) {
+        for (size_t i = activated.size() * s / TA; i < activated.size() * (s + 1) / TA; ++i) {
+            const Task& a = activated[i];
+            if (!lit(a.v, a.u)) continue;
+            for (uint32_t uj : qnei_[a.u])
+                for (uint32_t vj : C(a.v, a.u, uj)) whole[s].push_back({a.v, vj, a.u, uj});
+        }
+    });
+    concat(delta_ins, whole);
 }
 
 // calig.cpp:776-804: for every pair of the batch (as listed), each lit u1 of
 // v1 whose (u1 -> u2) list holds v2 yields the delta edge in both directions,
-// which is also scheduled for removal from the old index.
+// which is also scheduled for removal from the old index.  Read-only: slices
+// of the batch on threads, concatenated in batch order.
 void CaLiGIndex::construct_update(uint32_t start, uint32_t count) {
     const uint32_t end = std::min<uint32_t>(start + count, (uint32_t)update_.size());
     const uint32_t n = (uint32_t)glabel_.size();
-    for (uint32_t t = start; t + 1 < end; t += 2) {
-        const int a = update_[t], b = update_[t + 1];
-        if (a < 0 || b < 0 || (uint32_t)a >= n || (uint32_t)b >= n) continue;
-        const uint32_t v1 = (uint32_t)a, v2 = (uint32_t)b;
-        if (glabel_[v1] < 0) continue;
-        for (uint32_t u1 : qlist_[glabel_[v1]]) {
-            if (!lit(v1, u1)) continue;
-            for (uint32_t u2 : qnei_[u1]) {
-                if (!sorted_has(C(v1, u1, u2), v2)) continue;
-                delta_update.push_back({v1, v2, u1, u2});
-                delta_del.push_back({v1, v2, u1, u2});
-                delta_update.push_back({v2, v1, u2, u1});
-                delta_del.push_back({v2, v1, u2, u1});
+    const uint32_t npairs = end > start ? (end - start) / 2 : 0;
+    const uint32_t T = npairs >= par_min_ ? threads_ : 1u;
+    std::vector<std::vector<DeltaOp>> upd(T);
+    run_threads(T, [&](uint32_t s) {
+        for (uint32_t p = (uint32_t)((uint64_t)npairs * s / T); p < (uint32_t)((uint64_t)npairs * (s + 1) / T); ++p) {
+            const int a = update_[start + 2 * p], b = update_[start + 2 * p + 1];
+            if (a < 0 || b < 0 || (uint32_t)a >= n || (uint32_t)b >= n) continue;
+            const uint32_t v1 = (uint32_t)a, v2 = (uint32_t)b;
+            if (glabel_[v1] < 0) continue;
+            for (uint32_t u1 : qlist_[glabel_[v1]]) {
+                if (!lit(v1, u1)) continue;
+                for (uint32_t u2 : qnei_[u1]) {
+                    if (!sorted_has(C(v1, u1, u2), v2)) continue;
+                    upd[s].push_back({v1, v2, u1, u2});
+                    upd[s].push_back({v2, v1, u2, u1});
+                }
             }
         }
-    }
+    });
+    concat(delta_update, upd);
+    concat(delta_del, upd);
 }
 
 }  // namespace cgb

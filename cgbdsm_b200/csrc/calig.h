@@ -36,7 +36,8 @@ public:
     // constructCand + staticFilter (calig.cpp:325-356, 705-717)
     void construct();
 
-    // Host threads for the list-parallel phases (0 = all hardware threads).
+    // Host threads for the list-parallel phases (0 = all hardware threads);
+    // also reads CGB_PRODUCER_MIN_PARALLEL (smallest phase run on threads).
     void set_threads(uint32_t n);
 
     // One batch over update[start, start+count) (ints; two per edge).
@@ -77,6 +78,7 @@ private:
     std::vector<uint32_t> li_, checked_;
     std::vector<int> update_;
     uint32_t threads_ = 1;
+    uint64_t par_min_ = 4096;
 
     inline uint64_t list_index(uint32_t v, uint32_t ui, uint32_t uj) const {
         return cbase_[v] + block_off_[ui] + (uint32_t)npos_[ui * qn_ + uj];
@@ -92,7 +94,8 @@ private:
 
     struct Task { uint32_t u, v; };
     struct Tmp { uint32_t ui, uj, vi, vj; };
-    void add_and_check(std::vector<Task>& add, std::vector<Task>& add_del, std::vector<Task>& activated);
+    void add_and_check(std::vector<Task>& add, std::vector<Task>& settled, std::vector<Task>& add_del,
+                       std::vector<Task>& activated);
     void del_and_check(std::vector<Task>& del);
 };
 

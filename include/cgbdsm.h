@@ -196,7 +196,8 @@ typedef struct {
  * .edge.bin; calig.cpp:218-323) whose update stream is derived from the
  * graph, and update_path is ignored (main_calig.cpp:93-101).  threads: host
  * threads for Stage 1's list-parallel phases (0 = all hardware threads; the
- * emitted key multisets do not depend on it). */
+ * emitted key multisets do not depend on it).  Phases smaller than
+ * $CGB_PRODUCER_MIN_PARALLEL items (default 4096) run on the calling thread. */
 cgb_status cgb_producer_open(const char* query_path, const char* data_path, const char* update_path,
                              uint32_t batch_size_ints, uint32_t threads, cgb_producer** out);
 void cgb_producer_close(cgb_producer* p);

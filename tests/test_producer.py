@@ -19,15 +19,14 @@ def to_original(keys, new2old):
     return np.sort((d << np.uint64(59)) | (n2o[u] << np.uint64(32)) | n2o[v])
 
 
-@pytest.mark.parametrize("name", CASES)
-def test_producer_keys_match_reference(name, workdir):
+def _compare_with_reference(name, workdir, threads=0):
     if not bind.have_ref():
         pytest.skip("oracle/_ref/libcgbref.so not built")
     spec = SPECS[name]
     p = materialize(spec, workdir)
     ref = bind.RefPipeline(p["query"], p["data"], p["update"], spec.cli_batch_size)
     ref.set_count(False)
-    prod = Producer(p["query"], p["data"], p["update"], spec.cli_batch_size)
+    prod = Producer(p["query"], p["data"], p["update"], spec.cli_batch_size, threads=threads)
     assert prod.num_batches == ref.num_batches
     init, dv = prod.initial()
     assert dv == ref.dv_count
@@ -46,6 +45,20 @@ def test_producer_keys_match_reference(name, workdir):
                               np.unique(to_original(r["ins"], ref.new2old()))), f"batch {b}: ins keys differ"
     ref.close()
     prod.close()
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_producer_keys_match_reference(name, workdir):
+    _compare_with_reference(name, workdir)
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_partitioned_producer_keys_match_reference(name, workdir, monkeypatch):
+    """Every phase forced onto 3 threads (vertices partitioned among them by
+    hash), including the fix-point rounds of a handful of tasks: the key
+    multisets stay the reference's."""
+    monkeypatch.setenv("CGB_PRODUCER_MIN_PARALLEL", "0")
+    _compare_with_reference(name, workdir, threads=3)
 
 
 def test_parallel_producer_matches_reference_on_rmat_1m(workdir):
