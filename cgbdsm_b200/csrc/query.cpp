@@ -126,73 +126,91 @@ void plan_edges(const QueryMeta& q, const float* avg_deg, EdgePlan* plans, bool 
         pos[a] = 0;
         pos[b] = 1;
         auto lab = [&](uint32_t u) { return q.labels.empty() ? 0u : q.labels[u]; };
+        // A tail vertex with several lists that hangs off the last core
+        // vertex would be counted by one intersection per last-level
+        // candidate, and would keep the rest of the tail from being constant
+        // per prefix; enumerated as a core vertex its intersection runs
+        // chunked and narrowed.  Such vertices move to the core (`forced`)
+        // and the tail and last vertex are chosen again.
+        std::vector<char> forced(q.qv, 0), is_tail;
         std::vector<uint32_t> tail;
-        if (analytic_tail && q.qv > 2) {
-            std::vector<char> in_t(q.qv, 0);
-            std::vector<uint32_t> cand;
-            for (uint32_t u = 0; u < q.qv; ++u)
-                if (u != a && u != b) cand.push_back(u);
-            std::stable_sort(cand.begin(), cand.end(),
-                             [&](uint32_t x, uint32_t y) { return q.nbrs[x].size() < q.nbrs[y].size(); });
-            auto core_connected = [&]() {
-                std::vector<char> seen(q.qv, 0);
-                std::vector<uint32_t> st{a};
-                seen[a] = 1;
-                uint32_t reached = 1, need = 0;
-                for (uint32_t u = 0; u < q.qv; ++u) need += in_t[u] ? 0 : 1;
-                while (!st.empty()) {
-                    uint32_t u = st.back();
-                    st.pop_back();
-                    for (uint32_t w : q.nbrs[u])
-                        if (!in_t[w] && !seen[w]) { seen[w] = 1; ++reached; st.push_back(w); }
-                }
-                return reached == need;
-            };
-            for (uint32_t u : cand) {
-                bool adj = false;
-                for (uint32_t w : q.nbrs[u]) adj |= in_t[w] != 0;
-                if (adj) continue;
-                in_t[u] = 1;
-                if (!core_connected()) in_t[u] = 0;
-            }
-            for (uint32_t u : cand)
-                if (in_t[u]) tail.push_back(u);
-            std::stable_sort(tail.begin(), tail.end(), [&](uint32_t x, uint32_t y) { return lab(x) < lab(y); });
-            std::vector<uint32_t> kept;
-            for (size_t i = 0; i < tail.size();) {
-                size_t j = i;
-                while (j < tail.size() && lab(tail[j]) == lab(tail[i])) ++j;
-                for (size_t k = i; k < j && k < i + 3; ++k) kept.push_back(tail[k]);
-                i = j;
-            }
-            tail.swap(kept);
-        }
-        std::vector<char> is_tail(q.qv, 0);
-        for (uint32_t u : tail) is_tail[u] = 1;
-        const uint32_t n_core = q.qv - (uint32_t)tail.size();
-        // last core vertex: the one with the fewest tail neighbours (its
-        // tail lists must be re-scanned per candidate), among those whose
-        // removal keeps the rest of the core connected
+        uint32_t n_core = q.qv;
         int last = -1;
-        if (pick_last && n_core > 2) {
-            int best_t = 1 << 30, best_c = -1;
-            for (uint32_t u = 0; u < q.qv; ++u) {
-                if (is_tail[u] || u == a || u == b) continue;
-                std::vector<char> seen(q.qv, 0);
-                std::vector<uint32_t> st{a};
-                seen[a] = 1;
-                uint32_t reached = 1;
-                while (!st.empty()) {
-                    uint32_t x = st.back();
-                    st.pop_back();
-                    for (uint32_t w : q.nbrs[x])
-                        if (!is_tail[w] && w != u && !seen[w]) { seen[w] = 1; ++reached; st.push_back(w); }
+        for (;;) {
+            tail.clear();
+            if (analytic_tail && q.qv > 2) {
+                std::vector<char> in_t(q.qv, 0);
+                std::vector<uint32_t> cand;
+                for (uint32_t u = 0; u < q.qv; ++u)
+                    if (u != a && u != b && !forced[u]) cand.push_back(u);
+                std::stable_sort(cand.begin(), cand.end(),
+                                 [&](uint32_t x, uint32_t y) { return q.nbrs[x].size() < q.nbrs[y].size(); });
+                auto core_connected = [&]() {
+                    std::vector<char> seen(q.qv, 0);
+                    std::vector<uint32_t> st{a};
+                    seen[a] = 1;
+                    uint32_t reached = 1, need = 0;
+                    for (uint32_t u = 0; u < q.qv; ++u) need += in_t[u] ? 0 : 1;
+                    while (!st.empty()) {
+                        uint32_t u = st.back();
+                        st.pop_back();
+                        for (uint32_t w : q.nbrs[u])
+                            if (!in_t[w] && !seen[w]) { seen[w] = 1; ++reached; st.push_back(w); }
+                    }
+                    return reached == need;
+                };
+                for (uint32_t u : cand) {
+                    bool adj = false;
+                    for (uint32_t w : q.nbrs[u]) adj |= in_t[w] != 0;
+                    if (adj) continue;
+                    in_t[u] = 1;
+                    if (!core_connected()) in_t[u] = 0;
                 }
-                if (reached != n_core - 1) continue;
-                int nt = 0, ncn = 0;
-                for (uint32_t w : q.nbrs[u]) { nt += is_tail[w] ? 1 : 0; ncn += is_tail[w] ? 0 : 1; }
-                if (nt < best_t || (nt == best_t && ncn > best_c)) { best_t = nt; best_c = ncn; last = (int)u; }
+                for (uint32_t u : cand)
+                    if (in_t[u]) tail.push_back(u);
+                std::stable_sort(tail.begin(), tail.end(), [&](uint32_t x, uint32_t y) { return lab(x) < lab(y); });
+                std::vector<uint32_t> kept;
+                for (size_t i = 0; i < tail.size();) {
+                    size_t j = i;
+                    while (j < tail.size() && lab(tail[j]) == lab(tail[i])) ++j;
+                    for (size_t k = i; k < j && k < i + 3; ++k) kept.push_back(tail[k]);
+                    i = j;
+                }
+                tail.swap(kept);
             }
+            is_tail.assign(q.qv, 0);
+            for (uint32_t u : tail) is_tail[u] = 1;
+            n_core = q.qv - (uint32_t)tail.size();
+            // last core vertex: the one with the fewest tail neighbours (its
+            // tail lists must be re-scanned per candidate), among those whose
+            // removal keeps the rest of the core connected
+            last = -1;
+            if (pick_last && n_core > 2) {
+                int best_t = 1 << 30, best_c = -1;
+                for (uint32_t u = 0; u < q.qv; ++u) {
+                    if (is_tail[u] || u == a || u == b) continue;
+                    std::vector<char> seen(q.qv, 0);
+                    std::vector<uint32_t> st{a};
+                    seen[a] = 1;
+                    uint32_t reached = 1;
+                    while (!st.empty()) {
+                        uint32_t x = st.back();
+                        st.pop_back();
+                        for (uint32_t w : q.nbrs[x])
+                            if (!is_tail[w] && w != u && !seen[w]) { seen[w] = 1; ++reached; st.push_back(w); }
+                    }
+                    if (reached != n_core - 1) continue;
+                    int nt = 0, ncn = 0;
+                    for (uint32_t w : q.nbrs[u]) { nt += is_tail[w] ? 1 : 0; ncn += is_tail[w] ? 0 : 1; }
+                    if (nt < best_t || (nt == best_t && ncn > best_c)) { best_t = nt; best_c = ncn; last = (int)u; }
+                }
+            }
+            int move = -1;
+            if (last >= 0)
+                for (uint32_t t : tail)
+                    if (q.nbrs[t].size() >= 2 && q.eidx[(uint32_t)last * kMaxQV + t] != 255) { move = (int)t; break; }
+            if (move < 0) break;
+            forced[move] = 1;
         }
         for (uint32_t j = 2; j < n_core; ++j) {
             if (last >= 0 && j == n_core - 1) {
