@@ -604,6 +604,64 @@ __device__ __forceinline__ void add_release(unsigned int* p, unsigned int v) {
 
 constexpr uint32_t kTaskWords = 16;
 constexpr uint32_t kNoTicket = 0xffffffffu;
+constexpr uint32_t kNoVertex = 0xffffffffu;  // m[1] of a grouped unit: matches no candidate
+
+// First index of the ascending X[0..n) whose value is >= c (> c when upper),
+// for a warp-uniform c: 32-ary search, each round one load per lane.
+__device__ __forceinline__ uint32_t warp_bound(const uint32_t* __restrict__ X, uint32_t n, uint32_t c, bool upper,
+                                               uint32_t lane) {
+    uint32_t lo = 0, hi = n;  // the answer lies in [lo, hi]
+    while (hi - lo > 32) {
+        const uint32_t span = hi - lo;
+        bool below = false;  // lanes 0..30 test the pivots lo + floor(span * (lane + 1) / 32)
+        if (lane < 31) {
+            const uint32_t x = __ldg(X + lo + (uint32_t)(((uint64_t)span * (lane + 1)) >> 5));
+            below = upper ? x <= c : x < c;
+        }
+        const uint32_t k = __popc(__ballot_sync(kFull, below));
+        const uint32_t nlo = k ? lo + (uint32_t)(((uint64_t)span * k) >> 5) + 1u : lo;
+        hi = k < 31 ? lo + (uint32_t)(((uint64_t)span * (k + 1)) >> 5) : hi;
+        lo = nlo;
+    }
+    bool below = false;
+    if (lo + lane < hi) {
+        const uint32_t x = __ldg(X + lo + lane);
+        below = upper ? x <= c : x < c;
+    }
+    return lo + __popc(__ballot_sync(kFull, below));
+}
+
+// Seed group of a grouped unit: X = the delta list of (seed_dir, m[0]), the
+// x values of all seeds (x, m[0]) with multiplicity.  Up to 32 values live
+// one per lane in xv.
+struct SeedGroup {
+    const uint32_t* x;
+    uint32_t n;
+    uint32_t xv;
+    // multiplicity of the warp-uniform c in X
+    __device__ __forceinline__ uint32_t mult(uint32_t c, uint32_t lane) const {
+        if (n <= 32) return __popc(__ballot_sync(kFull, xv == c));
+        return warp_bound(x, n, c, true, lane) - warp_bound(x, n, c, false, lane);
+    }
+    // sum over the lanes with `on` of the multiplicity of their own c
+    __device__ __forceinline__ uint32_t mult_sum(uint32_t c, bool on) const {
+        uint32_t r = 0;
+        if (n <= 32) {
+            for (uint32_t i = 0; i < n; ++i) r += (__shfl_sync(kFull, xv, i) == c) ? 1u : 0u;
+        } else {
+            uint32_t lo = 0, len = n;
+            while (len > 0) {
+                const uint32_t half = len >> 1;
+                if (__ldg(x + lo + half) < c) { lo += half + 1; len -= half + 1; }
+                else len = half;
+            }
+            for (uint32_t i = lo; i < n && __ldg(x + i) == c; ++i) ++r;
+        }
+        r = on ? r : 0u;
+        for (int o = 16; o > 0; o >>= 1) r += __shfl_xor_sync(kFull, r, o);
+        return r;
+    }
+};
 // Ready tag of ticket t in launch `epoch`: the epoch's low 20 bits and the
 // ring lap of t, so a slot reused in a later lap or launch never shows a
 // stale tag to the consumer of t.
@@ -640,6 +698,7 @@ __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
 
     // per-depth state held by lane == depth
     uint32_t st_ncand = 0, st_pos = 0, st_next = 0, st_len = 0, st_gen = 0;
+    uint32_t st_hs = 0;  // grouped units: X multiplicity of the vertices at hit positions < depth
     unsigned long long cnt = 0;  // lane-local partial count of the current edge
     unsigned long long n_seeds = 0, n_chunks = 0, n_tested = 0, n_tail = 0, n_tasks = 0;
     unsigned long long n_bytes = 0;  // algorithmic bytes: seed keys, records, list words, probe sectors
@@ -697,12 +756,21 @@ __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
             item = a.shard + item * a.num_shards;
             while (ei + 1 < (int)a.qe && s_pre[ei + 1] <= item) ++ei;
             const uint64_t key = a.dkeys[s_lo[ei] + (item - s_pre[ei])];
+            ++n_seeds;
+            if (c_plan[ei].grouped && item > s_pre[ei]) {
+                // a grouped edge runs one DFS per first vertex: only the first
+                // seed of each run of equal first vertices starts one
+                const uint64_t prev = a.dkeys[s_lo[ei] + (item - s_pre[ei]) - 1];
+                if (((prev ^ key) >> a.B & vmask) == 0) {
+                    if (lane == 0) add_release((unsigned int*)&a.qctr[3], 1u);
+                    continue;
+                }
+            }
             if (lane == 0) {
                 m[0] = (uint32_t)((key >> a.B) & vmask);
-                m[1] = (uint32_t)(key & vmask);
+                m[1] = c_plan[ei].grouped ? kNoVertex : (uint32_t)(key & vmask);
                 n_bytes += 8;
             }
-            ++n_seeds;
         } else {
             // lane 0 saw the ticket's ready tag: the task's words are published
             volatile uint32_t* tk = a.tasks + (size_t)(item & (a.task_cap - 1u)) * kTaskWords;
@@ -727,10 +795,18 @@ __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
         const EdgePlan& P = c_plan[ei];
         const uint32_t nc = P.n_core;
         const bool has_tail = nc < P.n;
+        SeedGroup X{nullptr, 0u, kNoVertex};
+        if (P.grouped) {
+            const uint4 xr = a.rec[(size_t)P.seed_dir * a.dvcap + m[0]];
+            X.x = a.dval + xr.z;
+            X.n = xr.w;
+            if (X.n <= 32 && lane < X.n) X.xv = __ldg(X.x + lane);
+            if (lane == 0) n_bytes += 16 + 4ull * min(X.n, 32u);
+        }
         if (kind == 1 && nc == 2) {  // the seed edge alone is the core: only the tail remains
             const unsigned long long tc =
                 (P.n == 2) ? 1ull : tail_count_warp(P, m, bn, a.rec, a.dvcap, a.pool, a.dval, self_loops, lane, n_bytes);
-            if (lane == 0) { cnt += tc; ++n_tail; }
+            if (lane == 0) { cnt += P.grouped ? tc * X.n : tc; ++n_tail; }
             __syncwarp();
             if (lane == 0) add_release((unsigned int*)&a.qctr[3], 1u);
             continue;
@@ -762,6 +838,12 @@ __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
         dirty = 0;  // new unit: every cached tail count is stale
         setup(jbase);
         if (kind == 2 && lane == jbase) { st_gen = tgen; st_next = tlo; st_len = thi; }
+        if (P.grouped) {
+            uint32_t h = 0;
+            for (uint32_t p = 2; p < jbase; ++p)
+                if ((P.hit_mask >> p) & 1u) h += X.mult(m[p], lane);
+            if (lane == jbase) st_hs = h;
+        }
         __syncwarp();
         uint32_t j = jbase;
         while (j >= jbase) {
@@ -778,6 +860,11 @@ __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
                 if (lane == 0) m[j] = s_cand[w][j][pos] & kCandMask;
                 __syncwarp();
                 dirty = min(dirty, j);
+                if (P.grouped) {
+                    uint32_t h = __shfl_sync(kFull, st_hs, j);
+                    if ((P.hit_mask >> j) & 1u) h += X.mult(m[j], lane);
+                    if (lane == j + 1) st_hs = h;
+                }
                 ++j;
                 setup(j);
                 continue;
@@ -906,6 +993,10 @@ __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
                 }
                 ++n_chunks;
                 if (j == nc - 1) {
+                    // grouped units weigh each embedding by |X| minus the X
+                    // multiplicity of its hit-position vertices
+                    const uint32_t hs = P.grouped ? __shfl_sync(kFull, st_hs, j) : 0u;
+                    const bool hit_last = P.grouped && ((P.hit_mask >> j) & 1u);
                     if (has_tail && P.tail_const && a.tail_cache) {
                         // the tail count depends on the prefix only: one value per prefix
                         const uint32_t bal = __ballot_sync(kFull, ok);
@@ -915,7 +1006,12 @@ __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
                                 tail_const = tail_const_value(P, s_tc[w]);
                                 dirty = kClean;
                             }
-                            if (lane == 0) { cnt += (unsigned long long)__popc(bal) * tail_const; n_tail += __popc(bal); }
+                            unsigned long long wsum = __popc(bal);
+                            if (P.grouped) {
+                                wsum *= (unsigned long long)(X.n - hs);
+                                if (hit_last) wsum -= X.mult_sum(c, ok);
+                            }
+                            if (lane == 0) { cnt += wsum * tail_const; n_tail += __popc(bal); }
                         }
                     } else if (has_tail) {
                         // every surviving candidate completes a core embedding: count its tail
@@ -937,9 +1033,16 @@ __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
                                                 n_bytes)
                                     : tail_count_warp(P, m, bn, a.rec, a.dvcap, a.pool, a.dval, self_loops, lane,
                                                       n_bytes);
-                            if (lane == 0) { cnt += tc; ++n_tail; }
+                            unsigned long long wt = 1;
+                            if (P.grouped) wt = X.n - hs - (hit_last ? X.mult(cl, lane) : 0u);
+                            if (lane == 0) { cnt += tc * wt; ++n_tail; }
                             __syncwarp();
                         }
+                    } else if (P.grouped) {
+                        const uint32_t nok = __popc(__ballot_sync(kFull, ok));
+                        unsigned long long wsum = (unsigned long long)nok * (X.n - hs);
+                        if (hit_last) wsum -= X.mult_sum(c, ok);
+                        if (lane == 0) cnt += wsum;
                     } else {
                         cnt += ok ? 1ull : 0ull;
                     }
@@ -1567,7 +1670,7 @@ cgb_status cgb_build_index(cgb_handle* h, const uint64_t* keys, uint64_t n, uint
     float avg[kMaxDir] = {0};
     for (uint32_t d = 0; d < h->nd; ++d) avg[d] = nodes[d] ? (float)card[d] / (float)nodes[d] : 0.f;
     cgb::plan_edges(h->q, avg, h->plans, !(h->cfg.flags & CGB_FLAG_ENUMERATE_TAIL),
-                    !(h->cfg.flags & CGB_FLAG_PLAIN_CORE_ORDER));
+                    !(h->cfg.flags & CGB_FLAG_PLAIN_CORE_ORDER), !(h->cfg.flags & CGB_FLAG_NO_SEED_GROUPS));
     CK(cudaMemcpyToSymbol(c_plan, h->plans, sizeof(EdgePlan) * kMaxQE));
     {
         // valid-bit plans from the reference's starting edge

@@ -113,12 +113,17 @@ std::string build_query_meta(uint32_t qv, uint32_t qe, const uint32_t* edges, co
 // cartesian_product.cu:304-427).  Tail vertices are grouped by label (only
 // same-label vertices can collide); groups are limited to 3 members, extra
 // members go back to the core.
-void plan_edges(const QueryMeta& q, const float* avg_deg, EdgePlan* plans, bool analytic_tail, bool pick_last) {
+void plan_edges(const QueryMeta& q, const float* avg_deg, EdgePlan* plans, bool analytic_tail, bool pick_last,
+                bool group_pendant) {
     for (uint32_t ei = 0; ei < q.qe; ++ei) {
         EdgePlan& p = plans[ei];
         std::memset(&p, 0, sizeof(p));
         p.n = (uint8_t)q.qv;
         uint32_t a = q.qe_u[ei], b = q.qe_v[ei];
+        // a pendant endpoint goes to position 1: seeds then arrive sorted by
+        // the other endpoint, one contiguous run per grouped DFS
+        if (q.nbrs[a].size() == 1 && q.nbrs[b].size() > 1) std::swap(a, b);
+        const bool pendant = group_pendant && !q.labels.empty() && q.qv > 2 && q.nbrs[b].size() == 1;
         p.vs[0] = (uint8_t)a;
         p.vs[1] = (uint8_t)b;
         p.seed_dir = q.eidx[a * kMaxQV + b];
@@ -133,6 +138,9 @@ void plan_edges(const QueryMeta& q, const float* avg_deg, EdgePlan* plans, bool 
         // chunked and narrowed.  Such vertices move to the core (`forced`)
         // and the tail and last vertex are chosen again.
         std::vector<char> forced(q.qv, 0), is_tail;
+        if (pendant)  // a tail vertex of the pendant's label would need per-member weights
+            for (uint32_t u = 0; u < q.qv; ++u)
+                if (u != a && u != b && q.labels[u] == q.labels[b]) forced[u] = 1;
         std::vector<uint32_t> tail;
         uint32_t n_core = q.qv;
         int last = -1;
@@ -281,6 +289,11 @@ void plan_edges(const QueryMeta& q, const float* avg_deg, EdgePlan* plans, bool 
                 for (uint32_t b = p.bn_off[t]; b < p.bn_off[t + 1]; ++b) cst &= p.bn_pos[b] != jl;
             }
             p.tail_const = cst ? 1 : 0;
+        }
+        if (pendant) {
+            p.grouped = 1;
+            for (uint32_t j = 2; j < n_core; ++j)
+                if (lab(p.vs[j]) == lab(b)) p.hit_mask |= (uint16_t)(1u << j);
         }
     }
 }

@@ -51,11 +51,19 @@ struct EdgePlan {
     // differs from every tail label, so the tail count is the same for every
     // candidate of the last core position (labels must be known).
     uint8_t tail_const;
-    uint8_t pad;
+    // grouped: vs[1] is a pendant (query degree 1, only neighbour vs[0]) and
+    // no tail vertex shares its label.  Then the count of a seed (x, y)
+    // depends on x only through injectivity, so one DFS per y serves every
+    // seed edge at y: with X = y's delta list towards vs[1] (sorted, the
+    // seeds' x values with multiplicity), each embedding of the other
+    // vertices counts |X| minus the multiplicity in X of the vertices it
+    // places at hit_mask positions (core positions with vs[1]'s label).
+    uint8_t grouped;
     // excl[t] (tail position t): core positions whose matched vertex can lie
     // in t's candidate sets (same label; every core position when labels are
     // unknown); only those are excluded from t's counts.
     uint16_t excl[kMaxQV];
+    uint16_t hit_mask;
 };
 
 // Valid-bit plan of one query edge ei (the reference's 1-bit support masks,
@@ -91,7 +99,9 @@ std::string parse_query_file(const std::string& path, std::vector<uint32_t>& lab
 // avg_deg[dir]: mean run length of direction dir in the initial index.
 // analytic_tail = false keeps every vertex in the enumerated core.
 // pick_last = true puts the core vertex with the fewest tail neighbours last.
+// group_pendant = true groups the seeds of edges with a pendant endpoint
+// (EdgePlan::grouped; needs labels).
 void plan_edges(const QueryMeta& q, const float* avg_deg, EdgePlan* plans, bool analytic_tail = true,
-                bool pick_last = true);
+                bool pick_last = true, bool group_pendant = true);
 
 }  // namespace cgb

@@ -55,6 +55,7 @@ FLAG_NO_TAIL_CACHE = 0x10
 FLAG_PLAIN_CORE_ORDER = 0x20
 FLAG_VALID_BITS = 0x40
 FLAG_MASK_PRUNE = 0x80
+FLAG_NO_SEED_GROUPS = 0x100
 
 
 class BatchKeys(ctypes.Structure):

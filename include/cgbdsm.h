@@ -62,6 +62,7 @@ typedef struct {
 #define CGB_FLAG_PLAIN_CORE_ORDER 0x20u   /* greedy core order only (no choice of the last core vertex) */
 #define CGB_FLAG_VALID_BITS 0x40u         /* compute the reference's valid bits every matched batch     */
 #define CGB_FLAG_MASK_PRUNE 0x80u         /* valid bits, and skip core candidates whose bit is clear    */
+#define CGB_FLAG_NO_SEED_GROUPS 0x100u    /* one DFS per seed even where a pendant endpoint allows one per group */
 
 /* Limits (reference: utils/config.h:5-6; key layout calig_helper_gamma.cu:228-229). */
 #define CGB_MAX_QV 12

@@ -10,8 +10,8 @@ import numpy as np
 import pytest
 
 from cgbdsm_b200 import CgbError, Engine
-from cgbdsm_b200.engine import (FLAG_ENUMERATE_TAIL, FLAG_FORCE_SPLIT, FLAG_MASK_PRUNE, FLAG_NO_TAIL_CACHE,
-                                FLAG_VALID_BITS)
+from cgbdsm_b200.engine import (FLAG_ENUMERATE_TAIL, FLAG_FORCE_SPLIT, FLAG_MASK_PRUNE, FLAG_NO_SEED_GROUPS,
+                                FLAG_NO_TAIL_CACHE, FLAG_VALID_BITS)
 from cgbdsm_b200.workloads import SPECS, materialize, read_query
 from oracle import bind
 
@@ -25,9 +25,9 @@ def _key(d, u, v):
 
 
 @pytest.mark.parametrize("flags", [0, FLAG_ENUMERATE_TAIL, FLAG_FORCE_SPLIT | FLAG_ENUMERATE_TAIL, FLAG_FORCE_SPLIT,
-                                   FLAG_NO_TAIL_CACHE],
+                                   FLAG_NO_TAIL_CACHE, FLAG_NO_SEED_GROUPS],
                          ids=["counted_tail", "enumerated_tail", "stolen_enumerated", "stolen_counted",
-                              "counted_no_prefix_cache"])
+                              "counted_no_prefix_cache", "seed_per_dfs"])
 @pytest.mark.parametrize("name", PIPELINE_CASES)
 def test_engine_matches_reference_cpu_path(name, flags, workdir):
     if not bind.have_ref():
@@ -90,28 +90,68 @@ def test_random_streams_with_self_loops(seed):
     _random_stream(100 + seed, 0.15)
 
 
-def _random_stream(seed, self_loop_rate):
+@pytest.mark.parametrize("seed", range(12))
+def test_random_labelled_streams(seed):
+    """Labelled queries with pendant vertices: seed edges with a pendant
+    endpoint run one DFS per seed group (the other endpoint), each embedding
+    weighted by the group's seeds it does not reuse; the keys respect the
+    labels (as the producer's candidate lists do), duplicate delta pairs and
+    self-loops included.  Every other seed also runs with one DFS per seed."""
+    _random_stream(200 + seed, 0.1 if seed % 3 == 2 else 0.0, nlabels=1 + seed % 3)
+
+
+def _random_stream(seed, self_loop_rate, nlabels=0):
     rng = np.random.default_rng(1000 + seed)
     qv = int(rng.integers(3, 7))
     qedges = _random_query(rng, qv, int(rng.integers(0, 4)))
     dv0 = 60
-    eng = Engine(flags=FLAG_FORCE_SPLIT if seed % 2 else 0)
-    eng.load_query(qv, qedges)
+    flags = FLAG_FORCE_SPLIT if seed % 2 else 0
+    if nlabels and seed % 4 >= 2:
+        flags |= FLAG_NO_SEED_GROUPS
+    eng = Engine(flags=flags)
     orc = bind.Oracle(qv, qedges)
+    if nlabels:
+        # labels: query vertices and data vertices drawn from nlabels values;
+        # a key (a -> b, x, y) only pairs x of a's label with y of b's label
+        qlab = [int(x) for x in rng.integers(0, nlabels, qv)]
+        eng.load_query(qv, qedges, qlab)
+        dlab = rng.integers(0, nlabels, 4096)
+        dlab[:2 * nlabels] = np.arange(2 * nlabels) % nlabels  # hubs 0 .. 2*nlabels-1 cover every label
+    else:
+        eng.load_query(qv, qedges)
+
+    def pick(dv, lab, avoid=-1):
+        while True:
+            x = int(rng.integers(0, dv))
+            if x != avoid and (not nlabels or dlab[x] == lab):
+                return x
 
     def rand_pairs(n, dv):
-        # a third of the pairs touch vertex 0 or 1, so some lists are long
-        # enough (> 96) for the DFS to split them through the work queue
+        # a third of the pairs touch a hub (vertex 0 or 1, or per label), so
+        # some lists are long enough (> 96) for the DFS to split them through
+        # the work queue
         out = []
         for _ in range(n):
             a, b = qedges[int(rng.integers(0, len(qedges)))]
-            x, y = rng.choice(dv, 2, replace=False)
-            if rng.random() < 0.33:
-                x = int(rng.integers(0, 2))
-                if y == x:
-                    y = 2
-            if rng.random() < self_loop_rate:
-                y = x
+            if nlabels:
+                if rng.random() < 0.5:
+                    a, b = b, a
+                la, lb = qlab[a], qlab[b]
+                x = pick(dv, la)
+                if rng.random() < 0.33:
+                    x = la + nlabels * int(rng.integers(0, 2))
+                if rng.random() < self_loop_rate and la == lb:
+                    y = x
+                else:
+                    y = pick(dv, lb, avoid=x)
+            else:
+                x, y = rng.choice(dv, 2, replace=False)
+                if rng.random() < 0.33:
+                    x = int(rng.integers(0, 2))
+                    if y == x:
+                        y = 2
+                if rng.random() < self_loop_rate:
+                    y = x
             out.append((a, b, int(x), int(y)))
         return out
 
