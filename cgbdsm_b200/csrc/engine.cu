@@ -474,7 +474,7 @@ __device__ void tail_prepare(const EdgePlan& P, const uint32_t* m, uint4* bn, un
                              unsigned long long& bytes) {
     const uint32_t nc = P.n_core, n = P.n, j = nc - 1;
     for (uint32_t k = P.bn_off[nc] + lane; k < P.bn_off[n]; k += 32) {
-        if (P.bn_pos[k] >= j) continue;
+        if (P.bn_pos[k] >= j || P.bn_pos[k] < dirty) continue;  // records of unchanged owners are current
         uint4 r = rec[(size_t)P.bn_dir[k] * dvcap + m[P.bn_pos[k]]];
         if (!P.bn_dvis[k]) r.w = 0;
         bn[k] = r;
@@ -643,19 +643,35 @@ struct SeedGroup {
         if (n <= 32) return __popc(__ballot_sync(kFull, xv == c));
         return warp_bound(x, n, c, true, lane) - warp_bound(x, n, c, false, lane);
     }
-    // sum over the lanes with `on` of the multiplicity of their own c
-    __device__ __forceinline__ uint32_t mult_sum(uint32_t c, bool on) const {
+    // sum over the lanes with `on` of the multiplicity of their own c: only
+    // the values of X inside the chunk's range [cmin, cmax] are looked at
+    __device__ __forceinline__ uint32_t mult_sum(uint32_t c, bool on, uint32_t lane) const {
+        uint32_t cmin = on ? c : 0xffffffffu, cmax = on ? c : 0u;
+        for (int o = 16; o > 0; o >>= 1) {
+            cmin = min(cmin, __shfl_xor_sync(kFull, cmin, o));
+            cmax = max(cmax, __shfl_xor_sync(kFull, cmax, o));
+        }
+        if (cmin > cmax) return 0;
         uint32_t r = 0;
         if (n <= 32) {
-            for (uint32_t i = 0; i < n; ++i) r += (__shfl_sync(kFull, xv, i) == c) ? 1u : 0u;
-        } else {
-            uint32_t lo = 0, len = n;
-            while (len > 0) {
-                const uint32_t half = len >> 1;
-                if (__ldg(x + lo + half) < c) { lo += half + 1; len -= half + 1; }
-                else len = half;
+            uint32_t bits = __ballot_sync(kFull, lane < n && xv >= cmin && xv <= cmax);
+            while (bits) {
+                const uint32_t i = __ffs(bits) - 1;
+                bits &= bits - 1;
+                r += (__shfl_sync(kFull, xv, i) == c) ? 1u : 0u;
             }
-            for (uint32_t i = lo; i < n && __ldg(x + i) == c; ++i) ++r;
+        } else {
+            const uint32_t lo = warp_bound(x, n, cmin, false, lane), hi = warp_bound(x, n, cmax, true, lane);
+            if (lo == hi) return 0;
+            if (on) {
+                uint32_t p = lo, len = hi - lo;
+                while (len > 0) {
+                    const uint32_t half = len >> 1;
+                    if (__ldg(x + p + half) < c) { p += half + 1; len -= half + 1; }
+                    else len = half;
+                }
+                for (; p < hi && __ldg(x + p) == c; ++p) ++r;
+            }
         }
         r = on ? r : 0u;
         for (int o = 16; o > 0; o >>= 1) r += __shfl_xor_sync(kFull, r, o);
@@ -1001,15 +1017,15 @@ __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
                         // the tail count depends on the prefix only: one value per prefix
                         const uint32_t bal = __ballot_sync(kFull, ok);
                         if (bal) {
-                            if (dirty != kClean) {
+                            if (dirty <= P.tail_dep) {
                                 tail_prepare(P, m, bn, s_tc[w], dirty, a.rec, a.dvcap, a.pool, a.dval, self_loops, lane, n_bytes);
                                 tail_const = tail_const_value(P, s_tc[w]);
-                                dirty = kClean;
                             }
+                            dirty = kClean;
                             unsigned long long wsum = __popc(bal);
                             if (P.grouped) {
                                 wsum *= (unsigned long long)(X.n - hs);
-                                if (hit_last) wsum -= X.mult_sum(c, ok);
+                                if (hit_last) wsum -= X.mult_sum(c, ok, lane);
                             }
                             if (lane == 0) { cnt += wsum * tail_const; n_tail += __popc(bal); }
                         }
@@ -1020,11 +1036,11 @@ __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
                             const int l = __ffs(bal) - 1;
                             bal &= bal - 1;
                             const uint32_t cl = __shfl_sync(kFull, c, l);
-                            if (dirty != kClean && a.tail_cache) {
+                            if (dirty <= P.tail_dep && a.tail_cache) {
                                 // first embedding since the prefix changed: recount the stale prefix-only subsets
                                 tail_prepare(P, m, bn, s_tc[w], dirty, a.rec, a.dvcap, a.pool, a.dval, self_loops, lane, n_bytes);
-                                dirty = kClean;
                             }
+                            dirty = kClean;
                             if (lane == 0) m[j] = cl;
                             __syncwarp();
                             const unsigned long long tc =
@@ -1041,7 +1057,7 @@ __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
                     } else if (P.grouped) {
                         const uint32_t nok = __popc(__ballot_sync(kFull, ok));
                         unsigned long long wsum = (unsigned long long)nok * (X.n - hs);
-                        if (hit_last) wsum -= X.mult_sum(c, ok);
+                        if (hit_last) wsum -= X.mult_sum(c, ok, lane);
                         if (lane == 0) cnt += wsum;
                     } else {
                         cnt += ok ? 1ull : 0ull;

@@ -290,6 +290,12 @@ void plan_edges(const QueryMeta& q, const float* avg_deg, EdgePlan* plans, bool 
             }
             p.tail_const = cst ? 1 : 0;
         }
+        for (uint32_t t = n_core; t < q.qv; ++t) {
+            for (uint32_t b2 = p.bn_off[t]; b2 < p.bn_off[t + 1]; ++b2)
+                if (p.bn_pos[b2] + 1u < n_core) p.tail_dep = std::max<uint8_t>(p.tail_dep, p.bn_pos[b2]);
+            for (uint32_t c = 0; c + 1 < n_core; ++c)
+                if ((p.excl[t] >> c) & 1u) p.tail_dep = std::max<uint8_t>(p.tail_dep, (uint8_t)c);
+        }
         if (pendant) {
             p.grouped = 1;
             for (uint32_t j = 2; j < n_core; ++j)

@@ -64,6 +64,10 @@ struct EdgePlan {
     // unknown); only those are excluded from t's counts.
     uint16_t excl[kMaxQV];
     uint16_t hit_mask;
+    // tail_dep: the deepest core position below n_core - 1 that a tail count
+    // reads (a list's owner or an excluded vertex); a prefix change at a
+    // deeper position leaves every prefix-only tail count as it was.
+    uint8_t tail_dep;
 };
 
 // Valid-bit plan of one query edge ei (the reference's 1-bit support masks,
