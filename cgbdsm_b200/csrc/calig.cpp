@@ -441,60 +441,94 @@ bool CaLiGIndex::check_nei(uint32_t v, uint32_t u) {
 }
 
 // Both fix-points below run on threads_ threads (large rounds), thread k
-// owning every data vertex v with owner(v, T) == k: the candidate lists of v, its
-// LI and checked bits.  A round first scans the task lists read-only (every
-// thread scans all of them and keeps the items whose target vertex it owns,
-// so each thread sees its items in the reference's queue order), then each
-// thread edits only the lists it owns.  The sequential round reads the
-// pre-round lists and LI while building its work list, and its set results
-// (list contents, deltas, the next queue) do not depend on the order of the
-// edits; the one order-dependent step — which same-label group a checked
-// (u, v) is tested against — depends on the order of v's own items only,
-// which the owner keeps.
+// owning every data vertex v with owner(v, T) == k: the candidate lists of v,
+// its LI and checked bits.  A round first scans the task queue read-only in
+// T slices of about equal list length, thread s dropping each item into the
+// bucket of its target vertex's owner; then each owner takes its buckets in
+// slice order (so it sees its items in the reference's queue order) and
+// edits only the lists it owns.  The sequential round reads the pre-round
+// lists and LI while building its work list, and its set results (list
+// contents, deltas, the next queue) do not depend on the order of the edits;
+// the one order-dependent step — which same-label group a checked (u, v) is
+// tested against — depends on the order of v's own items only, which the
+// owner keeps.
+
+// Splits the tasks into T slices of about equal total list length (the
+// scan's cost): slice s is tasks [cut[s], cut[s + 1]).  Returns the total.
+size_t CaLiGIndex::slice_tasks(const std::vector<Task>& q, uint32_t T, std::vector<size_t>& cut) {
+    std::vector<size_t> pre(q.size() + 1, 0);
+    for (size_t i = 0; i < q.size(); ++i) {
+        size_t w = 1;
+        for (uint32_t uj : qnei_[q[i].u]) w += C(q[i].v, q[i].u, uj).size();
+        pre[i + 1] = pre[i] + w;
+    }
+    cut.assign(T + 1, q.size());
+    cut[0] = 0;
+    for (uint32_t s = 1; s < T; ++s)
+        cut[s] = (size_t)(std::lower_bound(pre.begin(), pre.end(), pre.back() * s / T) - pre.begin());
+    return pre.back();
+}
 
 // calig.cpp:410-475 delAndCheck (one round; `del` becomes the next round).
 void CaLiGIndex::del_and_check(std::vector<Task>& del) {
     dedupe(del);
-    size_t work = 0;
-    for (auto& t : del)
-        for (uint32_t uj : qnei_[t.u]) work += C(t.v, t.u, uj).size();
-    const uint32_t T = work >= par_min_ ? threads_ : 1u;
+    std::vector<size_t> cut;
+    const uint32_t T = slice_tasks(del, threads_, cut) >= par_min_ ? threads_ : 1u;
+    if (T == 1) cut = {0, del.size()};
     struct Item { uint64_t list; uint32_t vi, vj, ui, uj; };
-    std::vector<std::vector<Item>> items(T);
-    run_threads(T, [&](uint32_t k) {
-        for (auto& t : del)
+    std::vector<std::vector<Item>> items((size_t)T * T);  // [slice * T + owner]
+    run_threads(T, [&](uint32_t s) {
+        for (size_t i = cut[s]; i < cut[s + 1]; ++i) {
+            const Task& t = del[i];
             for (uint32_t uj : qnei_[t.u])
                 for (uint32_t vj : C(t.v, t.u, uj))
-                    if (owner(vj, T) == k && lit(vj, uj)) items[k].push_back({list_index(vj, uj, t.u), t.v, vj, t.u, uj});
+                    if (lit(vj, uj))
+                        items[(size_t)s * T + owner(vj, T)].push_back({list_index(vj, uj, t.u), t.v, vj, t.u, uj});
+        }
     });
     struct Chk { uint32_t u, v; int group; };
     std::vector<std::vector<Task>> next(T);
     std::vector<std::vector<DeltaOp>> erased(T);
     run_threads(T, [&](uint32_t k) {
-        const auto& it = items[k];
+        std::vector<Item> it;
+        for (uint32_t s = 0; s < T; ++s) {
+            auto& b = items[(size_t)s * T + k];
+            it.insert(it.end(), b.begin(), b.end());
+            std::vector<Item>().swap(b);
+        }
         // erase each list's values in one pass; a list that ends empty turns
         // its (uj, vj) off (the sequential round sees it empty at its last
         // item; earlier items' group checks of a vertex that ends off change
         // nothing)
-        // (list, vi << 32 | item) keys: grouped by list, values ascending
-        std::vector<std::pair<uint64_t, uint64_t>> ord(it.size());
-        for (size_t i = 0; i < it.size(); ++i) ord[i] = {it[i].list, (uint64_t)it[i].vi << 32 | i};
-        std::sort(ord.begin(), ord.end());
+        // Group the items by list.  Within a list they arrive in ascending
+        // vi (the queue is sorted by vertex and the slices keep its order),
+        // so (list, item) keys, packed into one word when they fit, order
+        // every group by value as erase_run needs.
+        std::vector<uint32_t> ord(it.size());
+        const int ib = std::max(1, 64 - __builtin_clzll((unsigned long long)it.size() | 1ull));
+        if (lists_.size() < (1ull << (64 - ib))) {
+            std::vector<uint64_t> key(it.size());
+            for (size_t i = 0; i < it.size(); ++i) key[i] = it[i].list << ib | i;
+            std::sort(key.begin(), key.end());
+            for (size_t i = 0; i < it.size(); ++i) ord[i] = (uint32_t)(key[i] & ((1ull << ib) - 1));
+        } else {
+            std::iota(ord.begin(), ord.end(), 0u);
+            std::stable_sort(ord.begin(), ord.end(), [&](uint32_t a, uint32_t b) { return it[a].list < it[b].list; });
+        }
         std::vector<uint8_t> ends_empty(it.size()), hit;
         std::vector<uint32_t> vals;
         for (size_t g0 = 0; g0 < ord.size();) {
             size_t g1 = g0 + 1;
-            while (g1 < ord.size() && ord[g1].first == ord[g0].first) ++g1;
+            while (g1 < ord.size() && it[ord[g1]].list == it[ord[g0]].list) ++g1;
             vals.clear();
-            for (size_t q = g0; q < g1; ++q) vals.push_back((uint32_t)(ord[q].second >> 32));
+            for (size_t q = g0; q < g1; ++q) vals.push_back(it[ord[q]].vi);
             hit.assign(vals.size(), 0);
-            auto& L = lists_[ord[g0].first];
+            auto& L = lists_[it[ord[g0]].list];
             erase_run(L, vals.data(), vals.size(), hit.data());
             for (size_t q = g0; q < g1; ++q) {
-                const uint32_t i = (uint32_t)ord[q].second;
-                const Item& e = it[i];
+                const Item& e = it[ord[q]];
                 if (hit[q - g0]) erased[k].push_back({e.vj, e.vi, e.uj, e.ui});
-                ends_empty[i] = L.empty();
+                ends_empty[ord[q]] = L.empty();
             }
             g0 = g1;
         }
@@ -547,62 +581,79 @@ void CaLiGIndex::add_and_check(std::vector<Task>& add, std::vector<Task>& settle
                                std::vector<Task>& add_del, std::vector<Task>& activated) {
     dedupe(add);
     dedupe(settled);
-    size_t work = 0;
-    for (auto* q : {&add, &settled})
-        for (auto& t : *q)
-            for (uint32_t uj : qnei_[t.u]) work += C(t.v, t.u, uj).size();
-    const uint32_t T = work >= par_min_ ? threads_ : 1u;
-    struct Ins { uint64_t list; uint32_t vi, vj, ui, uj; };
-    std::vector<std::vector<Ins>> ins(T);
-    std::vector<std::vector<Task>> check(T);
-    run_threads(T, [&](uint32_t k) {
-        for (int pass = 0; pass < 2; ++pass)
-            for (auto& t : pass ? settled : add)
-                for (uint32_t uj : qnei_[t.u])
-                    for (uint32_t vj : C(t.v, t.u, uj)) {
-                        if (owner(vj, T) != k) continue;
-                        if (!pass) {
-                            const uint64_t L = list_index(vj, uj, t.u);
-                            if (!sorted_has(lists_[L], t.v)) ins[k].push_back({L, t.v, vj, t.u, uj});
-                        }
-                        if (!lit(vj, uj)) {
-                            check[k].push_back({uj, vj});
-                            checked_[vj] &= ~(1u << uj);
-                        }
-                    }
-    });
+    // one queue: activations first, then the settled tasks
+    const size_t nfresh = add.size();
+    add.insert(add.end(), settled.begin(), settled.end());
     settled.clear();
+    std::vector<size_t> cut;
+    const uint32_t T = slice_tasks(add, threads_, cut) >= par_min_ ? threads_ : 1u;
+    if (T == 1) cut = {0, add.size()};
+    struct Ins { uint64_t list; uint32_t vi, vj, ui, uj; };
+    std::vector<std::vector<Ins>> ins((size_t)T * T);     // [slice * T + owner]
+    std::vector<std::vector<Task>> check((size_t)T * T);
+    run_threads(T, [&](uint32_t s) {
+        for (size_t i = cut[s]; i < cut[s + 1]; ++i) {
+            const Task& t = add[i];
+            const bool fresh = i < nfresh;
+            for (uint32_t uj : qnei_[t.u])
+                for (uint32_t vj : C(t.v, t.u, uj)) {
+                    const size_t b = (size_t)s * T + owner(vj, T);
+                    if (fresh) ins[b].push_back({list_index(vj, uj, t.u), t.v, vj, t.u, uj});
+                    if (!lit(vj, uj)) check[b].push_back({uj, vj});
+                }
+        }
+    });
     std::vector<std::vector<Task>> next(T), act(T), drop(T);
     std::vector<std::vector<DeltaOp>> added(T);
     run_threads(T, [&](uint32_t k) {
-        auto& it = ins[k];
-        std::sort(it.begin(), it.end(), [](const Ins& a, const Ins& b) {
+        // Lookups: dependent cache misses (list header, then list words), run
+        // in groups whose next lines are prefetched for the whole group.
+        std::vector<Ins> miss;
+        constexpr size_t kGroup = 16;
+        for (uint32_t s = 0; s < T; ++s) {
+            const auto& b = ins[(size_t)s * T + k];
+            for (size_t g0 = 0; g0 < b.size(); g0 += kGroup) {
+                const size_t g1 = std::min(b.size(), g0 + kGroup);
+                for (size_t i = g0; i < g1; ++i) __builtin_prefetch(&lists_[b[i].list]);
+                for (size_t i = g0; i < g1; ++i) {
+                    const auto& L = lists_[b[i].list];
+                    if (!L.empty()) __builtin_prefetch(L.data() + L.size() / 2);
+                }
+                for (size_t i = g0; i < g1; ++i)
+                    if (!sorted_has(lists_[b[i].list], b[i].vi)) miss.push_back(b[i]);
+            }
+        }
+        std::sort(miss.begin(), miss.end(), [](const Ins& a, const Ins& b) {
             return a.list != b.list ? a.list < b.list : a.vi < b.vi;
         });
         std::vector<uint32_t> vals;
-        for (size_t g0 = 0; g0 < it.size();) {
+        for (size_t g0 = 0; g0 < miss.size();) {
             size_t g1 = g0 + 1;
-            while (g1 < it.size() && it[g1].list == it[g0].list) ++g1;
+            while (g1 < miss.size() && miss[g1].list == miss[g0].list) ++g1;
             vals.clear();
             for (size_t q = g0; q < g1; ++q) {
-                vals.push_back(it[q].vi);
-                added[k].push_back({it[q].vj, it[q].vi, it[q].uj, it[q].ui});
+                vals.push_back(miss[q].vi);
+                added[k].push_back({miss[q].vj, miss[q].vi, miss[q].uj, miss[q].ui});
             }
-            insert_run(lists_[it[g0].list], vals.data(), vals.size());
+            insert_run(lists_[miss[g0].list], vals.data(), vals.size());
             g0 = g1;
         }
+        // checks: clear the round's checked bits, then test each (u, v) once;
         // check_nei(v, u) reads v's own lists only, all final for this round
-        for (auto& c : check[k]) {
-            if ((checked_[c.v] >> c.u) & 1u) continue;
-            checked_[c.v] |= 1u << c.u;
-            if (check_nei(c.v, c.u)) {
-                li_[c.v] |= 1u << c.u;
-                next[k].push_back(c);
-                act[k].push_back(c);
-            } else {
-                drop[k].push_back(c);
+        for (uint32_t s = 0; s < T; ++s)
+            for (auto& c : check[(size_t)s * T + k]) checked_[c.v] &= ~(1u << c.u);
+        for (uint32_t s = 0; s < T; ++s)
+            for (auto& c : check[(size_t)s * T + k]) {
+                if ((checked_[c.v] >> c.u) & 1u) continue;
+                checked_[c.v] |= 1u << c.u;
+                if (check_nei(c.v, c.u)) {
+                    li_[c.v] |= 1u << c.u;
+                    next[k].push_back(c);
+                    act[k].push_back(c);
+                } else {
+                    drop[k].push_back(c);
+                }
             }
-        }
     });
     concat(delta_ins, added);
     concat(activated, act);

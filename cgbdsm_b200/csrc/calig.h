@@ -97,6 +97,7 @@ private:
     void add_and_check(std::vector<Task>& add, std::vector<Task>& settled, std::vector<Task>& add_del,
                        std::vector<Task>& activated);
     void del_and_check(std::vector<Task>& del);
+    size_t slice_tasks(const std::vector<Task>& q, uint32_t T, std::vector<size_t>& cut);
 };
 
 }  // namespace cgb
