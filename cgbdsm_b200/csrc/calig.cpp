@@ -372,45 +372,101 @@ void CaLiGIndex::set_threads(uint32_t n) {
     if (const char* e = std::getenv("CGB_PRODUCER_MIN_PARALLEL")) par_min_ = std::strtoull(e, nullptr, 10);
 }
 
-// calig.cpp:325-356 constructCand, then 705-717 staticFilter.
+void EdgeSet::reset(size_t max_edges) {
+    size_t cap = 1024;
+    while (cap < max_edges + max_edges / 2) cap <<= 1;
+    slots_.assign(cap, kEmpty);
+    bits_ = __builtin_ctzll(cap);
+    count_ = 0;
+}
+
+void EdgeSet::reserve(size_t more) {
+    if ((count_ + more) * 4 <= slots_.size() * 3) return;
+    std::vector<uint64_t> old;
+    old.swap(slots_);
+    reset(count_ + more);
+    for (uint64_t k : old)
+        if (k != kEmpty) insert((uint32_t)(k >> 32), (uint32_t)k);
+}
+
+bool EdgeSet::has(uint32_t a, uint32_t b) const {
+    const uint64_t k = key(a, b);
+    for (size_t i = slot(k);; i = (i + 1) & (slots_.size() - 1)) {
+        const uint64_t s = __atomic_load_n(&slots_[i], __ATOMIC_RELAXED);
+        if (s == k) return true;
+        if (s == kEmpty) return false;
+    }
+}
+
+void EdgeSet::insert(uint32_t a, uint32_t b) {
+    const uint64_t k = key(a, b);
+    for (size_t i = slot(k);; i = (i + 1) & (slots_.size() - 1)) {
+        uint64_t s = __atomic_load_n(&slots_[i], __ATOMIC_RELAXED);
+        if (s == k) return;
+        if (s == kEmpty) {
+            if (__atomic_compare_exchange_n(&slots_[i], &s, k, false, __ATOMIC_RELAXED, __ATOMIC_RELAXED)) {
+                __atomic_fetch_add(&count_, 1, __ATOMIC_RELAXED);
+                return;
+            }
+            if (s == k) return;  // another thread put the same key here
+        }
+    }
+}
+
+// calig.cpp:325-356 constructCand, then 705-717 staticFilter.  Vertices are
+// independent in both (each writes its own lists and LI), so they run on
+// slices of the vertex range.
 void CaLiGIndex::construct() {
     const uint32_t n = (uint32_t)glabel_.size();
     cbase_.assign(n + 1, 0);
     uint64_t total = 0;
+    size_t adj = 0;
     for (uint32_t v = 0; v < n; ++v) {
         cbase_[v] = total;
         if (glabel_[v] >= 0) total += block_size_[glabel_[v]];
+        adj += nei_[v].size();
     }
     cbase_[n] = total;
     lists_.assign(total, {});
-    for (uint32_t v = 0; v < n; ++v) {
-        li_[v] = 0;
-        checked_[v] = 0;
-        const int s = glabel_[v];
-        if (s < 0) continue;
-        for (uint32_t ui : qlist_[s]) {
-            for (uint32_t vj : nei_[v]) {
-                const int lj = glabel_[vj];
-                if (lj < 0) continue;
-                for (uint32_t uj : qnei_[ui])
-                    if (label_slot_[qlabel_[uj]] == lj) C(v, ui, uj).push_back(vj);  // nei_ sorted -> lists sorted
+    edges_.reset(adj / 2 + update_.size() / 2);
+    const uint32_t T = n >= par_min_ ? threads_ : 1u;
+    std::vector<std::vector<Task>> delp(T);
+    run_threads(T, [&](uint32_t s) {
+        const uint32_t v0 = (uint32_t)((uint64_t)n * s / T), v1 = (uint32_t)((uint64_t)n * (s + 1) / T);
+        for (uint32_t v = v0; v < v1; ++v) {
+            li_[v] = 0;
+            checked_[v] = 0;
+            for (uint32_t y : nei_[v])
+                if (v <= y) edges_.insert(v, y);
+            const int sl = glabel_[v];
+            if (sl < 0) continue;
+            for (uint32_t ui : qlist_[sl]) {
+                for (uint32_t vj : nei_[v]) {
+                    const int lj = glabel_[vj];
+                    if (lj < 0) continue;
+                    for (uint32_t uj : qnei_[ui])
+                        if (label_slot_[qlabel_[uj]] == lj) C(v, ui, uj).push_back(vj);  // nei_ sorted -> lists sorted
+                }
+                li_[v] |= 1u << ui;
             }
-            li_[v] |= 1u << ui;
         }
-    }
-    // staticFilter: turnOff every lit (v, ui) failing checkNei, then delAndCheck to the fix-point
+        // staticFilter: turnOff every lit (v, ui) failing checkNei (v's own lists only)
+        for (uint32_t v = v0; v < v1; ++v) {
+            const int sl = glabel_[v];
+            if (sl < 0) continue;
+            for (uint32_t ui : qlist_[sl]) {
+                if (!lit(v, ui)) continue;
+                if (!check_nei(v, ui)) {
+                    li_[v] &= ~(1u << ui);
+                    delp[s].push_back({ui, v});
+                }
+            }
+        }
+    });
+    std::vector<std::vector<uint32_t>>().swap(nei_);
+    // then delAndCheck to the fix-point
     std::vector<Task> del;
-    for (uint32_t v = 0; v < n; ++v) {
-        const int s = glabel_[v];
-        if (s < 0) continue;
-        for (uint32_t ui : qlist_[s]) {
-            if (!lit(v, ui)) continue;
-            if (!check_nei(v, ui)) {
-                li_[v] &= ~(1u << ui);
-                del.push_back({ui, v});
-            }
-        }
-    }
+    concat(del, delp);
     delta_del.clear();
     while (!del.empty()) del_and_check(del);
     delta_del.clear();
@@ -684,7 +740,7 @@ void CaLiGIndex::update_index(uint32_t start, uint32_t count) {
             if (a < 0 || b < 0 || (uint32_t)a >= n || (uint32_t)b >= n) continue;
             const uint32_t v1 = (uint32_t)a, v2 = (uint32_t)b;
             if (glabel_[v1] < 0 || glabel_[v2] < 0) continue;
-            if (sorted_has(nei_[v1], v2)) continue;  // edge exists before this batch
+            if (edges_.has(v1, v2)) continue;  // edge exists before this batch
             ups[s].emplace_back(v1, v2);
             for (int o = 0; o < 2; ++o) {
                 const uint32_t x = o ? v2 : v1, y = o ? v1 : v2;
@@ -694,16 +750,16 @@ void CaLiGIndex::update_index(uint32_t start, uint32_t count) {
             }
         }
     });
-    // Adjacency and candidate-list inserts, then turnOnCheck (calig.cpp:657-693),
-    // by owner of the first vertex: its lists, LI and checked bits.
+    // The batch's edges join the edge set (all pairs of slice k on thread k);
+    // candidate-list inserts, then turnOnCheck (calig.cpp:657-693), by owner
+    // of the first vertex: its lists, LI and checked bits.
     std::vector<std::vector<Task>> addp(T), setp(T), actp(T);
+    size_t nup = 0;
+    for (auto& part : ups) nup += part.size();
+    edges_.reserve(nup);
     run_threads(T, [&](uint32_t k) {
+        for (auto& [x, y] : ups[k]) edges_.insert(x, y);
         std::vector<std::pair<uint64_t, uint32_t>> ins;
-        for (auto& part : ups)
-            for (auto& [x, y] : part) {
-                if (owner(x, T) == k) ins.emplace_back(x, y);
-                if (owner(y, T) == k) ins.emplace_back(y, x);
-            }
         std::vector<uint32_t> vals;
         auto apply = [&](auto&& list_of) {
             std::sort(ins.begin(), ins.end());
@@ -716,8 +772,6 @@ void CaLiGIndex::update_index(uint32_t start, uint32_t count) {
                 g0 = g1;
             }
         };
-        apply([&](uint64_t x) -> std::vector<uint32_t>& { return nei_[x]; });
-        ins.clear();
         std::vector<Task> check;
         for (auto& part : tmp)
             for (auto& t : part) {

@@ -21,6 +21,28 @@ struct DeltaOp {  // calig.h:35
     uint32_t vi, vj, ui, uj;
 };
 
+// Set of undirected data edges, for updateIndex's test whether a batch pair
+// is an edge already (calig.cpp:972-975): open addressing with linear
+// probing over keys min << 32 | max, sized when built for every edge the
+// update stream can add (load <= 2/3, no growth); inserts are lock-free (a
+// compare-and-swap on the empty slot), so batch pairs go in from all threads.
+class EdgeSet {
+public:
+    void reset(size_t max_edges);
+    // room for `more` inserts at load <= 3/4 (rehashes; single-threaded)
+    void reserve(size_t more);
+    bool has(uint32_t a, uint32_t b) const;
+    void insert(uint32_t a, uint32_t b);
+
+private:
+    static constexpr uint64_t kEmpty = ~0ull;  // no key: vertex ids are < 2^32 - 1
+    std::vector<uint64_t> slots_;
+    int bits_ = 10;
+    size_t count_ = 0;  // keys held (updated atomically by insert)
+    static uint64_t key(uint32_t a, uint32_t b) { return a < b ? (uint64_t)a << 32 | b : (uint64_t)b << 32 | a; }
+    size_t slot(uint64_t k) const { return (size_t)((k * 0x9E3779B97F4A7C15ull) >> (64 - bits_)); }
+};
+
 class CaLiGIndex {
 public:
     // Loading (reference text formats, calig.cpp:111-216, 719-733).
@@ -72,7 +94,8 @@ private:
 
     // data
     std::vector<int> glabel_;        // dense label index or -1 (pruned)
-    std::vector<std::vector<uint32_t>> nei_;
+    std::vector<std::vector<uint32_t>> nei_;  // adjacency while loading and constructing; freed after
+    EdgeSet edges_;                           // the data edges from construct() on
     std::vector<uint64_t> cbase_;    // per vertex: first list index
     std::vector<std::vector<uint32_t>> lists_;
     std::vector<uint32_t> li_, checked_;
