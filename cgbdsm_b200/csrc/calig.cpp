@@ -153,14 +153,36 @@ void concat(std::vector<T>& dst, std::vector<std::vector<T>>& parts) {
     for (auto& p : parts) dst.insert(dst.end(), p.begin(), p.end());
 }
 
-// Sorts and deduplicates a task queue.  Repeated tasks in the reference's
-// queues only redo inserts that fail and checks guarded by the checked bit, so
-// processing each distinct task once yields the same index and deltas.
+// LSD radix sort of keys by their low `bits` bits, 11 bits per pass.
+void radix_sort(std::vector<uint64_t>& a, int bits) {
+    std::vector<uint64_t> b(a.size());
+    std::vector<size_t> cnt(2049);
+    for (int shift = 0; shift < bits; shift += 11) {
+        std::fill(cnt.begin(), cnt.end(), 0);
+        for (uint64_t x : a) ++cnt[((x >> shift) & 2047) + 1];
+        for (int i = 0; i < 2048; ++i) cnt[i + 1] += cnt[i];
+        for (uint64_t x : a) b[cnt[(x >> shift) & 2047]++] = x;
+        a.swap(b);
+    }
+}
+
+// Sorts a task queue by (v, u) and drops repeats.  Repeated tasks in the
+// reference's queues only redo inserts that fail and checks guarded by the
+// checked bit, so processing each distinct task once yields the same index
+// and deltas.  Keys v << 5 | u (query vertices < 32), radix-sorted.
 template <typename T>
 void dedupe(std::vector<T>& q) {
-    std::sort(q.begin(), q.end(), [](const T& a, const T& b) { return a.v != b.v ? a.v < b.v : a.u < b.u; });
-    q.erase(std::unique(q.begin(), q.end(), [](const T& a, const T& b) { return a.v == b.v && a.u == b.u; }),
-            q.end());
+    if (q.size() < 2) return;
+    std::vector<uint64_t> key(q.size());
+    uint64_t top = 0;
+    for (size_t i = 0; i < q.size(); ++i) {
+        key[i] = (uint64_t)q[i].v << 5 | q[i].u;
+        top |= key[i];
+    }
+    radix_sort(key, 64 - __builtin_clzll(top | 1));
+    key.erase(std::unique(key.begin(), key.end()), key.end());
+    q.resize(key.size());
+    for (size_t i = 0; i < key.size(); ++i) q[i] = {(uint32_t)(key[i] & 31u), (uint32_t)(key[i] >> 5)};
 }
 
 }  // namespace
@@ -429,12 +451,14 @@ void CaLiGIndex::construct() {
     cbase_[n] = total;
     lists_.assign(total, {});
     edges_.reset(adj / 2 + update_.size() / 2);
+    li_.assign(n, 0);
+    words_ = (n + 63) / 64;
+    litbits_.assign((size_t)qn_ * words_, 0);
     const uint32_t T = n >= par_min_ ? threads_ : 1u;
     std::vector<std::vector<Task>> delp(T);
     run_threads(T, [&](uint32_t s) {
         const uint32_t v0 = (uint32_t)((uint64_t)n * s / T), v1 = (uint32_t)((uint64_t)n * (s + 1) / T);
         for (uint32_t v = v0; v < v1; ++v) {
-            li_[v] = 0;
             checked_[v] = 0;
             for (uint32_t y : nei_[v])
                 if (v <= y) edges_.insert(v, y);
@@ -447,7 +471,7 @@ void CaLiGIndex::construct() {
                     for (uint32_t uj : qnei_[ui])
                         if (label_slot_[qlabel_[uj]] == lj) C(v, ui, uj).push_back(vj);  // nei_ sorted -> lists sorted
                 }
-                li_[v] |= 1u << ui;
+                light(v, ui);
             }
         }
         // staticFilter: turnOff every lit (v, ui) failing checkNei (v's own lists only)
@@ -457,7 +481,7 @@ void CaLiGIndex::construct() {
             for (uint32_t ui : qlist_[sl]) {
                 if (!lit(v, ui)) continue;
                 if (!check_nei(v, ui)) {
-                    li_[v] &= ~(1u << ui);
+                    unlight(v, ui);
                     delp[s].push_back({ui, v});
                 }
             }
@@ -499,8 +523,8 @@ bool CaLiGIndex::check_nei(uint32_t v, uint32_t u) {
 // Both fix-points below run on threads_ threads (large rounds), thread k
 // owning every data vertex v with owner(v, T) == k: the candidate lists of v,
 // its LI and checked bits.  A round first scans the task queue read-only in
-// T slices of about equal list length, thread s dropping each item into the
-// bucket of its target vertex's owner; then each owner takes its buckets in
+// T slices of equal item count, thread s dropping each item into the bucket
+// of its target vertex's owner; then each owner takes its buckets in
 // slice order (so it sees its items in the reference's queue order) and
 // edits only the lists it owns.  The sequential round reads the pre-round
 // lists and LI while building its work list, and its set results (list
@@ -509,38 +533,66 @@ bool CaLiGIndex::check_nei(uint32_t v, uint32_t u) {
 // tested against — depends on the order of v's own items only, which the
 // owner keeps.
 
-// Splits the tasks into T slices of about equal total list length (the
-// scan's cost): slice s is tasks [cut[s], cut[s + 1]).  Returns the total.
-size_t CaLiGIndex::slice_tasks(const std::vector<Task>& q, uint32_t T, std::vector<size_t>& cut) {
-    std::vector<size_t> pre(q.size() + 1, 0);
-    for (size_t i = 0; i < q.size(); ++i) {
-        size_t w = 1;
-        for (uint32_t uj : qnei_[q[i].u]) w += C(q[i].v, q[i].u, uj).size();
-        pre[i + 1] = pre[i] + w;
+// The items of a round are the entries of the lists C(t.v, t.u, uj) of every
+// task t and every uj in qnei_[t.u], in queue order.  segments() lists one
+// Seg per such list with the index of its first item and returns the item
+// count; scan_items() visits items [lo, hi) in order, so T threads can take
+// equal shares even when one hub task holds most of a round.
+size_t CaLiGIndex::segments(const std::vector<Task>& q, std::vector<Seg>& segs) {
+    // the list headers are cache misses: tasks in T index slices, then the
+    // slices' item offsets shifted by the running total
+    const uint32_t n = (uint32_t)q.size();
+    const uint32_t T = n >= par_min_ / 8 ? threads_ : 1u;
+    std::vector<std::vector<Seg>> part(T);
+    std::vector<size_t> sum(T + 1, 0);
+    run_threads(T, [&](uint32_t s) {
+        size_t total = 0;
+        for (uint32_t i = (uint32_t)((uint64_t)n * s / T); i < (uint32_t)((uint64_t)n * (s + 1) / T); ++i)
+            for (uint32_t uj : qnei_[q[i].u]) {
+                const size_t len = C(q[i].v, q[i].u, uj).size();
+                if (len) part[s].push_back({i, uj, total});
+                total += len;
+            }
+        sum[s + 1] = total;
+    });
+    segs.clear();
+    for (uint32_t s = 0; s < T; ++s) {
+        sum[s + 1] += sum[s];
+        for (auto& sg : part[s]) segs.push_back({sg.task, sg.uj, sg.first + sum[s]});
     }
-    cut.assign(T + 1, q.size());
-    cut[0] = 0;
-    for (uint32_t s = 1; s < T; ++s)
-        cut[s] = (size_t)(std::lower_bound(pre.begin(), pre.end(), pre.back() * s / T) - pre.begin());
-    return pre.back();
+    return sum[T];
+}
+
+template <class Fn>
+void CaLiGIndex::scan_items(const std::vector<Task>& q, const std::vector<Seg>& segs, size_t lo, size_t hi,
+                            Fn&& fn) {
+    if (lo >= hi) return;
+    size_t g = (size_t)(std::upper_bound(segs.begin(), segs.end(), lo,
+                                         [](size_t x, const Seg& sg) { return x < sg.first; }) - segs.begin()) - 1;
+    for (size_t at = lo; at < hi && g < segs.size(); ++g) {
+        const Seg& sg = segs[g];
+        const Task& t = q[sg.task];
+        const auto& L = C(t.v, t.u, sg.uj);
+        const size_t end = std::min(hi, sg.first + L.size());
+        for (size_t p = at - sg.first; sg.first + p < end; ++p) fn(sg.task, t, sg.uj, L[p]);
+        at = end;
+    }
 }
 
 // calig.cpp:410-475 delAndCheck (one round; `del` becomes the next round).
 void CaLiGIndex::del_and_check(std::vector<Task>& del) {
     dedupe(del);
-    std::vector<size_t> cut;
-    const uint32_t T = slice_tasks(del, threads_, cut) >= par_min_ ? threads_ : 1u;
-    if (T == 1) cut = {0, del.size()};
+    std::vector<Seg> segs;
+    const size_t total = segments(del, segs);
+    const uint32_t T = total >= par_min_ ? threads_ : 1u;
     struct Item { uint64_t list; uint32_t vi, vj, ui, uj; };
     std::vector<std::vector<Item>> items((size_t)T * T);  // [slice * T + owner]
     run_threads(T, [&](uint32_t s) {
-        for (size_t i = cut[s]; i < cut[s + 1]; ++i) {
-            const Task& t = del[i];
-            for (uint32_t uj : qnei_[t.u])
-                for (uint32_t vj : C(t.v, t.u, uj))
-                    if (lit(vj, uj))
-                        items[(size_t)s * T + owner(vj, T)].push_back({list_index(vj, uj, t.u), t.v, vj, t.u, uj});
-        }
+        scan_items(del, segs, total * s / T, total * (s + 1) / T,
+                   [&](uint32_t, const Task& t, uint32_t uj, uint32_t vj) {
+                       if (lit(vj, uj))
+                           items[(size_t)s * T + owner(vj, T)].push_back({list_index(vj, uj, t.u), t.v, vj, t.u, uj});
+                   });
     });
     struct Chk { uint32_t u, v; int group; };
     std::vector<std::vector<Task>> next(T);
@@ -565,7 +617,7 @@ void CaLiGIndex::del_and_check(std::vector<Task>& del) {
         if (lists_.size() < (1ull << (64 - ib))) {
             std::vector<uint64_t> key(it.size());
             for (size_t i = 0; i < it.size(); ++i) key[i] = it[i].list << ib | i;
-            std::sort(key.begin(), key.end());
+            radix_sort(key, ib + (64 - __builtin_clzll((unsigned long long)lists_.size() | 1ull)));
             for (size_t i = 0; i < it.size(); ++i) ord[i] = (uint32_t)(key[i] & ((1ull << ib) - 1));
         } else {
             std::iota(ord.begin(), ord.end(), 0u);
@@ -592,7 +644,7 @@ void CaLiGIndex::del_and_check(std::vector<Task>& del) {
         for (size_t i = 0; i < it.size(); ++i) {
             const Item& e = it[i];
             if (ends_empty[i]) {
-                li_[e.vj] &= ~(1u << e.uj);
+                unlight(e.vj, e.uj);
                 next[k].push_back({e.uj, e.vj});
             } else {
                 const int g = rep_of_label_[e.uj][label_slot_[qlabel_[e.ui]]];
@@ -607,7 +659,7 @@ void CaLiGIndex::del_and_check(std::vector<Task>& del) {
             checked_[c.v] |= 1u << c.u;
             std::vector<uint32_t> used;
             if (!try_nei(c.v, c.u, rep_[c.u][c.group], 0, used)) {
-                li_[c.v] &= ~(1u << c.u);
+                unlight(c.v, c.u);
                 next[k].push_back({c.u, c.v});
             }
         }
@@ -641,23 +693,19 @@ void CaLiGIndex::add_and_check(std::vector<Task>& add, std::vector<Task>& settle
     const size_t nfresh = add.size();
     add.insert(add.end(), settled.begin(), settled.end());
     settled.clear();
-    std::vector<size_t> cut;
-    const uint32_t T = slice_tasks(add, threads_, cut) >= par_min_ ? threads_ : 1u;
-    if (T == 1) cut = {0, add.size()};
+    std::vector<Seg> segs;
+    const size_t total = segments(add, segs);
+    const uint32_t T = total >= par_min_ ? threads_ : 1u;
     struct Ins { uint64_t list; uint32_t vi, vj, ui, uj; };
     std::vector<std::vector<Ins>> ins((size_t)T * T);     // [slice * T + owner]
     std::vector<std::vector<Task>> check((size_t)T * T);
     run_threads(T, [&](uint32_t s) {
-        for (size_t i = cut[s]; i < cut[s + 1]; ++i) {
-            const Task& t = add[i];
-            const bool fresh = i < nfresh;
-            for (uint32_t uj : qnei_[t.u])
-                for (uint32_t vj : C(t.v, t.u, uj)) {
-                    const size_t b = (size_t)s * T + owner(vj, T);
-                    if (fresh) ins[b].push_back({list_index(vj, uj, t.u), t.v, vj, t.u, uj});
-                    if (!lit(vj, uj)) check[b].push_back({uj, vj});
-                }
-        }
+        scan_items(add, segs, total * s / T, total * (s + 1) / T,
+                   [&](uint32_t i, const Task& t, uint32_t uj, uint32_t vj) {
+                       const size_t b = (size_t)s * T + owner(vj, T);
+                       if (i < nfresh) ins[b].push_back({list_index(vj, uj, t.u), t.v, vj, t.u, uj});
+                       if (!lit(vj, uj)) check[b].push_back({uj, vj});
+                   });
     });
     std::vector<std::vector<Task>> next(T), act(T), drop(T);
     std::vector<std::vector<DeltaOp>> added(T);
@@ -703,7 +751,7 @@ void CaLiGIndex::add_and_check(std::vector<Task>& add, std::vector<Task>& settle
                 if ((checked_[c.v] >> c.u) & 1u) continue;
                 checked_[c.v] |= 1u << c.u;
                 if (check_nei(c.v, c.u)) {
-                    li_[c.v] |= 1u << c.u;
+                    light(c.v, c.u);
                     next[k].push_back(c);
                     act[k].push_back(c);
                 } else {
@@ -789,7 +837,7 @@ void CaLiGIndex::update_index(uint32_t start, uint32_t count) {
             checked_[c.v] |= 1u << c.u;
             if (lit(c.v, c.u)) continue;
             if (check_nei(c.v, c.u)) {
-                li_[c.v] |= 1u << c.u;
+                light(c.v, c.u);
                 addp[k].push_back(c);
                 actp[k].push_back(c);
             }

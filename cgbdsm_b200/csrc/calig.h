@@ -99,6 +99,12 @@ private:
     std::vector<uint64_t> cbase_;    // per vertex: first list index
     std::vector<std::vector<uint32_t>> lists_;
     std::vector<uint32_t> li_, checked_;
+    // LI transposed: bit v of row u (row = words_ 64-bit words) is bit u of
+    // li_[v].  The scans test one (v, u) per item; a row is n / 8 bytes and
+    // stays in a core's L2 where li_ (4 n bytes) does not.  Rows are shared
+    // by vertices of different owners: updates are atomic.
+    std::vector<uint64_t> litbits_;
+    size_t words_ = 0;
     std::vector<int> update_;
     uint32_t threads_ = 1;
     uint64_t par_min_ = 4096;
@@ -107,7 +113,18 @@ private:
         return cbase_[v] + block_off_[ui] + (uint32_t)npos_[ui * qn_ + uj];
     }
     inline std::vector<uint32_t>& C(uint32_t v, uint32_t ui, uint32_t uj) { return lists_[list_index(v, ui, uj)]; }
-    inline bool lit(uint32_t v, uint32_t u) const { return (li_[v] >> u) & 1u; }
+    inline bool lit(uint32_t v, uint32_t u) const {
+        return (__atomic_load_n(&litbits_[u * words_ + (v >> 6)], __ATOMIC_RELAXED) >> (v & 63)) & 1u;
+    }
+    // set / clear bit u of li_[v] (the owner of v only)
+    inline void light(uint32_t v, uint32_t u) {
+        li_[v] |= 1u << u;
+        __atomic_fetch_or(&litbits_[u * words_ + (v >> 6)], 1ull << (v & 63), __ATOMIC_RELAXED);
+    }
+    inline void unlight(uint32_t v, uint32_t u) {
+        li_[v] &= ~(1u << u);
+        __atomic_fetch_and(&litbits_[u * words_ + (v >> 6)], ~(1ull << (v & 63)), __ATOMIC_RELAXED);
+    }
     bool has_slot(uint32_t v, uint32_t u) const {
         return glabel_[v] >= 0 && glabel_[v] == label_slot_[qlabel_[u]];
     }
@@ -120,7 +137,10 @@ private:
     void add_and_check(std::vector<Task>& add, std::vector<Task>& settled, std::vector<Task>& add_del,
                        std::vector<Task>& activated);
     void del_and_check(std::vector<Task>& del);
-    size_t slice_tasks(const std::vector<Task>& q, uint32_t T, std::vector<size_t>& cut);
+    struct Seg { uint32_t task, uj; size_t first; };
+    size_t segments(const std::vector<Task>& q, std::vector<Seg>& segs);
+    template <class Fn>
+    void scan_items(const std::vector<Task>& q, const std::vector<Seg>& segs, size_t lo, size_t hi, Fn&& fn);
 };
 
 }  // namespace cgb
