@@ -333,19 +333,22 @@ struct ListRef {
     uint32_t dl;
 };
 
-__device__ __forceinline__ bool sorted_has(const uint32_t* __restrict__ p, uint32_t n, uint32_t x) {
-    uint32_t lo = 0, len = n;
-    while (len > 0) {
-        uint32_t half = len >> 1;
-        if (__ldg(p + lo + half) < x) { lo += half + 1; len -= half + 1; }
-        else len = half;
+// Membership in the ascending p[0..n): halves the range with a select
+// instead of a branch, so the trip count is ceil(log2 n) for every x.
+// Invariant: if x is present it lies in [p, p + n).
+__device__ __forceinline__ bool sorted_has_bl(const uint32_t* __restrict__ p, uint32_t n, uint32_t x) {
+    if (n == 0) return false;
+    while (n > 1) {
+        const uint32_t half = n >> 1;
+        p = (__ldg(p + half) <= x) ? p + half : p;
+        n -= half;
     }
-    return lo < n && __ldg(p + lo) == x;
+    return __ldg(p) == x;
 }
 
 __device__ __forceinline__ bool list_contains(const uint32_t* __restrict__ pool, const uint32_t* __restrict__ dval,
                                               const uint4& r, uint32_t x) {
-    return sorted_has(pool + r.x, r.y, x) || (r.w && sorted_has(dval + r.z, r.w, x));
+    return sorted_has_bl(pool + r.x, r.y, x) || (r.w && sorted_has_bl(dval + r.z, r.w, x));
 }
 
 
@@ -694,7 +697,6 @@ __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
     __shared__ uint4 s_bn[kDfsWarps][kMaxBN];
     __shared__ uint32_t s_m[kDfsWarps][kMaxQV];
     __shared__ unsigned long long s_tc[kDfsWarps][kMaxQV * 8];
-    __shared__ uint2 s_rng[kDfsWarps][32];  // narrowed [lo, hi) per (backward list, part) of a chunk
     __shared__ uint32_t s_pre[kMaxQE + 1];
     __shared__ uint32_t s_lo[kMaxQE];
 
@@ -961,49 +963,21 @@ __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
                     if (ok && a.vb)  // the valid bits are a sound superset: a clear bit cannot match
                         ok = (__ldg(a.vb + ((size_t)ei * a.qv + P.vs[j]) * a.vb_stride + (c >> 5)) >> (c & 31)) & 1u;
                 }
-                if (o1 - o0 > 1) {
-                    // Narrow every other backward list to the chunk's value range
-                    // [cmin, cmax] once (one lane per list part, two searches each),
-                    // so each candidate's probe runs over the narrowed window only.
-                    uint32_t cmin = ok ? c : 0xffffffffu, cmax = ok ? c : 0u;
-                    for (int o = 16; o > 0; o >>= 1) {
-                        cmin = min(cmin, __shfl_xor_sync(kFull, cmin, o));
-                        cmax = max(cmax, __shfl_xor_sync(kFull, cmax, o));
-                    }
-                    const uint32_t nparts = 2 * (o1 - o0);
-                    if (lane < nparts && cmin <= cmax) {
-                        const uint32_t k = o0 + (lane >> 1);
-                        const uint4 r = bn[k];
-                        const uint32_t* p = (lane & 1) ? a.dval + r.z : a.pool + r.x;
-                        const uint32_t n = (lane & 1) ? r.w : r.y;
-                        uint32_t lo = 0, len = n;
-                        while (len > 0) {
-                            const uint32_t half = len >> 1;
-                            if (__ldg(p + lo + half) < cmin) { lo += half + 1; len -= half + 1; }
-                            else len = half;
-                        }
-                        uint32_t hi = lo;
-                        len = n - lo;
-                        while (len > 0) {
-                            const uint32_t half = len >> 1;
-                            if (__ldg(p + hi + half) <= cmax) { hi += half + 1; len -= half + 1; }
-                            else len = half;
-                        }
-                        s_rng[w][lane] = make_uint2(lo, hi);
-                        n_bytes += 32u * 2u * (33u - __clz(n | 1u));
-                    }
-                    __syncwarp();
-                }
                 if (ok) {
+                    // Each candidate is searched in every other backward list,
+                    // stopping at the first miss.  All lanes search the same list
+                    // with the same trip count, so the branch-free search keeps
+                    // the warp converged, and the first steps of every lane hit
+                    // the same words.
                     for (uint32_t k = o0; k < o1 && ok; ++k) {
                         if (k == o0 + g) continue;
                         const uint4 r = bn[k];
-                        const uint2 rm = s_rng[w][2 * (k - o0)];
-                        const uint2 rd = s_rng[w][2 * (k - o0) + 1];
-                        n_bytes += 32u * (33u - __clz((rm.y - rm.x) | 1u));
-                        if (rd.y > rd.x) n_bytes += 32u * (33u - __clz((rd.y - rd.x) | 1u));
-                        ok = sorted_has(a.pool + r.x + rm.x, rm.y - rm.x, c) ||
-                             (rd.y > rd.x && sorted_has(a.dval + r.z + rd.x, rd.y - rd.x, c));
+                        n_bytes += 32u * (33u - __clz(r.y | 1u));
+                        ok = sorted_has_bl(a.pool + r.x, r.y, c);
+                        if (!ok && r.w) {
+                            n_bytes += 32u * (33u - __clz(r.w | 1u));
+                            ok = sorted_has_bl(a.dval + r.z, r.w, c);
+                        }
                     }
                     ++n_tested;
                 }
