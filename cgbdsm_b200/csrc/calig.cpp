@@ -93,15 +93,6 @@ inline bool sorted_insert(std::vector<uint32_t>& v, uint32_t x) {
     v.insert(it, x);
     return true;
 }
-// Runs fn(0..n-1), each on its own thread (inline when n == 1).
-template <class Fn>
-void run_threads(uint32_t n, Fn fn) {
-    if (n <= 1) { fn(0u); return; }
-    std::vector<std::thread> pool;
-    pool.reserve(n);
-    for (uint32_t k = 0; k < n; ++k) pool.emplace_back(fn, k);
-    for (auto& t : pool) t.join();
-}
 
 inline bool sorted_erase(std::vector<uint32_t>& v, uint32_t x) {
     auto it = std::lower_bound(v.begin(), v.end(), x);
@@ -878,6 +869,24 @@ void CaLiGIndex::construct_update(uint32_t start, uint32_t count) {
     const uint32_t T = npairs >= par_min_ ? threads_ : 1u;
     std::vector<std::vector<DeltaOp>> upd(T);
     run_threads(T, [&](uint32_t s) {
+        // lookups in groups of 16 whose list headers, then list words, are
+        // prefetched together (each is a dependent cache miss); results are
+        // emitted in the pairs' order
+        constexpr size_t kGroup = 16;
+        struct Look { const std::vector<uint32_t>* L; uint32_t v1, v2, u1, u2; };
+        Look grp[kGroup];
+        size_t ng = 0;
+        auto flush = [&]() {
+            for (size_t i = 0; i < ng; ++i)
+                if (!grp[i].L->empty()) __builtin_prefetch(grp[i].L->data() + grp[i].L->size() / 2);
+            for (size_t i = 0; i < ng; ++i) {
+                const Look& q = grp[i];
+                if (!sorted_has(*q.L, q.v2)) continue;
+                upd[s].push_back({q.v1, q.v2, q.u1, q.u2});
+                upd[s].push_back({q.v2, q.v1, q.u2, q.u1});
+            }
+            ng = 0;
+        };
         for (uint32_t p = (uint32_t)((uint64_t)npairs * s / T); p < (uint32_t)((uint64_t)npairs * (s + 1) / T); ++p) {
             const int a = update_[start + 2 * p], b = update_[start + 2 * p + 1];
             if (a < 0 || b < 0 || (uint32_t)a >= n || (uint32_t)b >= n) continue;
@@ -886,12 +895,14 @@ void CaLiGIndex::construct_update(uint32_t start, uint32_t count) {
             for (uint32_t u1 : qlist_[glabel_[v1]]) {
                 if (!lit(v1, u1)) continue;
                 for (uint32_t u2 : qnei_[u1]) {
-                    if (!sorted_has(C(v1, u1, u2), v2)) continue;
-                    upd[s].push_back({v1, v2, u1, u2});
-                    upd[s].push_back({v2, v1, u2, u1});
+                    const std::vector<uint32_t>* L = &C(v1, u1, u2);
+                    __builtin_prefetch(L);
+                    grp[ng++] = {L, v1, v2, u1, u2};
+                    if (ng == kGroup) flush();
                 }
             }
         }
+        flush();
     });
     concat(delta_update, upd);
     concat(delta_del, upd);

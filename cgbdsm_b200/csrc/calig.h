@@ -13,9 +13,20 @@
 #pragma once
 #include <cstdint>
 #include <string>
+#include <thread>
 #include <vector>
 
 namespace cgb {
+
+// Runs fn(0..n-1), each on its own thread (inline when n == 1).
+template <class Fn>
+void run_threads(uint32_t n, Fn fn) {
+    if (n <= 1) { fn(0u); return; }
+    std::vector<std::thread> pool;
+    pool.reserve(n);
+    for (uint32_t k = 0; k < n; ++k) pool.emplace_back(fn, k);
+    for (auto& t : pool) t.join();
+}
 
 struct DeltaOp {  // calig.h:35
     uint32_t vi, vj, ui, uj;
@@ -58,6 +69,7 @@ public:
     // constructCand + staticFilter (calig.cpp:325-356, 705-717)
     void construct();
 
+    uint32_t threads() const { return threads_; }
     // Host threads for the list-parallel phases (0 = all hardware threads);
     // also reads CGB_PRODUCER_MIN_PARALLEL (smallest phase run on threads).
     void set_threads(uint32_t n);

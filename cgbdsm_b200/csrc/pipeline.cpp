@@ -39,14 +39,49 @@ struct cgb_producer {
     inline uint32_t nid(uint32_t v) const { return v < dense.size() ? dense[v] : UINT32_MAX; }
     inline uint32_t dir(uint32_t ui, uint32_t uj) const { return eidx[ui * qv + uj]; }
 
+    // New compressed ids go to lit, unmapped vertices in ascending id order:
+    // slices of the id range are scanned on threads and numbered in order.
     void update_mapping() {
         const auto& li = idx.li();
         const uint32_t n = (uint32_t)li.size();
-        for (uint32_t v = 0; v < n; ++v)
-            if (li[v] && dense[v] == UINT32_MAX) {
+        const uint32_t T = n >= (1u << 16) ? idx.threads() : 1u;
+        std::vector<std::vector<uint32_t>> fresh(T);
+        cgb::run_threads(T, [&](uint32_t s) {
+            for (uint32_t v = (uint32_t)((uint64_t)n * s / T); v < (uint32_t)((uint64_t)n * (s + 1) / T); ++v)
+                if (li[v] && dense[v] == UINT32_MAX) fresh[s].push_back(v);
+        });
+        for (auto& f : fresh)
+            for (uint32_t v : f) {
                 dense[v] = (uint32_t)new2old.size();
                 new2old.push_back(v);
             }
+    }
+
+    // Keys of the delta ops that `keep` accepts and whose ends are mapped, in
+    // the ops' order (slices on threads, concatenated); per_dir counts them.
+    template <class Keep>
+    void encode(const std::vector<cgb::DeltaOp>& ops, Keep keep, std::vector<uint64_t>& out,
+                std::vector<uint32_t>* per_dir) {
+        const size_t n = ops.size();
+        const uint32_t T = n >= (1u << 14) ? idx.threads() : 1u;
+        std::vector<std::vector<uint64_t>> part(T);
+        std::vector<std::vector<uint32_t>> cnt(T, std::vector<uint32_t>(32, 0));
+        cgb::run_threads(T, [&](uint32_t s) {
+            for (size_t i = n * s / T; i < n * (s + 1) / T; ++i) {
+                const cgb::DeltaOp& d = ops[i];
+                if (!keep(d)) continue;
+                const uint32_t nu = nid(d.vi), nv = nid(d.vj);
+                if (nu == UINT32_MAX || nv == UINT32_MAX) continue;
+                const uint32_t dd = dir(d.ui, d.uj);
+                part[s].push_back(enc(dd, nu, nv));
+                cnt[s][dd]++;
+            }
+        });
+        out.clear();
+        for (auto& q : part) out.insert(out.end(), q.begin(), q.end());
+        if (per_dir)
+            for (auto& c : cnt)
+                for (uint32_t dd = 0; dd < 32; ++dd) (*per_dir)[dd] += c[dd];
     }
 };
 
@@ -154,29 +189,12 @@ cgb_status cgb_producer_next(cgb_producer* p, cgb_batch_keys* out) {
     // LI-filtered insert keys and delete keys, both restricted to mapped ids
     p->update_mapping();
     const auto& li = p->idx.li();
-    p->ins.clear();
-    for (auto& d : p->idx.delta_ins) {
-        if (!((li[d.vi] >> d.ui) & 1u)) continue;
-        const uint32_t nu = p->nid(d.vi), nv = p->nid(d.vj);
-        if (nu == UINT32_MAX || nv == UINT32_MAX) continue;
-        p->ins.push_back(enc(p->dir(d.ui, d.uj), nu, nv));
-    }
-    p->del.clear();
-    for (auto& d : p->idx.delta_del) {
-        const uint32_t nu = p->nid(d.vi), nv = p->nid(d.vj);
-        if (nu == UINT32_MAX || nv == UINT32_MAX) continue;
-        p->del.push_back(enc(p->dir(d.ui, d.uj), nu, nv));
-    }
+    p->encode(p->idx.delta_ins, [&](const cgb::DeltaOp& d) { return ((li[d.vi] >> d.ui) & 1u) != 0; }, p->ins,
+              nullptr);
+    p->encode(p->idx.delta_del, [](const cgb::DeltaOp&) { return true; }, p->del, nullptr);
     // PrepareUpdateIndex (calig_helper_gamma.cu:403-445)
-    p->delta.clear();
     std::vector<uint32_t> per_dir(32, 0);
-    for (auto& d : p->idx.delta_update) {
-        const uint32_t nu = p->nid(d.vi), nv = p->nid(d.vj);
-        if (nu == UINT32_MAX || nv == UINT32_MAX) continue;
-        const uint32_t dd = p->dir(d.ui, d.uj);
-        p->delta.push_back(enc(dd, nu, nv));
-        per_dir[dd]++;
-    }
+    p->encode(p->idx.delta_update, [](const cgb::DeltaOp&) { return true; }, p->delta, &per_dir);
     p->edge_ok.assign(p->qe, 0);
     for (uint32_t e = 0; e < p->qe; ++e)
         p->edge_ok[e] = per_dir[p->qe_dir[2 * e]] && per_dir[p->qe_dir[2 * e + 1]];
