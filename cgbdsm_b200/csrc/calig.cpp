@@ -616,9 +616,20 @@ void CaLiGIndex::del_and_check(std::vector<Task>& del) {
         }
         std::vector<uint8_t> ends_empty(it.size()), hit;
         std::vector<uint32_t> vals;
-        for (size_t g0 = 0; g0 < ord.size();) {
-            size_t g1 = g0 + 1;
-            while (g1 < ord.size() && it[ord[g1]].list == it[ord[g0]].list) ++g1;
+        // group starts, so that the lists a few groups ahead are prefetched
+        // (header 8 groups ahead, then its words 4 ahead)
+        std::vector<uint32_t> gs;
+        for (size_t q = 0; q < ord.size(); ++q)
+            if (q == 0 || it[ord[q]].list != it[ord[q - 1]].list) gs.push_back((uint32_t)q);
+        gs.push_back((uint32_t)ord.size());
+        const size_t ngr = gs.size() - 1;
+        for (size_t g = 0; g < ngr; ++g) {
+            if (g + 8 < ngr) __builtin_prefetch(&lists_[it[ord[gs[g + 8]]].list]);
+            if (g + 4 < ngr) {
+                const auto& Lp = lists_[it[ord[gs[g + 4]]].list];
+                if (!Lp.empty()) __builtin_prefetch(Lp.data() + Lp.size() / 2);
+            }
+            const size_t g0 = gs[g], g1 = gs[g + 1];
             vals.clear();
             for (size_t q = g0; q < g1; ++q) vals.push_back(it[ord[q]].vi);
             hit.assign(vals.size(), 0);
@@ -629,7 +640,6 @@ void CaLiGIndex::del_and_check(std::vector<Task>& del) {
                 if (hit[q - g0]) erased[k].push_back({e.vj, e.vi, e.uj, e.ui});
                 ends_empty[ord[q]] = L.empty();
             }
-            g0 = g1;
         }
         std::vector<Chk> chk;
         for (size_t i = 0; i < it.size(); ++i) {
