@@ -561,6 +561,44 @@ __device__ unsigned long long tail_eval(const EdgePlan& P, const uint32_t* m, ui
     return prod;
 }
 
+// Tail count for the candidate c of the last core position, evaluated by
+// one lane (plans with tail_lane): every cached subset count is prefix-only
+// and c is removed from it when c lies in all of the subset's lists (only
+// for groups sharing the last core vertex's label).  Lanes diverge only in
+// the searches.
+__device__ unsigned long long tail_eval_lane(const EdgePlan& P, const uint4* bn, const unsigned long long* cache,
+                                             const uint32_t* __restrict__ pool, const uint32_t* __restrict__ dval,
+                                             uint32_t c, unsigned long long& bytes) {
+    const uint32_t nc = P.n_core, n = P.n, j = nc - 1;
+    unsigned long long prod = 1;
+    uint32_t t = nc;
+    while (t < n && prod) {
+        uint32_t e = t;
+        while (e < n && P.tail_gid[e] == P.tail_gid[t]) ++e;
+        const uint32_t k = e - t;
+        const bool same_label = (P.excl[t] >> j) & 1u;
+        unsigned long long sc[8];
+        for (uint32_t mask = 1; mask < (1u << k); ++mask) {
+            unsigned long long cv = cache[t * 8 + mask];
+            if (same_label) {
+                bool in = true;
+                for (uint32_t i = 0; i < k && in; ++i)
+                    if (mask & (1u << i))
+                        for (uint32_t q = P.bn_off[t + i]; q < P.bn_off[t + i + 1] && in; ++q) {
+                            const uint4 r = bn[q];
+                            bytes += 32u * (33u - __clz(r.y | 1u));
+                            in = list_contains(pool, dval, r, c);
+                        }
+                cv -= in ? 1ull : 0ull;
+            }
+            sc[mask] = cv;
+        }
+        prod *= group_count(sc, k);
+        t = e;
+    }
+    return prod;
+}
+
 // Tail count of a plan with tail_const: every subset is prefix-only and no
 // candidate of the last core position can lie in a tail list, so the count
 // is the product of the cached group counts.
@@ -1002,6 +1040,20 @@ __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
                                 if (hit_last) wsum -= X.mult_sum(c, ok, lane);
                             }
                             if (lane == 0) { cnt += wsum * tail_const; n_tail += __popc(bal); }
+                        }
+                    } else if (has_tail && P.tail_lane && a.tail_cache && !hit_last) {
+                        // the tail depends on the candidate only through prefix-only
+                        // lists: every lane counts its own candidate's tail
+                        const uint32_t bal = __ballot_sync(kFull, ok);
+                        if (bal) {
+                            if (dirty <= P.tail_dep)
+                                tail_prepare(P, m, bn, s_tc[w], dirty, a.rec, a.dvcap, a.pool, a.dval, self_loops, lane, n_bytes);
+                            dirty = kClean;
+                            if (ok) {
+                                const unsigned long long tc = tail_eval_lane(P, bn, s_tc[w], a.pool, a.dval, c, n_bytes);
+                                cnt += P.grouped ? tc * (unsigned long long)(X.n - hs) : tc;
+                            }
+                            if (lane == 0) n_tail += __popc(bal);
                         }
                     } else if (has_tail) {
                         // every surviving candidate completes a core embedding: count its tail

@@ -296,6 +296,11 @@ void plan_edges(const QueryMeta& q, const float* avg_deg, EdgePlan* plans, bool 
             for (uint32_t c = 0; c + 1 < n_core; ++c)
                 if ((p.excl[t] >> c) & 1u) p.tail_dep = std::max<uint8_t>(p.tail_dep, (uint8_t)c);
         }
+        if (n_core >= 2 && n_core < q.qv && !p.tail_const) {
+            bool off_last = false;
+            for (uint32_t b2 = p.bn_off[n_core]; b2 < p.bn_off[q.qv]; ++b2) off_last |= p.bn_pos[b2] + 1u == n_core;
+            p.tail_lane = off_last ? 0 : 1;
+        }
         if (pendant) {
             p.grouped = 1;
             for (uint32_t j = 2; j < n_core; ++j)

@@ -64,6 +64,10 @@ struct EdgePlan {
     // unknown); only those are excluded from t's counts.
     uint16_t excl[kMaxQV];
     uint16_t hit_mask;
+    // tail_lane: no tail list hangs off the last core vertex, so a candidate
+    // there changes the tail count only by lying in prefix-only lists (same
+    // label); each lane then evaluates its own candidate's tail count.
+    uint8_t tail_lane;
     // tail_dep: the deepest core position below n_core - 1 that a tail count
     // reads (a list's owner or an excluded vertex); a prefix change at a
     // deeper position leaves every prefix-only tail count as it was.
