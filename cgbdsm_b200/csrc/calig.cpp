@@ -782,7 +782,7 @@ void CaLiGIndex::update_index(uint32_t start, uint32_t count) {
     // turnOnCond (calig.cpp:640-655) on slices of the batch, against the
     // adjacency before the batch (a pair listed twice is new both times)
     std::vector<std::vector<std::pair<uint32_t, uint32_t>>> ups(T);
-    std::vector<std::vector<Tmp>> tmp(T);
+    std::vector<std::vector<Tmp>> tmp((size_t)T * T);  // [slice * T + owner of the first vertex]
     run_threads(T, [&](uint32_t s) {
         for (uint32_t p = (uint32_t)((uint64_t)npairs * s / T); p < (uint32_t)((uint64_t)npairs * (s + 1) / T); ++p) {
             const int a = update_[start + 2 * p], b = update_[start + 2 * p + 1];
@@ -795,7 +795,8 @@ void CaLiGIndex::update_index(uint32_t start, uint32_t count) {
                 const uint32_t x = o ? v2 : v1, y = o ? v1 : v2;
                 for (uint32_t ui : qlist_[glabel_[x]])
                     for (uint32_t uj : qnei_[ui])
-                        if (label_slot_[qlabel_[uj]] == glabel_[y]) tmp[s].push_back({ui, uj, x, y});
+                        if (label_slot_[qlabel_[uj]] == glabel_[y])
+                            tmp[(size_t)s * T + owner(x, T)].push_back({ui, uj, x, y});
             }
         }
     });
@@ -822,9 +823,8 @@ void CaLiGIndex::update_index(uint32_t start, uint32_t count) {
             }
         };
         std::vector<Task> check;
-        for (auto& part : tmp)
-            for (auto& t : part) {
-                if (owner(t.vi, T) != k) continue;
+        for (uint32_t sl = 0; sl < T; ++sl)
+            for (auto& t : tmp[(size_t)sl * T + k]) {
                 ins.emplace_back(list_index(t.vi, t.ui, t.uj), t.vj);
                 if (lit(t.vi, t.ui)) setp[k].push_back({t.ui, t.vi});
                 else {
