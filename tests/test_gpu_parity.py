@@ -100,10 +100,21 @@ def test_random_labelled_streams(seed):
     _random_stream(200 + seed, 0.1 if seed % 3 == 2 else 0.0, nlabels=1 + seed % 3)
 
 
-def _random_stream(seed, self_loop_rate, nlabels=0):
+@pytest.mark.parametrize("seed", range(6))
+def test_pendant_with_same_label_tail(seed):
+    """A hub with a pendant and a second degree-1 neighbour of the pendant's
+    label: the grouped plan keeps that neighbour as a counted tail and
+    subtracts, per embedding, the seeds that are its candidates."""
+    query = (5, [(0, 1), (0, 2), (0, 3), (0, 4), (3, 4)], [0, 1, 1, 2, 3])
+    _random_stream(400 + seed, 0.1 if seed % 2 else 0.0, nlabels=4, query=query)
+
+
+def _random_stream(seed, self_loop_rate, nlabels=0, query=None):
     rng = np.random.default_rng(1000 + seed)
     qv = int(rng.integers(3, 7))
     qedges = _random_query(rng, qv, int(rng.integers(0, 4)))
+    if query is not None:
+        qv, qedges = query[0], query[1]
     dv0 = 60
     flags = FLAG_FORCE_SPLIT if seed % 2 else 0
     if nlabels and seed % 4 >= 2:
@@ -114,6 +125,8 @@ def _random_stream(seed, self_loop_rate, nlabels=0):
         # labels: query vertices and data vertices drawn from nlabels values;
         # a key (a -> b, x, y) only pairs x of a's label with y of b's label
         qlab = [int(x) for x in rng.integers(0, nlabels, qv)]
+        if query is not None:
+            qlab = list(query[2])
         eng.load_query(qv, qedges, qlab)
         dlab = rng.integers(0, nlabels, 4096)
         dlab[:2 * nlabels] = np.arange(2 * nlabels) % nlabels  # hubs 0 .. 2*nlabels-1 cover every label
