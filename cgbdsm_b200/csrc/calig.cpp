@@ -1,6 +1,10 @@
 #include "calig.h"
 
 #include <algorithm>
+#include <unistd.h>
+#include <atomic>
+#include <condition_variable>
+#include <mutex>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -13,6 +17,89 @@
 namespace cgb {
 
 namespace {
+
+// Workers wait on a generation counter: a job bumps it; each worker runs
+// the tasks it claims from a shared counter, the caller too, and the caller
+// returns when every task has finished.  Workers spin briefly before
+// sleeping, so back-to-back phases do not pay a wake-up.
+class WorkerPool {
+public:
+    explicit WorkerPool(uint32_t n) {
+        for (uint32_t i = 0; i < n; ++i) workers_.emplace_back([this] { loop(); });
+    }
+    ~WorkerPool() {
+        {
+            std::lock_guard<std::mutex> g(m_);
+            stop_ = true;
+            ++gen_;
+        }
+        cv_.notify_all();
+        for (auto& t : workers_) t.join();
+    }
+    uint32_t size() const { return (uint32_t)workers_.size(); }
+    void run(uint32_t n, const std::function<void(uint32_t)>& fn) {
+        std::lock_guard<std::mutex> job(job_m_);
+        fn_ = &fn;
+        ntasks_ = n;
+        next_.store(0, std::memory_order_relaxed);
+        done_.store(0, std::memory_order_relaxed);
+        {
+            std::lock_guard<std::mutex> g(m_);
+            gen_.fetch_add(1, std::memory_order_release);
+        }
+        cv_.notify_all();
+        work();
+        while (done_.load(std::memory_order_acquire) < n) std::this_thread::yield();
+        fn_ = nullptr;
+    }
+    static thread_local bool in_job;
+
+private:
+    std::vector<std::thread> workers_;
+    std::mutex m_, job_m_;
+    std::condition_variable cv_;
+    std::atomic<uint64_t> gen_{0};
+    std::atomic<uint32_t> next_{0}, done_{0};
+    const std::function<void(uint32_t)>* fn_ = nullptr;
+    uint32_t ntasks_ = 0;
+    bool stop_ = false;
+
+    void work() {
+        in_job = true;
+        for (;;) {
+            const uint32_t k = next_.fetch_add(1, std::memory_order_relaxed);
+            if (k >= ntasks_) break;
+            (*fn_)(k);
+            done_.fetch_add(1, std::memory_order_release);
+        }
+        in_job = false;
+    }
+    void loop() {
+        uint64_t seen = 0;
+        for (;;) {
+            uint64_t g = gen_.load(std::memory_order_acquire);
+            for (int spin = 0; g == seen && spin < 20000; ++spin) {
+                std::this_thread::yield();
+                g = gen_.load(std::memory_order_acquire);
+            }
+            if (g == seen) {
+                std::unique_lock<std::mutex> lk(m_);
+                cv_.wait(lk, [&] { return gen_.load(std::memory_order_acquire) != seen; });
+                g = gen_.load(std::memory_order_acquire);
+            }
+            seen = g;
+            if (stop_) return;
+            work();
+        }
+    }
+};
+thread_local bool WorkerPool::in_job = false;
+
+WorkerPool& worker_pool() {
+    static WorkerPool pool(std::max(1u, std::thread::hardware_concurrency()) - 1);
+    return pool;
+}
+const pid_t g_pool_pid = getpid();  // a forked child has no workers: it runs jobs inline
 
 // Whole-file reader + integer tokenizer (the reference streams with >>).
 bool slurp(const std::string& path, std::vector<char>& buf) {
@@ -177,6 +264,14 @@ void dedupe(std::vector<T>& q) {
 }
 
 }  // namespace
+
+void pool_run(uint32_t n, const std::function<void(uint32_t)>& fn) {
+    if (n <= 1 || WorkerPool::in_job || getpid() != g_pool_pid) {
+        for (uint32_t k = 0; k < n; ++k) fn(k);
+        return;
+    }
+    worker_pool().run(n, fn);
+}
 
 // calig.cpp:111-164: 'v id label' lines (label -1 -> 0), then 'e a b label'.
 std::string CaLiGIndex::load_query(const std::string& path) {
