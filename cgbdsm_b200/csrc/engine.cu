@@ -28,6 +28,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdarg>
+#include <cstdlib>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -287,6 +288,61 @@ __global__ void k_seed_ranges(const uint64_t* __restrict__ dkeys, uint64_t n, ui
 }
 
 // ---------------------------------------------------------------------------
+// run bit sets: every old run of at least kRunBitsMinLen entries is also kept
+// as a bit set over the compressed ids, rebuilt each batch after the index
+// update, so that a membership test in a long (hub) run, in the DFS probes
+// and in the tail counts, is one load instead of a binary search
+// ---------------------------------------------------------------------------
+constexpr uint32_t kNoSlot = 0xffffffffu;
+constexpr uint32_t kRunBitsMinLen = 128;        // $CGB_RUN_BITS_MIN_LEN overrides (tests use 1)
+constexpr size_t kRunBitsBytes = 512ull << 20;  // runs beyond this budget are searched
+
+// Slot of every (direction, vertex) whose old run is long enough, in claim
+// order while slots last (ctr counts claims), else kNoSlot; sel[slot] =
+// dir << 27 | vertex.
+__global__ void k_rb_select(const uint4* __restrict__ rec, uint32_t dvcap, uint32_t dv, uint32_t nd, uint32_t min_len,
+                            uint32_t cap, uint32_t* slot, uint32_t* sel, unsigned int* ctr) {
+    const size_t n = (size_t)nd * dv;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const uint32_t d = (uint32_t)(i / dv), u = (uint32_t)(i % dv);
+        uint32_t sl = kNoSlot;
+        if (rec[(size_t)d * dvcap + u].y >= min_len) {
+            const unsigned int c = atomicAdd(ctr, 1u);
+            if (c < cap) {
+                sl = c;
+                sel[c] = d << 27 | u;
+            }
+        }
+        slot[(size_t)d * dvcap + u] = sl;
+    }
+}
+
+__global__ void k_rb_zero(uint32_t* bits, uint32_t words, uint32_t cap, const unsigned int* ctr) {
+    const size_t n = (size_t)min(*ctr, cap) * words;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        bits[i] = 0;
+}
+
+// one warp per selected run: the bits of its words, set with atomicOr
+// (lanes can share a word)
+__global__ void k_rb_fill(const uint4* __restrict__ rec, uint32_t dvcap, const uint32_t* __restrict__ pool,
+                          const uint32_t* __restrict__ sel, uint32_t cap, const unsigned int* ctr, uint32_t* bits,
+                          uint32_t words) {
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t nsel = min(*ctr, cap);
+    const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; c < nsel; c += nw) {
+        const uint32_t du = sel[c];
+        const uint4 r = rec[(size_t)(du >> 27) * dvcap + (du & ((1u << 27) - 1u))];
+        uint32_t* b = bits + (size_t)c * words;
+        for (uint32_t t = lane; t < r.y; t += 32) {
+            const uint32_t v = __ldg(pool + r.x + t);
+            atomicOr(b + (v >> 5), 1u << (v & 31));
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
 // persistent warp DFS (count only)
 // ---------------------------------------------------------------------------
 struct DfsArgs {
@@ -316,6 +372,9 @@ struct DfsArgs {
     const uint32_t* vb;          // valid bits [qe][qv][vb_stride] or nullptr (no pruning)
     uint32_t vb_stride;
     uint32_t qv;
+    const uint32_t* rb_slot;     // run bit sets: slot of (dir, vertex) [nd][dvcap] or nullptr (none)
+    const uint32_t* rb_bits;     // [slot][rb_words]
+    uint32_t rb_words;
 };
 
 __device__ __forceinline__ unsigned long long global_ns() {
@@ -351,6 +410,31 @@ __device__ __forceinline__ bool list_contains(const uint32_t* __restrict__ pool,
     return sorted_has_bl(pool + r.x, r.y, x) || (r.w && sorted_has_bl(dval + r.z, r.w, x));
 }
 
+// Bit sets of the long old runs (rebuilt each batch): slot[(dir, vertex)]
+// names a bit set over the compressed ids, or kNoSlot; a warp keeps the slot
+// of every resolved record bn[k] in bslot[k].  slot == nullptr: none.
+struct RunBits {
+    const uint32_t* slot;
+    const uint32_t* bits;
+    uint32_t words;
+    uint32_t* bslot;
+    __device__ __forceinline__ void note(uint32_t k, size_t at) const {
+        if (slot) bslot[k] = __ldg(slot + at);
+    }
+    // x in the resolved list bn[k] = r: one bit test for a long old run
+    __device__ __forceinline__ bool has(uint32_t k, const uint4& r, const uint32_t* __restrict__ pool,
+                                       const uint32_t* __restrict__ dval, uint32_t x) const {
+        if (slot) {
+            const uint32_t sl = bslot[k];
+            if (sl != kNoSlot) {
+                if ((__ldg(bits + (size_t)sl * words + (x >> 5)) >> (x & 31)) & 1u) return true;
+                return r.w && sorted_has_bl(dval + r.z, r.w, x);
+            }
+        }
+        return list_contains(pool, dval, r, x);
+    }
+};
+
 
 // Number of x in the intersection of the resolved lists bn[ids[0..nl)] with x
 // not among the matched core vertices m[t], t in the bit set excl (positions
@@ -361,7 +445,7 @@ __device__ __forceinline__ bool list_contains(const uint32_t* __restrict__ pool,
 __device__ unsigned long long isect_count(const uint4* bn, const uint8_t* ids, uint32_t nl, const uint32_t* m,
                                           uint32_t excl, const uint32_t* __restrict__ pool,
                                           const uint32_t* __restrict__ dval, uint32_t lane,
-                                          unsigned long long& bytes) {
+                                          unsigned long long& bytes, const RunBits& rb) {
     if (nl == 1) {
         const uint4 r = bn[ids[0]];
         bool in = false;
@@ -369,7 +453,7 @@ __device__ unsigned long long isect_count(const uint4* bn, const uint8_t* ids, u
             // a vertex held by two positions (a self-loop seed edge) is excluded once
             bool dup = false;
             for (uint32_t e = excl & ((1u << lane) - 1u); e; e &= e - 1) dup |= m[__ffs(e) - 1] == m[lane];
-            if (!dup) in = list_contains(pool, dval, r, m[lane]);
+            if (!dup) in = rb.has(ids[0], r, pool, dval, m[lane]);
             bytes += 32u * (33u - __clz(r.y | 1u));
         }
         return (unsigned long long)(r.y + r.w) - __popc(__ballot_sync(kFull, in));
@@ -392,7 +476,7 @@ __device__ unsigned long long isect_count(const uint4* bn, const uint8_t* ids, u
                 if (i == g) continue;
                 const uint4 r = bn[ids[i]];
                 bytes += 32u * (33u - __clz(r.y | 1u));
-                ok = list_contains(pool, dval, r, x);
+                ok = rb.has(ids[i], r, pool, dval, x);
             }
         }
         c += __popc(__ballot_sync(kFull, ok));
@@ -424,13 +508,15 @@ __device__ __forceinline__ unsigned long long group_count(const unsigned long lo
 __device__ unsigned long long tail_count_warp(const EdgePlan& P, const uint32_t* m, uint4* bn, const uint4* rec,
                                               uint32_t dvcap, const uint32_t* __restrict__ pool,
                                               const uint32_t* __restrict__ dval, bool self_loops, uint32_t lane,
-                                              unsigned long long& bytes) {
+                                              unsigned long long& bytes, const RunBits& rb) {
     const uint32_t nc = P.n_core, n = P.n;
     // resolve every tail BN record once
     for (uint32_t k = P.bn_off[nc] + lane; k < P.bn_off[n]; k += 32) {
-        uint4 r = rec[(size_t)P.bn_dir[k] * dvcap + m[P.bn_pos[k]]];
+        const size_t at = (size_t)P.bn_dir[k] * dvcap + m[P.bn_pos[k]];
+        uint4 r = rec[at];
         if (!P.bn_dvis[k]) r.w = 0;
         bn[k] = r;
+        rb.note(k, at);
         bytes += 16;
     }
     __syncwarp();
@@ -448,7 +534,7 @@ __device__ unsigned long long tail_count_warp(const EdgePlan& P, const uint32_t*
                 if (mask & (1u << i))
                     for (uint32_t q = P.bn_off[t + i]; q < P.bn_off[t + i + 1]; ++q) ids[nl++] = (uint8_t)q;
             const uint32_t ex = P.excl[t] & ~(self_loops ? 0u : owner_mask(P, ids, nl));
-            sc[mask] = isect_count(bn, ids, nl, m, ex, pool, dval, lane, bytes);
+            sc[mask] = isect_count(bn, ids, nl, m, ex, pool, dval, lane, bytes, rb);
         }
         prod *= group_count(sc, k);
         t = e;
@@ -474,13 +560,15 @@ constexpr uint32_t kClean = 0xffu;  // tail cache up to date
 __device__ void tail_prepare(const EdgePlan& P, const uint32_t* m, uint4* bn, unsigned long long* cache,
                              uint32_t dirty, const uint4* rec, uint32_t dvcap, const uint32_t* __restrict__ pool,
                              const uint32_t* __restrict__ dval, bool self_loops, uint32_t lane,
-                             unsigned long long& bytes) {
+                             unsigned long long& bytes, const RunBits& rb) {
     const uint32_t nc = P.n_core, n = P.n, j = nc - 1;
     for (uint32_t k = P.bn_off[nc] + lane; k < P.bn_off[n]; k += 32) {
         if (P.bn_pos[k] >= j || P.bn_pos[k] < dirty) continue;  // records of unchanged owners are current
-        uint4 r = rec[(size_t)P.bn_dir[k] * dvcap + m[P.bn_pos[k]]];
+        const size_t at = (size_t)P.bn_dir[k] * dvcap + m[P.bn_pos[k]];
+        uint4 r = rec[at];
         if (!P.bn_dvis[k]) r.w = 0;
         bn[k] = r;
+        rb.note(k, at);
         bytes += 16;
     }
     __syncwarp();
@@ -503,7 +591,7 @@ __device__ void tail_prepare(const EdgePlan& P, const uint32_t* m, uint4* bn, un
             const uint32_t ex = P.excl[t] & ((1u << j) - 1u) & ~(self_loops ? 0u : owner_mask(P, ids, nl));
             if (ex) dep = max(dep, 31u - __clz(ex));
             if (!dynamic && dep < dirty) continue;  // still valid
-            const unsigned long long v = dynamic ? kDynamic : isect_count(bn, ids, nl, m, ex, pool, dval, lane, bytes);
+            const unsigned long long v = dynamic ? kDynamic : isect_count(bn, ids, nl, m, ex, pool, dval, lane, bytes, rb);
             if (lane == 0) cache[t * 8 + mask] = v;
         }
         t = e;
@@ -515,14 +603,17 @@ __device__ void tail_prepare(const EdgePlan& P, const uint32_t* m, uint4* bn, un
 __device__ unsigned long long tail_eval(const EdgePlan& P, const uint32_t* m, uint4* bn,
                                         const unsigned long long* cache, const uint4* rec, uint32_t dvcap,
                                         const uint32_t* __restrict__ pool, const uint32_t* __restrict__ dval,
-                                        bool self_loops, uint32_t lane, unsigned long long& bytes) {
+                                        bool self_loops, uint32_t lane, unsigned long long& bytes,
+                                        const RunBits& rb) {
     const uint32_t nc = P.n_core, n = P.n, j = nc - 1;
     const uint32_t c = m[j];
     for (uint32_t k = P.bn_off[nc] + lane; k < P.bn_off[n]; k += 32) {
         if (P.bn_pos[k] != j) continue;
-        uint4 r = rec[(size_t)P.bn_dir[k] * dvcap + c];
+        const size_t at = (size_t)P.bn_dir[k] * dvcap + c;
+        uint4 r = rec[at];
         if (!P.bn_dvis[k]) r.w = 0;
         bn[k] = r;
+        rb.note(k, at);
         bytes += 16;
     }
     __syncwarp();
@@ -546,13 +637,13 @@ __device__ unsigned long long tail_eval(const EdgePlan& P, const uint32_t* m, ui
                 bool in = true;
                 if (lane < nl) {
                     const uint4 r = bn[ids[lane]];
-                    in = list_contains(pool, dval, r, c);
+                    in = rb.has(ids[lane], r, pool, dval, c);
                     bytes += 32u * (33u - __clz(r.y | 1u));
                 }
                 sc[mask] = cv - (__all_sync(kFull, in) ? 1ull : 0ull);
             } else {
                 const uint32_t ex = P.excl[t] & ~(self_loops ? 0u : owner_mask(P, ids, nl));
-                sc[mask] = isect_count(bn, ids, nl, m, ex, pool, dval, lane, bytes);
+                sc[mask] = isect_count(bn, ids, nl, m, ex, pool, dval, lane, bytes, rb);
             }
         }
         prod *= group_count(sc, k);
@@ -568,7 +659,7 @@ __device__ unsigned long long tail_eval(const EdgePlan& P, const uint32_t* m, ui
 // the searches.
 __device__ unsigned long long tail_eval_lane(const EdgePlan& P, const uint4* bn, const unsigned long long* cache,
                                              const uint32_t* __restrict__ pool, const uint32_t* __restrict__ dval,
-                                             uint32_t c, unsigned long long& bytes) {
+                                             uint32_t c, unsigned long long& bytes, const RunBits& rb) {
     const uint32_t nc = P.n_core, n = P.n, j = nc - 1;
     unsigned long long prod = 1;
     uint32_t t = nc;
@@ -587,7 +678,7 @@ __device__ unsigned long long tail_eval_lane(const EdgePlan& P, const uint4* bn,
                         for (uint32_t q = P.bn_off[t + i]; q < P.bn_off[t + i + 1] && in; ++q) {
                             const uint4 r = bn[q];
                             bytes += 32u * (33u - __clz(r.y | 1u));
-                            in = list_contains(pool, dval, r, c);
+                            in = rb.has(q, r, pool, dval, c);
                         }
                 cv -= in ? 1ull : 0ull;
             }
@@ -733,6 +824,7 @@ constexpr uint32_t kCandMask = (1u << kCandBits) - 1u;
 __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
     __shared__ uint32_t s_cand[kDfsWarps][kMaxQV][32];
     __shared__ uint4 s_bn[kDfsWarps][kMaxBN];
+    __shared__ uint32_t s_rbs[kDfsWarps][kMaxBN];  // run bit-set slot of each resolved record
     __shared__ uint32_t s_m[kDfsWarps][kMaxQV];
     __shared__ unsigned long long s_tc[kDfsWarps][kMaxQV * 8];
     __shared__ uint32_t s_pre[kMaxQE + 1];
@@ -750,6 +842,7 @@ __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
     const uint64_t vmask = (1ull << a.B) - 1ull;
     uint32_t* m = s_m[w];
     uint4* bn = s_bn[w];
+    const RunBits rb{a.rb_slot, a.rb_bits, a.rb_words, s_rbs[w]};
     volatile unsigned int* vq = a.qctr;  // [0] tasks reserved, [1] tickets issued, [3] completed, [6] seeds
 
     // per-depth state held by lane == depth
@@ -861,7 +954,7 @@ __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
         }
         if (kind == 1 && nc == 2) {  // the seed edge alone is the core: only the tail remains
             const unsigned long long tc =
-                (P.n == 2) ? 1ull : tail_count_warp(P, m, bn, a.rec, a.dvcap, a.pool, a.dval, self_loops, lane, n_bytes);
+                (P.n == 2) ? 1ull : tail_count_warp(P, m, bn, a.rec, a.dvcap, a.pool, a.dval, self_loops, lane, n_bytes, rb);
             if (lane == 0) { cnt += P.grouped ? tc * X.n : tc; ++n_tail; }
             __syncwarp();
             if (lane == 0) add_release((unsigned int*)&a.qctr[3], 1u);
@@ -875,9 +968,11 @@ __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
             uint32_t len = 0xffffffffu;
             if (lane < nb) {
                 const uint32_t k = o0 + lane;
-                uint4 r = a.rec[(size_t)P.bn_dir[k] * a.dvcap + m[P.bn_pos[k]]];
+                const size_t at = (size_t)P.bn_dir[k] * a.dvcap + m[P.bn_pos[k]];
+                uint4 r = a.rec[at];
                 if (!P.bn_dvis[k]) r.w = 0;
                 bn[k] = r;
+                rb.note(k, at);
                 len = r.y + r.w;
                 n_bytes += 16;
             }
@@ -1010,8 +1105,14 @@ __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
                     for (uint32_t k = o0; k < o1 && ok; ++k) {
                         if (k == o0 + g) continue;
                         const uint4 r = bn[k];
-                        n_bytes += 32u * (33u - __clz(r.y | 1u));
-                        ok = sorted_has_bl(a.pool + r.x, r.y, c);
+                        const uint32_t sl = rb.slot ? s_rbs[w][k] : kNoSlot;
+                        if (sl != kNoSlot) {
+                            n_bytes += 4;
+                            ok = (__ldg(rb.bits + (size_t)sl * rb.words + (c >> 5)) >> (c & 31)) & 1u;
+                        } else {
+                            n_bytes += 32u * (33u - __clz(r.y | 1u));
+                            ok = sorted_has_bl(a.pool + r.x, r.y, c);
+                        }
                         if (!ok && r.w) {
                             n_bytes += 32u * (33u - __clz(r.w | 1u));
                             ok = sorted_has_bl(a.dval + r.z, r.w, c);
@@ -1030,7 +1131,7 @@ __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
                         const uint32_t bal = __ballot_sync(kFull, ok);
                         if (bal) {
                             if (dirty <= P.tail_dep) {
-                                tail_prepare(P, m, bn, s_tc[w], dirty, a.rec, a.dvcap, a.pool, a.dval, self_loops, lane, n_bytes);
+                                tail_prepare(P, m, bn, s_tc[w], dirty, a.rec, a.dvcap, a.pool, a.dval, self_loops, lane, n_bytes, rb);
                                 tail_const = tail_const_value(P, s_tc[w]);
                             }
                             dirty = kClean;
@@ -1047,10 +1148,10 @@ __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
                         const uint32_t bal = __ballot_sync(kFull, ok);
                         if (bal) {
                             if (dirty <= P.tail_dep)
-                                tail_prepare(P, m, bn, s_tc[w], dirty, a.rec, a.dvcap, a.pool, a.dval, self_loops, lane, n_bytes);
+                                tail_prepare(P, m, bn, s_tc[w], dirty, a.rec, a.dvcap, a.pool, a.dval, self_loops, lane, n_bytes, rb);
                             dirty = kClean;
                             if (ok) {
-                                const unsigned long long tc = tail_eval_lane(P, bn, s_tc[w], a.pool, a.dval, c, n_bytes);
+                                const unsigned long long tc = tail_eval_lane(P, bn, s_tc[w], a.pool, a.dval, c, n_bytes, rb);
                                 cnt += P.grouped ? tc * (unsigned long long)(X.n - hs) : tc;
                             }
                             if (lane == 0) n_tail += __popc(bal);
@@ -1064,7 +1165,7 @@ __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
                             const uint32_t cl = __shfl_sync(kFull, c, l);
                             if (dirty <= P.tail_dep && a.tail_cache) {
                                 // first embedding since the prefix changed: recount the stale prefix-only subsets
-                                tail_prepare(P, m, bn, s_tc[w], dirty, a.rec, a.dvcap, a.pool, a.dval, self_loops, lane, n_bytes);
+                                tail_prepare(P, m, bn, s_tc[w], dirty, a.rec, a.dvcap, a.pool, a.dval, self_loops, lane, n_bytes, rb);
                             }
                             dirty = kClean;
                             if (lane == 0) m[j] = cl;
@@ -1072,9 +1173,9 @@ __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
                             const unsigned long long tc =
                                 a.tail_cache
                                     ? tail_eval(P, m, bn, s_tc[w], a.rec, a.dvcap, a.pool, a.dval, self_loops, lane,
-                                                n_bytes)
+                                                n_bytes, rb)
                                     : tail_count_warp(P, m, bn, a.rec, a.dvcap, a.pool, a.dval, self_loops, lane,
-                                                      n_bytes);
+                                                      n_bytes, rb);
                             unsigned long long wt = 1;
                             if (P.grouped) wt = X.n - hs - (hit_last ? X.mult(cl, lane) : 0u);
                             if (lane == 0) { cnt += tc * wt; ++n_tail; }
@@ -1312,6 +1413,14 @@ struct cgb_handle {
     unsigned int* d_qctr = nullptr;          // queue counters [8]
     unsigned long long last_stats[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     void* d_temp = nullptr; size_t temp_cap = 0;
+
+    // run bit sets (per batch)
+    uint32_t* d_rb_slot = nullptr; size_t rb_slot_cap = 0;  // [nd][dvcap]
+    uint32_t* d_rb_sel = nullptr; size_t rb_sel_cap = 0;
+    uint32_t* d_rb_bits = nullptr; size_t rb_bits_cap = 0;
+    unsigned int* d_rb_ctr = nullptr;
+    uint32_t rb_words = 0;
+    uint32_t rb_min_len = kRunBitsMinLen;
 
     // valid bits
     uint32_t vb_start[2] = {0, 0};   // starting edge (SelectStartingEdge)
@@ -1605,6 +1714,7 @@ cgb_status cgb_create(const cgb_config* cfg, cgb_handle** out) {
     cgb_handle* h = new cgb_handle();
     if (cfg) h->cfg = *cfg; else cgb_default_config(&h->cfg);
     h->device = h->cfg.device;
+    if (const char* e = std::getenv("CGB_RUN_BITS_MIN_LEN")) h->rb_min_len = (uint32_t)std::max(1l, std::atol(e));
     int ndev = 0;
     cudaError_t e = cudaGetDeviceCount(&ndev);
     if (e != cudaSuccess || ndev == 0) {
@@ -1646,7 +1756,7 @@ void cgb_destroy(cgb_handle* h) {
                     h->d_edits_alt, h->d_du, h->d_run_du, h->d_run_len, h->d_run_off, h->d_num_runs,
                     h->d_dkeys, h->d_dkeys_alt, h->d_dval, h->d_ddu, h->d_drun_du, h->d_drun_len, h->d_drun_off,
                     h->d_seed, h->d_counts, h->d_stats, h->d_tasks, h->d_qctr, h->d_temp, h->d_qe_dirs, h->d_edge_ok,
-                    h->d_vb};
+                    h->d_vb, h->d_rb_slot, h->d_rb_sel, h->d_rb_bits, h->d_rb_ctr};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (h->h_scal) cudaFreeHost(h->h_scal);
@@ -1828,6 +1938,29 @@ cgb_status cgb_apply_batch_device(cgb_handle* h, uint32_t dv_count, const uint64
         }
         CK(cudaEventRecord(h->ev[2], h->stream));
 
+        // 2c. bit sets of the long old runs (this batch's index)
+        const bool rb_on = !(h->cfg.flags & CGB_FLAG_NO_RUN_BITS);
+        if (rb_on) {
+            h->rb_words = (h->dv + 31) / 32;
+            // as many bit sets as the budget holds, never more than runs exist
+            const uint32_t cap = (uint32_t)std::min<size_t>(kRunBitsBytes / 4 / std::max(h->rb_words, 1u),
+                                                            std::max<size_t>((size_t)h->nd * h->dv, 1));
+            if ((s = grow(h, h->d_rb_slot, h->rb_slot_cap, (size_t)h->nd * h->dvcap)) != CGB_OK) return s;
+            if ((s = grow(h, h->d_rb_sel, h->rb_sel_cap, (size_t)cap)) != CGB_OK) return s;
+            if ((s = grow(h, h->d_rb_bits, h->rb_bits_cap, (size_t)cap * h->rb_words)) != CGB_OK) return s;
+            if (!h->d_rb_ctr) CK(cudaMalloc(&h->d_rb_ctr, sizeof(unsigned int)));
+            CK(cudaMemsetAsync(h->d_rb_ctr, 0, sizeof(unsigned int), h->stream));
+            k_rb_select<<<grid_for(h, (uint64_t)h->nd * h->dv), 256, 0, h->stream>>>(
+                h->rec, h->dvcap, h->dv, h->nd, h->rb_min_len, cap, h->d_rb_slot, h->d_rb_sel, h->d_rb_ctr);
+            LAUNCHED();
+            k_rb_zero<<<h->num_sms * 8, 256, 0, h->stream>>>(h->d_rb_bits, h->rb_words, cap, h->d_rb_ctr);
+            LAUNCHED();
+            k_rb_fill<<<h->num_sms * 8, 256, 0, h->stream>>>(h->rec, h->dvcap, h->pool, h->d_rb_sel, cap, h->d_rb_ctr,
+                                                             h->d_rb_bits, h->rb_words);
+            LAUNCHED();
+            CK(cudaGetLastError());
+        }
+
         // 3. matching
         DfsArgs da;
         da.rec = h->rec;
@@ -1859,6 +1992,9 @@ cgb_status cgb_apply_batch_device(cgb_handle* h, uint32_t dv_count, const uint64
         da.vb = (h->cfg.flags & CGB_FLAG_MASK_PRUNE) ? h->d_vb : nullptr;
         da.vb_stride = h->vb_stride;
         da.qv = h->q.qv;
+        da.rb_slot = rb_on ? h->d_rb_slot : nullptr;
+        da.rb_bits = h->d_rb_bits;
+        da.rb_words = h->rb_words;
         da.budget_ns = h->cfg.dfs_budget_ms ? (unsigned long long)h->cfg.dfs_budget_ms * 1000000ull
                                             : 600ull * 1000000000ull;
         // persistent grid: exactly the blocks that can be resident at once

@@ -56,6 +56,7 @@ FLAG_PLAIN_CORE_ORDER = 0x20
 FLAG_VALID_BITS = 0x40
 FLAG_MASK_PRUNE = 0x80
 FLAG_NO_SEED_GROUPS = 0x100
+FLAG_NO_RUN_BITS = 0x200
 
 
 class BatchKeys(ctypes.Structure):

@@ -63,6 +63,7 @@ typedef struct {
 #define CGB_FLAG_VALID_BITS 0x40u         /* compute the reference's valid bits every matched batch     */
 #define CGB_FLAG_MASK_PRUNE 0x80u         /* valid bits, and skip core candidates whose bit is clear    */
 #define CGB_FLAG_NO_SEED_GROUPS 0x100u    /* one DFS per seed even where a pendant endpoint allows one per group */
+#define CGB_FLAG_NO_RUN_BITS 0x200u       /* binary-search long runs instead of testing their per-batch bit sets */
 
 /* Limits (reference: utils/config.h:5-6; key layout calig_helper_gamma.cu:228-229). */
 #define CGB_MAX_QV 12

@@ -10,8 +10,8 @@ import numpy as np
 import pytest
 
 from cgbdsm_b200 import CgbError, Engine
-from cgbdsm_b200.engine import (FLAG_ENUMERATE_TAIL, FLAG_FORCE_SPLIT, FLAG_MASK_PRUNE, FLAG_NO_SEED_GROUPS,
-                                FLAG_NO_TAIL_CACHE, FLAG_VALID_BITS)
+from cgbdsm_b200.engine import (FLAG_ENUMERATE_TAIL, FLAG_FORCE_SPLIT, FLAG_MASK_PRUNE, FLAG_NO_RUN_BITS,
+                                FLAG_NO_SEED_GROUPS, FLAG_NO_TAIL_CACHE, FLAG_VALID_BITS)
 from cgbdsm_b200.workloads import SPECS, materialize, read_query
 from oracle import bind
 
@@ -25,9 +25,9 @@ def _key(d, u, v):
 
 
 @pytest.mark.parametrize("flags", [0, FLAG_ENUMERATE_TAIL, FLAG_FORCE_SPLIT | FLAG_ENUMERATE_TAIL, FLAG_FORCE_SPLIT,
-                                   FLAG_NO_TAIL_CACHE, FLAG_NO_SEED_GROUPS],
+                                   FLAG_NO_TAIL_CACHE, FLAG_NO_SEED_GROUPS, FLAG_NO_RUN_BITS],
                          ids=["counted_tail", "enumerated_tail", "stolen_enumerated", "stolen_counted",
-                              "counted_no_prefix_cache", "seed_per_dfs"])
+                              "counted_no_prefix_cache", "seed_per_dfs", "searched_runs"])
 @pytest.mark.parametrize("name", PIPELINE_CASES)
 def test_engine_matches_reference_cpu_path(name, flags, workdir):
     if not bind.have_ref():
@@ -88,6 +88,21 @@ def test_random_streams_with_self_loops(seed):
     change the counted tails: a matched vertex then lies in its own list and
     must be excluded from it."""
     _random_stream(100 + seed, 0.15)
+
+
+@pytest.mark.parametrize("name", PIPELINE_CASES)
+def test_every_run_bitset_matches_reference(name, workdir, monkeypatch):
+    """Long runs are tested through per-batch bit sets (DFS probes and tail
+    counts); with the length threshold at 1 every run has one.  Counts and
+    index stay the reference's."""
+    monkeypatch.setenv("CGB_RUN_BITS_MIN_LEN", "1")
+    test_engine_matches_reference_cpu_path(name, FLAG_FORCE_SPLIT if name == "t_rmat" else 0, workdir)
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_every_run_bitset_random_streams(seed, monkeypatch):
+    monkeypatch.setenv("CGB_RUN_BITS_MIN_LEN", "1")
+    _random_stream(300 + seed, 0.1 if seed % 2 else 0.0, nlabels=seed % 4)
 
 
 @pytest.mark.parametrize("seed", range(12))
