@@ -907,7 +907,17 @@ void CaLiGIndex::update_index(uint32_t start, uint32_t count) {
         std::vector<std::pair<uint64_t, uint32_t>> ins;
         std::vector<uint32_t> vals;
         auto apply = [&](auto&& list_of) {
-            std::sort(ins.begin(), ins.end());
+            // group by list, values ascending: packed list << 27 | value keys
+            // (vertex ids < 2^27) radix-sorted when the list index fits
+            const int lb = 64 - __builtin_clzll((unsigned long long)lists_.size() | 1ull);
+            if (lb <= 37) {
+                std::vector<uint64_t> key(ins.size());
+                for (size_t i = 0; i < ins.size(); ++i) key[i] = ins[i].first << 27 | ins[i].second;
+                radix_sort(key, lb + 27);
+                for (size_t i = 0; i < ins.size(); ++i) ins[i] = {key[i] >> 27, (uint32_t)(key[i] & ((1u << 27) - 1u))};
+            } else {
+                std::sort(ins.begin(), ins.end());
+            }
             for (size_t g0 = 0; g0 < ins.size();) {
                 size_t g1 = g0 + 1;
                 while (g1 < ins.size() && ins[g1].first == ins[g0].first) ++g1;
