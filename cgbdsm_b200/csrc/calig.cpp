@@ -18,8 +18,13 @@ namespace cgb {
 
 namespace {
 
-// Workers wait on a generation counter: a job bumps it; each worker runs
-// the tasks it claims from a shared counter, the caller too, and the caller
+// Workers wait on a generation counter: a job bumps it, and tasks are
+// claimed from `claim_` = generation << 32 | next index by compare-and-swap,
+// so a worker only ever claims tasks of the generation it woke for, while
+// that generation is current.  Before a new job replaces (fn_, ntasks_), the
+// old generation is closed in `claim_` (index field all ones); a late worker
+// that reads the new ntasks_ is therefore ordered after the close and its
+// compare-and-swap on the old value fails.  The caller takes tasks too and
 // returns when every task has finished.  Workers spin briefly before
 // sleeping, so back-to-back phases do not pay a wake-up.
 class WorkerPool {
@@ -30,27 +35,27 @@ public:
     ~WorkerPool() {
         {
             std::lock_guard<std::mutex> g(m_);
-            stop_ = true;
-            ++gen_;
+            stop_.store(true, std::memory_order_relaxed);
+            gen_.fetch_add(1, std::memory_order_release);
         }
         cv_.notify_all();
         for (auto& t : workers_) t.join();
     }
-    uint32_t size() const { return (uint32_t)workers_.size(); }
     void run(uint32_t n, const std::function<void(uint32_t)>& fn) {
         std::lock_guard<std::mutex> job(job_m_);
+        const uint32_t g = (uint32_t)gen_.load(std::memory_order_relaxed) + 1u;
+        claim_.store((uint64_t)(g - 1u) << 32 | kClosed, std::memory_order_relaxed);
         fn_ = &fn;
-        ntasks_ = n;
-        next_.store(0, std::memory_order_relaxed);
+        ntasks_.store(n, std::memory_order_release);
         done_.store(0, std::memory_order_relaxed);
         {
-            std::lock_guard<std::mutex> g(m_);
+            std::lock_guard<std::mutex> lk(m_);
+            claim_.store((uint64_t)g << 32, std::memory_order_release);
             gen_.fetch_add(1, std::memory_order_release);
         }
         cv_.notify_all();
-        work();
+        work(g);
         while (done_.load(std::memory_order_acquire) < n) std::this_thread::yield();
-        fn_ = nullptr;
     }
     static thread_local bool in_job;
 
@@ -59,17 +64,21 @@ private:
     std::mutex m_, job_m_;
     std::condition_variable cv_;
     std::atomic<uint64_t> gen_{0};
-    std::atomic<uint32_t> next_{0}, done_{0};
+    std::atomic<uint64_t> claim_{0};
+    std::atomic<uint32_t> done_{0};
+    std::atomic<bool> stop_{false};
+    std::atomic<uint32_t> ntasks_{0};
     const std::function<void(uint32_t)>* fn_ = nullptr;
-    uint32_t ntasks_ = 0;
-    bool stop_ = false;
+    static constexpr uint32_t kClosed = 0xffffffffu;
 
-    void work() {
+    void work(uint32_t g) {
         in_job = true;
         for (;;) {
-            const uint32_t k = next_.fetch_add(1, std::memory_order_relaxed);
-            if (k >= ntasks_) break;
-            (*fn_)(k);
+            uint64_t c = claim_.load(std::memory_order_acquire);
+            if ((uint32_t)(c >> 32) != g || (uint32_t)c >= ntasks_.load(std::memory_order_acquire)) break;
+            if (!claim_.compare_exchange_weak(c, c + 1, std::memory_order_acq_rel, std::memory_order_acquire))
+                continue;
+            (*fn_)((uint32_t)c);
             done_.fetch_add(1, std::memory_order_release);
         }
         in_job = false;
@@ -88,8 +97,8 @@ private:
                 g = gen_.load(std::memory_order_acquire);
             }
             seen = g;
-            if (stop_) return;
-            work();
+            if (stop_.load(std::memory_order_relaxed)) return;
+            work((uint32_t)g);
         }
     }
 };
