@@ -253,23 +253,104 @@ void radix_sort(std::vector<uint64_t>& a, int bits) {
     }
 }
 
+// LSD radix sort of a[0..n) by the low `bits` bits, 11 bits per pass, with
+// buf[0..n) as scratch; the result is left in a.
+void radix_sort_range(uint64_t* a, uint64_t* buf, size_t n, int bits) {
+    size_t cnt[2049];
+    uint64_t *src = a, *dst = buf;
+    for (int shift = 0; shift < bits; shift += 11) {
+        std::fill(cnt, cnt + 2049, 0);
+        for (size_t i = 0; i < n; ++i) ++cnt[((src[i] >> shift) & 2047) + 1];
+        for (int i = 0; i < 2048; ++i) cnt[i + 1] += cnt[i];
+        for (size_t i = 0; i < n; ++i) dst[cnt[(src[i] >> shift) & 2047]++] = src[i];
+        std::swap(src, dst);
+    }
+    if (src != a) std::copy(src, src + n, a);
+}
+
 // Sorts a task queue by (v, u) and drops repeats.  Repeated tasks in the
 // reference's queues only redo inserts that fail and checks guarded by the
 // checked bit, so processing each distinct task once yields the same index
-// and deltas.  Keys v << 5 | u (query vertices < 32), radix-sorted.
-template <typename T>
-void dedupe(std::vector<T>& q) {
-    if (q.size() < 2) return;
-    std::vector<uint64_t> key(q.size());
-    uint64_t top = 0;
-    for (size_t i = 0; i < q.size(); ++i) {
-        key[i] = (uint64_t)q[i].v << 5 | q[i].u;
-        top |= key[i];
+// and deltas.  Keys v << 5 | u (query vertices < 32), radix-sorted.  With
+// T > 1 threads the keys are split by their top (up to) 11 bits into ranges,
+// counted and scattered by T slices, and each range is sorted and
+// deduplicated on its own: many more ranges than threads, so the ranges of
+// low ids that skewed graphs crowd do not serialise the sort.
+template <typename Q>
+void dedupe(std::vector<Q>& q, uint32_t T) {
+    const size_t n = q.size();
+    if (n < 2) return;
+    std::vector<uint64_t> key(n);
+    if (T <= 1) {
+        uint64_t top = 0;
+        for (size_t i = 0; i < n; ++i) {
+            key[i] = (uint64_t)q[i].v << 5 | q[i].u;
+            top |= key[i];
+        }
+        radix_sort(key, 64 - __builtin_clzll(top | 1));
+        key.erase(std::unique(key.begin(), key.end()), key.end());
+        q.resize(key.size());
+        for (size_t i = 0; i < key.size(); ++i) q[i] = {(uint32_t)(key[i] & 31u), (uint32_t)(key[i] >> 5)};
+        return;
     }
-    radix_sort(key, 64 - __builtin_clzll(top | 1));
-    key.erase(std::unique(key.begin(), key.end()), key.end());
-    q.resize(key.size());
-    for (size_t i = 0; i < key.size(); ++i) q[i] = {(uint32_t)(key[i] & 31u), (uint32_t)(key[i] >> 5)};
+    std::vector<uint64_t> tops(T, 0);
+    run_threads(T, [&](uint32_t s) {
+        uint64_t top = 0;
+        for (size_t i = n * s / T; i < n * (s + 1) / T; ++i) {
+            key[i] = (uint64_t)q[i].v << 5 | q[i].u;
+            top |= key[i];
+        }
+        tops[s] = top;
+    });
+    uint64_t top = 0;
+    for (uint64_t t : tops) top |= t;
+    const int bits = 64 - __builtin_clzll(top | 1);
+    const int hb = std::min(bits, 11), shift = bits - hb;
+    const size_t B = (size_t)1 << hb;
+    std::vector<size_t> at((size_t)T * B, 0);  // [slice * B + range]: count, then write position
+    run_threads(T, [&](uint32_t s) {
+        size_t* c = &at[(size_t)s * B];
+        for (size_t i = n * s / T; i < n * (s + 1) / T; ++i) ++c[key[i] >> shift];
+    });
+    std::vector<size_t> rs(B + 1);  // range starts
+    size_t run = 0;
+    for (size_t r = 0; r < B; ++r) {
+        rs[r] = run;
+        for (uint32_t s = 0; s < T; ++s) {
+            const size_t c = at[(size_t)s * B + r];
+            at[(size_t)s * B + r] = run;
+            run += c;
+        }
+    }
+    rs[B] = run;
+    std::vector<uint64_t> tmp(n);
+    run_threads(T, [&](uint32_t s) {
+        size_t* w = &at[(size_t)s * B];
+        for (size_t i = n * s / T; i < n * (s + 1) / T; ++i) tmp[w[key[i] >> shift]++] = key[i];
+    });
+    // ranges in groups of 16 per task; keys of one range agree above `shift`
+    constexpr size_t G = 16;
+    const uint32_t ntask = (uint32_t)((B + G - 1) / G);
+    std::vector<size_t> uniq(B);
+    run_threads(ntask, [&](uint32_t g) {
+        for (size_t r = g * G; r < std::min(B, (g + 1) * G); ++r) {
+            uint64_t* a = tmp.data() + rs[r];
+            const size_t m = rs[r + 1] - rs[r];
+            if (m < 64) std::sort(a, a + m);
+            else radix_sort_range(a, key.data() + rs[r], m, shift);
+            uniq[r] = (size_t)(std::unique(a, a + m) - a);
+        }
+    });
+    std::vector<size_t> uo(B + 1, 0);
+    for (size_t r = 0; r < B; ++r) uo[r + 1] = uo[r] + uniq[r];
+    q.resize(uo[B]);
+    run_threads(ntask, [&](uint32_t g) {
+        for (size_t r = g * G; r < std::min(B, (g + 1) * G); ++r)
+            for (size_t j = 0; j < uniq[r]; ++j) {
+                const uint64_t x = tmp[rs[r] + j];
+                q[uo[r] + j] = {(uint32_t)(x & 31u), (uint32_t)(x >> 5)};
+            }
+    });
 }
 
 }  // namespace
@@ -629,61 +710,60 @@ bool CaLiGIndex::check_nei(uint32_t v, uint32_t u) {
 // owner keeps.
 
 // The items of a round are the entries of the lists C(t.v, t.u, uj) of every
-// task t and every uj in qnei_[t.u], in queue order.  segments() lists one
-// Seg per such list with the index of its first item and returns the item
-// count; scan_items() visits items [lo, hi) in order, so T threads can take
-// equal shares even when one hub task holds most of a round.
-size_t CaLiGIndex::segments(const std::vector<Task>& q, std::vector<Seg>& segs) {
-    // the list headers are cache misses: tasks in T index slices, then the
-    // slices' item offsets shifted by the running total
+// task t and every uj in qnei_[t.u], in queue order.  item_offsets() sets
+// first[i] to the index of task i's first item (first[n] = the item count,
+// returned); scan_items() visits items [lo, hi) in order, so T threads can
+// take equal shares even when one hub task holds most of a round.
+size_t CaLiGIndex::item_offsets(const std::vector<Task>& q, std::vector<size_t>& first) {
+    // the list headers are cache misses: counts in T index slices, then one
+    // prefix pass over the tasks
     const uint32_t n = (uint32_t)q.size();
     const uint32_t T = n >= par_min_ / 8 ? threads_ : 1u;
-    std::vector<std::vector<Seg>> part(T);
-    std::vector<size_t> sum(T + 1, 0);
+    first.resize((size_t)n + 1);
+    first[0] = 0;
     run_threads(T, [&](uint32_t s) {
-        size_t total = 0;
-        for (uint32_t i = (uint32_t)((uint64_t)n * s / T); i < (uint32_t)((uint64_t)n * (s + 1) / T); ++i)
-            for (uint32_t uj : qnei_[q[i].u]) {
-                const size_t len = C(q[i].v, q[i].u, uj).size();
-                if (len) part[s].push_back({i, uj, total});
-                total += len;
-            }
-        sum[s + 1] = total;
+        for (uint32_t i = (uint32_t)((uint64_t)n * s / T); i < (uint32_t)((uint64_t)n * (s + 1) / T); ++i) {
+            size_t c = 0;
+            for (uint32_t uj : qnei_[q[i].u]) c += C(q[i].v, q[i].u, uj).size();
+            first[(size_t)i + 1] = c;
+        }
     });
-    segs.clear();
-    for (uint32_t s = 0; s < T; ++s) {
-        sum[s + 1] += sum[s];
-        for (auto& sg : part[s]) segs.push_back({sg.task, sg.uj, sg.first + sum[s]});
-    }
-    return sum[T];
+    for (uint32_t i = 0; i < n; ++i) first[(size_t)i + 1] += first[i];
+    return first[n];
 }
 
 template <class Fn>
-void CaLiGIndex::scan_items(const std::vector<Task>& q, const std::vector<Seg>& segs, size_t lo, size_t hi,
+void CaLiGIndex::scan_items(const std::vector<Task>& q, const std::vector<size_t>& first, size_t lo, size_t hi,
                             Fn&& fn) {
     if (lo >= hi) return;
-    size_t g = (size_t)(std::upper_bound(segs.begin(), segs.end(), lo,
-                                         [](size_t x, const Seg& sg) { return x < sg.first; }) - segs.begin()) - 1;
-    for (size_t at = lo; at < hi && g < segs.size(); ++g) {
-        const Seg& sg = segs[g];
-        const Task& t = q[sg.task];
-        const auto& L = C(t.v, t.u, sg.uj);
-        const size_t end = std::min(hi, sg.first + L.size());
-        for (size_t p = at - sg.first; sg.first + p < end; ++p) fn(sg.task, t, sg.uj, L[p]);
-        at = end;
+    size_t i = (size_t)(std::upper_bound(first.begin(), first.end(), lo) - first.begin()) - 1;
+    for (size_t at = lo; at < hi && i < q.size(); ++i) {
+        const Task& t = q[i];
+        size_t base = first[i];
+        for (uint32_t uj : qnei_[t.u]) {
+            if (at >= hi) break;
+            const auto& L = C(t.v, t.u, uj);
+            const size_t len = L.size();
+            if (base + len > at) {
+                const size_t end = std::min(hi, base + len);
+                for (size_t p = at - base; base + p < end; ++p) fn((uint32_t)i, t, uj, L[p]);
+                at = end;
+            }
+            base += len;
+        }
     }
 }
 
 // calig.cpp:410-475 delAndCheck (one round; `del` becomes the next round).
 void CaLiGIndex::del_and_check(std::vector<Task>& del) {
-    dedupe(del);
-    std::vector<Seg> segs;
-    const size_t total = segments(del, segs);
+    dedupe(del, del.size() >= par_min_ / 8 ? threads_ : 1u);
+    std::vector<size_t> first;
+    const size_t total = item_offsets(del, first);
     const uint32_t T = total >= par_min_ ? threads_ : 1u;
     struct Item { uint64_t list; uint32_t vi, vj, ui, uj; };
     std::vector<std::vector<Item>> items((size_t)T * T);  // [slice * T + owner]
     run_threads(T, [&](uint32_t s) {
-        scan_items(del, segs, total * s / T, total * (s + 1) / T,
+        scan_items(del, first, total * s / T, total * (s + 1) / T,
                    [&](uint32_t, const Task& t, uint32_t uj, uint32_t vj) {
                        if (lit(vj, uj))
                            items[(size_t)s * T + owner(vj, T)].push_back({list_index(vj, uj, t.u), t.v, vj, t.u, uj});
@@ -792,20 +872,20 @@ void CaLiGIndex::del_and_check(std::vector<Task>& del) {
 // occurs once per round (tasks are distinct), so each is inserted once.
 void CaLiGIndex::add_and_check(std::vector<Task>& add, std::vector<Task>& settled,
                                std::vector<Task>& add_del, std::vector<Task>& activated) {
-    dedupe(add);
-    dedupe(settled);
+    dedupe(add, add.size() >= par_min_ / 8 ? threads_ : 1u);
+    dedupe(settled, settled.size() >= par_min_ / 8 ? threads_ : 1u);
     // one queue: activations first, then the settled tasks
     const size_t nfresh = add.size();
     add.insert(add.end(), settled.begin(), settled.end());
     settled.clear();
-    std::vector<Seg> segs;
-    const size_t total = segments(add, segs);
+    std::vector<size_t> first;
+    const size_t total = item_offsets(add, first);
     const uint32_t T = total >= par_min_ ? threads_ : 1u;
     struct Ins { uint64_t list; uint32_t vi, vj, ui, uj; };
     std::vector<std::vector<Ins>> ins((size_t)T * T);     // [slice * T + owner]
     std::vector<std::vector<Task>> check((size_t)T * T);
     run_threads(T, [&](uint32_t s) {
-        scan_items(add, segs, total * s / T, total * (s + 1) / T,
+        scan_items(add, first, total * s / T, total * (s + 1) / T,
                    [&](uint32_t i, const Task& t, uint32_t uj, uint32_t vj) {
                        const size_t b = (size_t)s * T + owner(vj, T);
                        if (i < nfresh) ins[b].push_back({list_index(vj, uj, t.u), t.v, vj, t.u, uj});

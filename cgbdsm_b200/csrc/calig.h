@@ -153,10 +153,9 @@ private:
     void add_and_check(std::vector<Task>& add, std::vector<Task>& settled, std::vector<Task>& add_del,
                        std::vector<Task>& activated);
     void del_and_check(std::vector<Task>& del);
-    struct Seg { uint32_t task, uj; size_t first; };
-    size_t segments(const std::vector<Task>& q, std::vector<Seg>& segs);
+    size_t item_offsets(const std::vector<Task>& q, std::vector<size_t>& first);
     template <class Fn>
-    void scan_items(const std::vector<Task>& q, const std::vector<Seg>& segs, size_t lo, size_t hi, Fn&& fn);
+    void scan_items(const std::vector<Task>& q, const std::vector<size_t>& first, size_t lo, size_t hi, Fn&& fn);
 };
 
 }  // namespace cgb
