@@ -200,28 +200,79 @@ inline bool sorted_has(const std::vector<uint32_t>& v, uint32_t x) {
     return std::binary_search(v.begin(), v.end(), x);
 }
 
-// Adds the ascending values x[0..k) to the sorted set L with one merge pass
-// (a hub's list takes many values per batch; one memmove each would be
-// quadratic).  The result is the set union, as k sorted_insert calls give.
-void insert_run(std::vector<uint32_t>& L, const uint32_t* x, size_t k) {
-    if (k == 1) { sorted_insert(L, x[0]); return; }
-    const size_t old = L.size();
-    L.insert(L.end(), x, x + k);
-    std::inplace_merge(L.begin(), L.begin() + (std::ptrdiff_t)old, L.end());
-    L.erase(std::unique(L.begin(), L.end()), L.end());
+// First index p >= r of the ascending d[0..n) with d[p] >= x, found by
+// galloping from r (exponential steps, then a binary search).
+inline size_t gallop_lb(const uint32_t* d, size_t n, size_t r, uint32_t x) {
+    size_t lo = r, hi = r, step = 1;
+    while (hi < n && d[hi] < x) {
+        lo = hi + 1;
+        hi += step;
+        step <<= 1;
+    }
+    if (hi > n) hi = n;
+    return (size_t)(std::lower_bound(d + lo, d + hi, x) - d);
 }
 
-// Removes the ascending distinct values x[0..k) from the sorted set L in one
-// pass; hit[i] = 1 when x[i] was present (what sorted_erase would return).
+// Adds the ascending values x[0..k) to the sorted set L: the result is the
+// set union, as k sorted_insert calls give (a hub's list takes many values
+// per batch; one memmove each would be quadratic).  Each value's insertion
+// point is found by galloping from the previous one; then L grows once and
+// the old stretches between the points move right with memmove, from the
+// back, so a long list that gains a few values is not walked element by
+// element.
+void insert_run(std::vector<uint32_t>& L, const uint32_t* x, size_t k) {
+    if (k == 1) { sorted_insert(L, x[0]); return; }
+    thread_local std::vector<size_t> pos;
+    thread_local std::vector<uint32_t> val;
+    pos.clear();
+    val.clear();
+    const size_t n = L.size();
+    size_t r = 0;
+    for (size_t j = 0; j < k; ++j) {
+        if (j && x[j] == x[j - 1]) continue;
+        const size_t p = gallop_lb(L.data(), n, r, x[j]);
+        r = p;
+        if (p < n && L[p] == x[j]) continue;
+        pos.push_back(p);
+        val.push_back(x[j]);
+    }
+    if (pos.empty()) return;
+    const size_t m = pos.size();
+    L.resize(n + m);
+    uint32_t* d = L.data();
+    // old entries [pos[i], end) have i + 1 new values before them
+    size_t end = n;
+    for (size_t i = m; i-- > 0;) {
+        const size_t p = pos[i];
+        if (end > p) std::memmove(d + p + i + 1, d + p, (end - p) * sizeof(uint32_t));
+        d[p + i] = val[i];
+        end = p;
+    }
+}
+
+// Removes the ascending distinct values x[0..k) from the sorted set L;
+// hit[i] = 1 when x[i] was present (what sorted_erase would return).  Each
+// value is found by galloping from the previous one and the kept stretches
+// between them move left with memmove.
 void erase_run(std::vector<uint32_t>& L, const uint32_t* x, size_t k, uint8_t* hit) {
     if (k == 1) { hit[0] = sorted_erase(L, x[0]); return; }
-    size_t w = 0, j = 0;
-    for (size_t i = 0; i < L.size(); ++i) {
-        while (j < k && x[j] < L[i]) hit[j++] = 0;
-        if (j < k && x[j] == L[i]) { hit[j++] = 1; continue; }
-        L[w++] = L[i];
+    uint32_t* d = L.data();
+    const size_t n = L.size();
+    size_t r = 0, w = 0;
+    for (size_t j = 0; j < k; ++j) {
+        const size_t p = gallop_lb(d, n, r, x[j]);
+        if (p > r) {
+            if (w != r) std::memmove(d + w, d + r, (p - r) * sizeof(uint32_t));
+            w += p - r;
+        }
+        r = p;
+        if (p < n && d[p] == x[j]) { hit[j] = 1; ++r; }
+        else hit[j] = 0;
     }
-    while (j < k) hit[j++] = 0;
+    if (n > r) {
+        if (w != r) std::memmove(d + w, d + r, (n - r) * sizeof(uint32_t));
+        w += n - r;
+    }
     L.resize(w);
 }
 
