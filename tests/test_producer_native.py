@@ -2,7 +2,8 @@
 own source: the persistent worker pool (calig.cpp WorkerPool, behind
 pool_run: back-to-back jobs of varied sizes, each task run exactly once and
 before its job returns) and the batched sorted-set edits (insert_run,
-erase_run) against the standard library's set algorithms."""
+erase_run) against the standard library's set algorithms, and the task-queue
+dedupe at 1, 3 and 8 threads against sort + unique."""
 import os
 import shutil
 import subprocess
