@@ -166,7 +166,8 @@ extern "C" cgb_status cgb_merge_keys_noalloc(const uint64_t* old_keys_device, ui
     if (!out_device || !out_n_device || (n_old && !old_keys_device) || (n_ins && !ins_device) ||
         (n_del && !del_device))
         return CGB_ERR_ARG;
-    if (n_ins + n_del > kMaxEdits) return CGB_ERR_LIMIT;  // more edits than the scratch array holds
+    // more edits than the scratch array holds (tested without forming n_ins + n_del, which could wrap)
+    if (n_ins > kMaxEdits || n_del > kMaxEdits - n_ins) return CGB_ERR_LIMIT;
     if (dv_count == 0 || dv_count > CGB_MAX_VID) return CGB_ERR_ARG;
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return CGB_ERR_CUDA;

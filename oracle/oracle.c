@@ -80,11 +80,6 @@ static int cmp_u64(const void* a, const void* b) {
     uint64_t x = *(const uint64_t*)a, y = *(const uint64_t*)b;
     return x < y ? -1 : x > y;
 }
-static int cmp_u32(const void* a, const void* b) {
-    uint32_t x = *(const uint32_t*)a, y = *(const uint32_t*)b;
-    return x < y ? -1 : x > y;
-}
-
 static void list_reserve(List* l, uint32_t n) {
     if (n <= l->cap) return;
     uint32_t c = l->cap ? l->cap : 4;

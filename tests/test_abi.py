@@ -31,3 +31,17 @@ def test_default_config_without_gpu():
     lib.cgb_default_config(ctypes.byref(cfg))
     assert (cfg.device, cfg.pool_words, cfg.dfs_blocks_per_sm, cfg.flags, cfg.dfs_budget_ms, cfg.shard_index,
             cfg.num_shards) == (0, 0, 0, 0, 0, 0, 0)
+
+
+def test_noalloc_limits_checked_before_any_device_call():
+    """The allocation-free index update refuses edit counts beyond its static scratch
+    (CGB_ERR_LIMIT = 4) and missing pointers (CGB_ERR_ARG = 1) on the host, before any
+    CUDA call, so these run without a GPU.  A pair of counts whose sum wraps 64 bits is
+    refused too."""
+    lib = engine.load_library()
+    p = ctypes.c_void_p(16)
+    cap = engine.NOALLOC_MAX_EDITS
+    for n_ins, n_del in ((cap + 1, 0), (0, cap + 1), (cap, 1), (2**64 - 1, 1), (1, 2**64 - 1)):
+        assert lib.cgb_merge_keys_noalloc(None, 0, p, n_ins, p, n_del, 10, p, p, None) == 4, (n_ins, n_del)
+    assert lib.cgb_merge_keys_noalloc(None, 0, p, 1, p, 0, 10, None, p, None) == 1
+    assert lib.cgb_merge_keys_noalloc(None, 5, p, 1, p, 0, 10, p, p, None) == 1
