@@ -49,6 +49,7 @@ constexpr uint32_t kFull = 0xffffffffu;
 constexpr int kDfsWarps = 8;  // warps per DFS block
 constexpr uint32_t kTaskCap = 1u << 20;  // stolen-range ring capacity (64 MiB), a power of two
 constexpr uint32_t kTaskSlack = 1u << 13; // tickets kept between the ring's tail and head
+constexpr uint64_t kMaxBatchKeys = 1ull << 36;  // per key array of one batch: 512 GiB, beyond any HBM
 
 __constant__ EdgePlan c_plan[kMaxQE];
 __constant__ cgb::VbPlan c_vb[kMaxQE];
@@ -1866,6 +1867,7 @@ cgb_status cgb_apply_batch_device(cgb_handle* h, uint32_t dv_count, const uint64
     if (dv_count < h->dv) return fail(h, CGB_ERR_ARG, "dv_count must not decrease (%u < %u)", dv_count, h->dv);
     if (dv_count > CGB_MAX_VID) return fail(h, CGB_ERR_LIMIT, "dv_count exceeds 2^27-1");
     if ((n_ins && !ins) || (n_del && !del) || (n_delta && !delta)) return CGB_ERR_ARG;
+    if (n_ins > kMaxBatchKeys || n_del > kMaxBatchKeys) return fail(h, CGB_ERR_LIMIT, "edit batch too large");
     if (n_delta > 0xffffffffull) return fail(h, CGB_ERR_LIMIT, "delta batch too large");
     CK(cudaSetDevice(h->device));
     cudaStream_t user = (cudaStream_t)stream;
@@ -2055,6 +2057,9 @@ cgb_status cgb_apply_batch(cgb_handle* h, uint32_t dv_count, const uint64_t* ins
                            const uint8_t* edge_ok, uint64_t* out_count) {
     if (!h || !out_count) return CGB_ERR_ARG;
     if ((n_ins && !ins) || (n_del && !del) || (n_delta && !delta)) return CGB_ERR_ARG;
+    // bounded before the sum below, which must not wrap
+    if (n_ins > kMaxBatchKeys || n_del > kMaxBatchKeys || n_delta > kMaxBatchKeys)
+        return fail(h, CGB_ERR_LIMIT, "batch too large");
     CK(cudaSetDevice(h->device));
     const uint64_t n = n_ins + n_del + n_delta;
     cgb_status s;
