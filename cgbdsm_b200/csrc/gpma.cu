@@ -529,6 +529,8 @@ cgb_status cgb_gpma_bulk_load(cgb_gpma* g, const uint64_t* keys_device, uint64_t
 cgb_status cgb_gpma_batch_update(cgb_gpma* g, const uint64_t* ins_device, uint64_t n_ins,
                                  const uint64_t* del_device, uint64_t n_del) {
     if (!g || (n_ins && !ins_device) || (n_del && !del_device)) return CGB_ERR_ARG;
+    // bounded before the sum below, which must not wrap (2^36 keys = 512 GiB, beyond any HBM)
+    if (n_ins > (1ull << 36) || n_del > (1ull << 36)) return gfail(g, CGB_ERR_LIMIT, "edit batch too large");
     GCK(cudaSetDevice(g->device));
     for (auto& x : g->stats) x = 0;
     const uint64_t n = n_ins + n_del;
