@@ -123,7 +123,7 @@ cgb_status cgb_producer_open(const char* query_path, const char* data_path, cons
             }
     p->qe = (uint32_t)p->qe_dir.size() / 2;
     const uint32_t nu = p->idx.num_update_ints();
-    p->num_batches = (p->batch_size >= nu) ? 1 : (nu + p->batch_size - 1) / p->batch_size;
+    p->num_batches = (p->batch_size >= nu) ? 1 : (uint32_t)(((uint64_t)nu + p->batch_size - 1) / p->batch_size);
     if (nu == 0) p->num_batches = 0;
     p->idx.construct();
     // ConvertGlobalIndex key generation (calig_helper_gamma.cu:248-277)
