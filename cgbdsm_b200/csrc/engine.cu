@@ -52,6 +52,8 @@ constexpr uint32_t kTaskSlack = 1u << 13; // tickets kept between the ring's tai
 constexpr uint64_t kMaxBatchKeys = 1ull << 36;  // per key array of one batch: 512 GiB, beyond any HBM
 
 __constant__ EdgePlan c_plan[kMaxQE];
+// plans are copied to shared memory as 32-bit words (k_dfs_count<true>)
+static_assert(sizeof(EdgePlan) % 4 == 0, "EdgePlan must be a whole number of words");
 __constant__ cgb::VbPlan c_vb[kMaxQE];
 __constant__ uint8_t c_dir_edge[kMaxDir];
 
@@ -62,6 +64,7 @@ struct PackInfo {
     uint32_t B;      // bits per vertex id
     uint32_t nd;     // directions
     uint32_t dv;     // compressed vertex count
+    uint32_t pad_ok; // an all-ones key is padding (skipped), not an invalid key
 };
 
 __device__ __forceinline__ bool decode_ext(uint64_t k, const PackInfo& pi, uint32_t& d, uint32_t& u,
@@ -88,7 +91,9 @@ __global__ void k_pack_edits(const uint64_t* __restrict__ in, uint64_t n, uint32
     uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
     for (; i < n; i += stride) {
         uint32_t d, u, v;
-        if (decode_ext(in[i], pi, d, u, v)) {
+        if (pi.pad_ok && in[i] == ~0ull) {
+            out[i] = ~0ull;
+        } else if (decode_ext(in[i], pi, d, u, v)) {
             if (op == 0 && u == v) atomicOr(self_seen, 1u);
             out[i] = (pack_duv(d, u, v, pi.B) << 1) | op;
         } else {
@@ -127,8 +132,14 @@ __global__ void k_extract_du(const uint64_t* __restrict__ in, uint64_t n, uint32
 }
 
 // ---------------------------------------------------------------------------
-// fused edit merge: one warp per touched (d, u)
+// fused edit merge of every touched (d, u): warp per run below kBigRun merged
+// entries, CTA per longer (hub) run
 // ---------------------------------------------------------------------------
+constexpr uint32_t kBigRun = 4096;       // merged entries (old run + edits) from which a CTA merges the run
+constexpr uint32_t kMergeWarps = 8;      // warps of a CTA merge
+constexpr uint32_t kSegWindows = 8;      // 32-entry windows a CTA warp merges per round
+constexpr uint32_t kNoVal = 0xffffffffu; // window padding: above every vertex id (< 2^27)
+
 struct MergeArgs {
     uint4* rec;
     uint32_t dvcap;
@@ -141,37 +152,153 @@ struct MergeArgs {
     const uint32_t* run_len;
     const uint32_t* run_off;
     const int* num_runs;
+    uint32_t* small_runs;        // run ids merged by a warp / by a CTA (k_merge_classify)
+    uint32_t* big_runs;
+    unsigned int* list_ctr;      // [0] small, [1] big
     uint32_t B;
     unsigned int* err;
     unsigned long long* stats;   // [5] merge bytes (edits 8 B, old run 4 B/word, new run 4 B/word, record 32 B), [6] runs
+    // run bit sets: a run that reaches rb_min_len without a bit set claims one
+    // (slot table [d][dvcap], slot owners, claim counter, new-slot list)
+    uint32_t* rb_slot;           // nullptr: not maintained by this merge
+    uint32_t* rb_sel;
+    unsigned int* rb_ctr;        // [0] slots claimed, [1] new slots this merge
+    uint32_t* rb_new;
+    uint32_t rb_cap;
+    uint32_t rb_min_len;
 };
 
 __device__ __forceinline__ uint32_t round4(uint32_t x) { return (x + 3u) & ~3u; }
 
-// Merge-path split for diagonal k of X (base values) and Y (edits, value = e>>1 & vmask):
-// X wins ties, so for equal values the base element precedes add, add precedes remove.
+// Number of entries of the ascending warp-held window w (lane k holds w[k],
+// padded with kNoVal) that are < x (or <= x when le): binary lifting over
+// shuffles, six steps.
+__device__ __forceinline__ uint32_t win_rank(uint32_t w, uint32_t x, bool le) {
+    uint32_t lo = 0;
+#pragma unroll
+    for (uint32_t step = 16; step >= 1; step >>= 1) {
+        const uint32_t v = __shfl_sync(kFull, w, lo + step - 1);
+        if (le ? v <= x : v < x) lo += step;
+    }
+    const uint32_t v = __shfl_sync(kFull, w, lo);
+    return lo + ((le ? v <= x : v < x) ? 1u : 0u);
+}
+
+// Merge-path split of diagonal k of X (old run) and Y (edits): the number of
+// X entries among the first k merged entries, X winning ties (so for equal
+// values the old entry precedes an add, and an add precedes a remove).
 __device__ __forceinline__ uint32_t merge_split(const uint32_t* X, uint32_t xl, const uint64_t* Y,
                                                 uint32_t yl, uint32_t k, uint64_t vmask) {
     uint32_t lo = k > yl ? k - yl : 0;
     uint32_t hi = k < xl ? k : xl;
     while (lo < hi) {
         uint32_t mid = (lo + hi) >> 1;
-        uint32_t yv = (uint32_t)((Y[k - 1 - mid] >> 1) & vmask);
-        if (X[mid] <= yv) lo = mid + 1;
+        uint32_t yv = (uint32_t)((__ldg(Y + (k - 1 - mid)) >> 1) & vmask);
+        if (__ldg(X + mid) <= yv) lo = mid + 1;
         else hi = mid;
     }
     return lo;
 }
 
+// One window step of a warp merge: the next nout (<= 32) entries of the merge
+// of X[i..) and Y[j..), from coalesced 32-entry windows of both.  Lane p
+// gets entry p in *val and whether it is emitted: the last entry of its value
+// group and not a remove, i.e. the set (X U adds) \ removes.  Advances i, j.
+// sbuf: 32 words of this warp's shared memory.
+__device__ __forceinline__ bool merge_window(const uint32_t* __restrict__ X, uint32_t xl,
+                                             const uint64_t* __restrict__ Y, uint32_t yl, uint64_t vmask,
+                                             uint32_t& i, uint32_t& j, uint32_t nout, uint32_t lane,
+                                             uint32_t* sbuf, uint32_t& val) {
+    const uint32_t xv = (i + lane < xl) ? __ldg(X + i + lane) : kNoVal;
+    uint32_t yv = kNoVal, yop = 0;
+    if (j + lane < yl) {
+        const uint64_t e = __ldg(Y + j + lane);
+        yv = (uint32_t)((e >> 1) & vmask);
+        yop = (uint32_t)(e & 1ull);
+    }
+    // merged position: an old entry follows the edits strictly below it, an
+    // edit follows the old entries up to and including its value
+    const uint32_t px = lane + win_rank(yv, xv, false);
+    const uint32_t py = lane + win_rank(xv, yv, true);
+    if (px < nout) sbuf[px] = xv;
+    if (py < nout) sbuf[py] = yv | (yop << 31);
+    const uint32_t cx = __popc(__ballot_sync(kFull, px < nout));
+    const uint32_t cy = nout - cx;
+    // the entry after the window's last: first unconsumed entry of X or Y
+    uint32_t nx = __shfl_sync(kFull, xv, cx & 31), ny = __shfl_sync(kFull, yv, cy & 31);
+    if (cx == 32) nx = (i + 32 < xl) ? __ldg(X + i + 32) : kNoVal;
+    if (cy == 32) ny = (j + 32 < yl) ? (uint32_t)((__ldg(Y + j + 32) >> 1) & vmask) : kNoVal;
+    __syncwarp();
+    bool emit = false;
+    if (lane < nout) {
+        const uint32_t e = sbuf[lane];
+        val = e & 0x7fffffffu;
+        const uint32_t nv = (lane + 1 < nout) ? (sbuf[lane + 1] & 0x7fffffffu) : min(nx, ny);
+        emit = nv != val && !(e >> 31);
+    }
+    __syncwarp();
+    i += cx;
+    j += cy;
+    return emit;
+}
+
+// Splits the runs into warp-merged and CTA-merged lists by merged length.
+__global__ void k_merge_classify(MergeArgs a) {
+    const int n = *a.num_runs;
+    const uint32_t vmask = (1u << a.B) - 1u;
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+        const uint32_t du = a.run_du[r];
+        if (du == 0xffffffffu) continue;  // invalid keys
+        const uint32_t xl = a.rec[(size_t)(du >> a.B) * a.dvcap + (du & vmask)].y;
+        if (xl + a.run_len[r] >= kBigRun) a.big_runs[atomicAdd(a.list_ctr + 1, 1u)] = (uint32_t)r;
+        else a.small_runs[atomicAdd(a.list_ctr + 0, 1u)] = (uint32_t)r;
+    }
+}
+
+// Pool space for a merged run of at most `bound` entries (~0 when exhausted).
+__device__ __forceinline__ unsigned long long pool_alloc(const MergeArgs& a, uint32_t bound) {
+    unsigned long long off = atomicAdd(a.pool_top, (unsigned long long)round4(bound));
+    if (off + round4(bound) > a.pool_cap) {
+        atomicOr(a.err, 4u);
+        off = ~0ull;
+    }
+    return off;
+}
+
+// Record update and accounting after a run was merged (one thread).
+__device__ __forceinline__ void merge_done(const MergeArgs& a, uint4* recp, uint4 old, unsigned long long off,
+                                           uint32_t outn, uint32_t yl, uint32_t d, uint32_t u) {
+    *recp = make_uint4((uint32_t)off, outn, old.z, old.w);
+    atomicAdd(a.stats + 5, 8ull * yl + 4ull * old.y + 4ull * outn + 32ull);
+    atomicAdd(a.stats + 6, 1ull);
+    long long dl = (long long)round4(outn) - (long long)round4(old.y);
+    if (dl) atomicAdd((unsigned long long*)a.live_words, (unsigned long long)dl);
+    // unused tail of the allocation is dead space until compaction
+    if (a.rb_slot && outn >= a.rb_min_len) {
+        uint32_t* sp = a.rb_slot + (size_t)d * a.dvcap + u;
+        if (*sp == kNoVal) {
+            const unsigned int c = atomicAdd(a.rb_ctr, 1u);
+            if (c < a.rb_cap) {
+                *sp = c;
+                a.rb_sel[c] = d << 27 | u;
+                a.rb_new[atomicAdd(a.rb_ctr + 1, 1u)] = c;
+            }
+        }
+    }
+}
+
+// Warp per run: 32 merged entries per step from two coalesced windows.
 __global__ void k_merge_runs(MergeArgs a) {
+    __shared__ uint32_t s_win[8][32];
     const uint32_t lane = threadIdx.x & 31;
     const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
-    const int nruns = *a.num_runs;
+    const uint32_t nruns = a.list_ctr[0];
     const uint64_t vmask = (1ull << a.B) - 1ull;
-    for (uint32_t r = gw; r < (uint32_t)nruns; r += nw) {
+    uint32_t* sbuf = s_win[(threadIdx.x >> 5) & 7];
+    for (uint32_t q = gw; q < nruns; q += nw) {
+        const uint32_t r = a.small_runs[q];
         const uint32_t du = a.run_du[r];
-        if (du == 0xffffffffu) continue;  // invalid keys
         const uint32_t d = du >> a.B, u = du & (uint32_t)vmask;
         const uint64_t* Y = a.edits + a.run_off[r];
         const uint32_t yl = a.run_len[r];
@@ -179,53 +306,85 @@ __global__ void k_merge_runs(MergeArgs a) {
         const uint4 old = *recp;
         const uint32_t* X = a.pool + old.x;
         const uint32_t xl = old.y;
-        const uint32_t bound = xl + yl;
         unsigned long long off = 0;
-        if (lane == 0) {
-            off = atomicAdd(a.pool_top, (unsigned long long)round4(bound));
-            if (off + round4(bound) > a.pool_cap) {
-                atomicOr(a.err, 4u);
-                off = ~0ull;
-            }
-        }
+        if (lane == 0) off = pool_alloc(a, xl + yl);
         off = __shfl_sync(kFull, off, 0);
         if (off == ~0ull) continue;  // pool exhausted: run left unchanged, error raised
         uint32_t* C = a.pool + off;
         const uint32_t total = xl + yl;
-        uint32_t outn = 0;
-        for (uint32_t k0 = 0; k0 < total; k0 += 32) {
-            const uint32_t k = k0 + lane;
-            bool emit = false;
+        uint32_t outn = 0, i = 0, j = 0;
+        for (uint32_t done = 0; done < total; done += 32) {
+            const uint32_t nout = min(32u, total - done);
             uint32_t val = 0;
-            if (k < total) {
-                uint32_t i = merge_split(X, xl, Y, yl, k, vmask);
-                uint32_t j = k - i;
-                // element k
-                bool fromX = (i < xl) && (j >= yl || X[i] <= (uint32_t)((Y[j] >> 1) & vmask));
-                uint32_t op = 0;
-                if (fromX) { val = X[i]; ++i; }
-                else { val = (uint32_t)((Y[j] >> 1) & vmask); op = (uint32_t)(Y[j] & 1ull); ++j; }
-                // element k + 1: last of its value group?
-                bool last = true;
-                if (k + 1 < total) {
-                    uint32_t nv = (i < xl && (j >= yl || X[i] <= (uint32_t)((Y[j] >> 1) & vmask)))
-                                      ? X[i] : (uint32_t)((Y[j] >> 1) & vmask);
-                    last = (nv != val);
-                }
-                emit = last && op == 0;
-            }
+            const bool emit = merge_window(X, xl, Y, yl, vmask, i, j, nout, lane, sbuf, val);
             const uint32_t bal = __ballot_sync(kFull, emit);
             if (emit) C[outn + __popc(bal & ((1u << lane) - 1u))] = val;
             outn += __popc(bal);
         }
-        if (lane == 0) {
-            *recp = make_uint4((uint32_t)off, outn, old.z, old.w);
-            atomicAdd(a.stats + 5, 8ull * yl + 4ull * xl + 4ull * outn + 32ull);
-            atomicAdd(a.stats + 6, 1ull);
-            long long dl = (long long)round4(outn) - (long long)round4(xl);
-            if (dl) atomicAdd((unsigned long long*)a.live_words, (unsigned long long)dl);
-            // unused tail of the allocation is dead space until compaction
+        if (lane == 0) merge_done(a, recp, old, off, outn, yl, d, u);
+    }
+}
+
+// CTA per long run: each round, warp w merges the 256 entries from diagonal
+// k0 + 256 w (one merge-path split per warp and round), stages what it emits
+// in shared memory, and the CTA writes the round's output contiguously.
+__global__ void __launch_bounds__(kMergeWarps * 32) k_merge_big(MergeArgs a) {
+    constexpr uint32_t kSeg = 32 * kSegWindows;
+    __shared__ uint32_t s_win[kMergeWarps][32];
+    __shared__ uint32_t s_out[kMergeWarps][kSeg];
+    __shared__ uint32_t s_cnt[kMergeWarps];
+    __shared__ unsigned long long s_off;
+    const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const uint32_t nruns = a.list_ctr[1];
+    const uint64_t vmask = (1ull << a.B) - 1ull;
+    for (uint32_t q = blockIdx.x; q < nruns; q += gridDim.x) {
+        const uint32_t r = a.big_runs[q];
+        const uint32_t du = a.run_du[r];
+        const uint32_t d = du >> a.B, u = du & (uint32_t)vmask;
+        const uint64_t* Y = a.edits + a.run_off[r];
+        const uint32_t yl = a.run_len[r];
+        uint4* recp = a.rec + (size_t)d * a.dvcap + u;
+        const uint4 old = *recp;
+        const uint32_t* X = a.pool + old.x;
+        const uint32_t xl = old.y;
+        const uint32_t total = xl + yl;
+        if (threadIdx.x == 0) s_off = pool_alloc(a, total);
+        __syncthreads();
+        const unsigned long long off = s_off;
+        if (off == ~0ull) { __syncthreads(); continue; }
+        uint32_t* C = a.pool + off;
+        uint32_t outn = 0;
+        for (uint32_t k0 = 0; k0 < total; k0 += kMergeWarps * kSeg) {
+            const uint32_t ks = k0 + w * kSeg;
+            uint32_t cnt = 0;
+            if (ks < total) {
+                const uint32_t ke = min(ks + kSeg, total);
+                uint32_t i = 0;
+                if (lane == 0) i = merge_split(X, xl, Y, yl, ks, vmask);
+                i = __shfl_sync(kFull, i, 0);
+                uint32_t j = ks - i;
+                for (uint32_t k = ks; k < ke; k += 32) {
+                    const uint32_t nout = min(32u, ke - k);
+                    uint32_t val = 0;
+                    const bool emit = merge_window(X, xl, Y, yl, vmask, i, j, nout, lane, s_win[w], val);
+                    const uint32_t bal = __ballot_sync(kFull, emit);
+                    if (emit) s_out[w][cnt + __popc(bal & ((1u << lane) - 1u))] = val;
+                    cnt += __popc(bal);
+                }
+            }
+            if (lane == 0) s_cnt[w] = cnt;
+            __syncthreads();
+            uint32_t before = 0, all = 0;
+            for (uint32_t t = 0; t < kMergeWarps; ++t) {
+                before += t < w ? s_cnt[t] : 0u;
+                all += s_cnt[t];
+            }
+            for (uint32_t t = lane; t < cnt; t += 32) C[outn + before + t] = s_out[w][t];
+            outn += all;
+            __syncthreads();
         }
+        if (threadIdx.x == 0) merge_done(a, recp, old, off, outn, yl, d, u);
+        __syncthreads();
     }
 }
 
@@ -239,14 +398,15 @@ __global__ void k_delta_values(const uint64_t* __restrict__ keys, uint64_t n, ui
     for (; i < n; i += stride) dval[i] = (uint32_t)(keys[i] & vmask);
 }
 
+// du = (d << lb | label bits) << B | u (lb = 0: no label bits).
 __global__ void k_delta_recs(uint4* rec, uint32_t dvcap, const uint32_t* run_du, const uint32_t* run_len,
-                             const uint32_t* run_off, const int* num_runs, uint32_t B, int clear) {
+                             const uint32_t* run_off, const int* num_runs, uint32_t B, int clear, uint32_t lb = 0) {
     const int n = *num_runs;
     const uint32_t umask = (1u << B) - 1u;
     for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
         uint32_t du = run_du[r];
         if (du == 0xffffffffu) continue;
-        uint4* p = rec + (size_t)(du >> B) * dvcap + (du & umask);
+        uint4* p = rec + (size_t)(du >> (B + lb)) * dvcap + (du & umask);
         uint4 v = *p;
         if (clear) { v.z = 0; v.w = 0; }
         else { v.z = run_off[r]; v.w = run_len[r]; }
@@ -298,23 +458,23 @@ constexpr uint32_t kNoSlot = 0xffffffffu;
 constexpr uint32_t kRunBitsMinLen = 128;        // $CGB_RUN_BITS_MIN_LEN overrides (tests use 1)
 constexpr size_t kRunBitsBytes = 512ull << 20;  // runs beyond this budget are searched
 
-// Slot of every (direction, vertex) whose old run is long enough, in claim
-// order while slots last (ctr counts claims), else kNoSlot; sel[slot] =
-// dir << 27 | vertex.
-__global__ void k_rb_select(const uint4* __restrict__ rec, uint32_t dvcap, uint32_t dv, uint32_t nd, uint32_t min_len,
+// Full rebuild: the slot of every (direction, vertex) of the table (all
+// dvcap rows) whose run is long enough, in claim order while slots last
+// (ctr[0] counts claims), else kNoSlot; sel[slot] = dir << 27 | vertex.
+// Afterwards each merge keeps the sets current (k_rb_fill_new, k_rb_edits).
+__global__ void k_rb_select(const uint4* __restrict__ rec, uint32_t dvcap, uint32_t nd, uint32_t min_len,
                             uint32_t cap, uint32_t* slot, uint32_t* sel, unsigned int* ctr) {
-    const size_t n = (size_t)nd * dv;
+    const size_t n = (size_t)nd * dvcap;
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-        const uint32_t d = (uint32_t)(i / dv), u = (uint32_t)(i % dv);
         uint32_t sl = kNoSlot;
-        if (rec[(size_t)d * dvcap + u].y >= min_len) {
+        if (rec[i].y >= min_len) {
             const unsigned int c = atomicAdd(ctr, 1u);
             if (c < cap) {
                 sl = c;
-                sel[c] = d << 27 | u;
+                sel[c] = (uint32_t)(i / dvcap) << 27 | (uint32_t)(i % dvcap);
             }
         }
-        slot[(size_t)d * dvcap + u] = sl;
+        slot[i] = sl;
     }
 }
 
@@ -343,6 +503,80 @@ __global__ void k_rb_fill(const uint4* __restrict__ rec, uint32_t dvcap, const u
     }
 }
 
+// Slots claimed by runs that grew past the length threshold in this merge
+// (ctr[1] of them, listed in fresh): zeroed, then filled from the merged run.
+__global__ void k_rb_fill_new(const uint4* __restrict__ rec, uint32_t dvcap, const uint32_t* __restrict__ pool,
+                              const uint32_t* __restrict__ sel, const uint32_t* __restrict__ fresh,
+                              const unsigned int* ctr, uint32_t* bits, uint32_t words) {
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t n = ctr[1];
+    const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t q = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; q < n; q += nw) {
+        const uint32_t c = fresh[q];
+        const uint32_t du = sel[c];
+        const uint4 r = rec[(size_t)(du >> 27) * dvcap + (du & ((1u << 27) - 1u))];
+        uint32_t* b = bits + (size_t)c * words;
+        for (uint32_t t = lane; t < words; t += 32) b[t] = 0;
+        __syncwarp();
+        for (uint32_t t = lane; t < r.y; t += 32) {
+            const uint32_t v = __ldg(pool + r.x + t);
+            atomicOr(b + (v >> 5), 1u << (v & 31));
+        }
+    }
+}
+
+// Applies a merge's sorted edits ((d,u,v) << 1 | op) to the bit sets of
+// runs that have one: the last edit of each (d,u,v) decides, as in the merge
+// (an add sets the bit, a remove clears it).
+__global__ void k_rb_edits(const uint64_t* __restrict__ edits, uint64_t n, uint32_t B, uint32_t dvcap,
+                           const uint32_t* __restrict__ slot, uint32_t* bits, uint32_t words) {
+    const uint64_t vmask = (1ull << B) - 1ull;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t e = edits[i];
+        if (e == ~0ull) continue;
+        if (i + 1 < n && (edits[i + 1] >> 1) == (e >> 1)) continue;  // not the last edit of its value
+        const uint64_t p = e >> 1;
+        const uint32_t v = (uint32_t)(p & vmask), u = (uint32_t)((p >> B) & vmask), d = (uint32_t)(p >> (2 * B));
+        const uint32_t sl = slot[(size_t)d * dvcap + u];
+        if (sl == kNoSlot) continue;
+        uint32_t* w = bits + (size_t)sl * words + (v >> 5);
+        if (e & 1ull) atomicAnd(w, ~(1u << (v & 31)));
+        else atomicOr(w, 1u << (v & 31));
+    }
+}
+
+// Index symmetry: number of entries y in run (d, x) whose mirror entry (x in
+// run (rev[d], y)) is missing.  Warp per run.
+__global__ void k_asymmetry(const uint4* __restrict__ rec, uint32_t dvcap, uint32_t dv, uint32_t nd,
+                            const uint32_t* __restrict__ pool, const uint8_t* __restrict__ rev,
+                            unsigned long long* bad) {
+    const uint32_t lane = threadIdx.x & 31;
+    const uint64_t total = (uint64_t)nd * dv;
+    unsigned long long miss = 0;
+    for (uint64_t i = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < total;
+         i += ((uint64_t)gridDim.x * blockDim.x) >> 5) {
+        const uint32_t d = (uint32_t)(i / dv), x = (uint32_t)(i % dv);
+        const uint4 r = rec[(size_t)d * dvcap + x];
+        const uint32_t rd = rev[d];
+        for (uint32_t t = lane; t < r.y; t += 32) {
+            const uint32_t y = pool[r.x + t];
+            bool ok = false;
+            if (y < dv && rd < nd) {
+                const uint4 m = rec[(size_t)rd * dvcap + y];
+                uint32_t lo = 0, hi = m.y;
+                while (lo < hi) {
+                    const uint32_t mid = (lo + hi) >> 1;
+                    if (pool[m.x + mid] < x) lo = mid + 1; else hi = mid;
+                }
+                ok = lo < m.y && pool[m.x + lo] == x;
+            }
+            miss += ok ? 0 : 1;
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) miss += __shfl_xor_sync(kFull, miss, o);
+    if (lane == 0 && miss) atomicAdd(bad, miss);
+}
+
 // ---------------------------------------------------------------------------
 // persistent warp DFS (count only)
 // ---------------------------------------------------------------------------
@@ -366,7 +600,7 @@ struct DfsArgs {
     unsigned int* qctr;          // [8]: tasks reserved, tickets issued, -, completed, -, -, seeds issued
     uint32_t epoch;              // per-launch tag written as a task's ready flag (never 0)
     uint32_t force_split;        // publish unstarted work at every chunk, waited for or not (tests)
-    uint32_t shard, num_shards;  // this engine expands seeds i with i % num_shards == shard
+    uint32_t shard, num_shards;  // this engine expands the seed groups whose key hashes to shard (seed_shard)
     uint32_t steal;              // share long shallow ranges through the queue
     uint32_t tail_cache;         // count prefix-only tail subsets once per prefix
     const unsigned int* self_seen;  // sticky self-loop flag (see k_pack_edits)
@@ -376,7 +610,17 @@ struct DfsArgs {
     const uint32_t* rb_slot;     // run bit sets: slot of (dir, vertex) [nd][dvcap] or nullptr (none)
     const uint32_t* rb_bits;     // [slot][rb_words]
     uint32_t rb_words;
+    const EdgePlan* plans;       // k_dfs_count<true>: every registered query's plans
+    const unsigned int* epoch_ptr;  // non-null: the launch tag is read here (k_epoch_bump)
 };
+
+// Next launch tag for a DFS launch that reads it from memory; the low 20
+// bits (the tag's epoch field) are never 0.
+__global__ void k_epoch_bump(unsigned int* e) {
+    unsigned int v = *e + 1;
+    if ((v & 0xfffffu) == 0) ++v;
+    *e = v;
+}
 
 __device__ __forceinline__ unsigned long long global_ns() {
     unsigned long long t;
@@ -712,8 +956,8 @@ __device__ __forceinline__ unsigned long long warp_sum(unsigned long long x) {
 }
 
 // Work units of the DFS: seeds (delta edges) from a counter, and stolen
-// ranges from a ring of tasks.  A task is 16 words: w0 = ei | depth << 8 |
-// generator << 16, w1/w2 = [lo, hi) of the generator list, w3 = ready tag,
+// ranges from a ring of tasks.  A task is 16 words: w0 = ei | depth << 16 |
+// generator << 24, w1/w2 = [lo, hi) of the generator list, w3 = ready tag,
 // w4..15 = the matched prefix.  A warp without a seed takes one ticket
 // (atomicAdd on the ticket counter) and waits for task number `ticket`;
 // tasks are numbered by an atomicAdd in the same order, so every task has
@@ -817,29 +1061,56 @@ struct SeedGroup {
 __device__ __forceinline__ uint32_t task_tag(uint32_t epoch, uint32_t t) {
     return ((epoch & 0xfffffu) << 12) | ((t / kTaskCap) & 0xfffu);
 }
+// Shard of the seed group (query edge ei, vertex x at the plan's first
+// position): splitmix64's finaliser of (ei << 32 | x), modulo the shard
+// count.  Seeds of one group (a grouped plan's run of equal first vertices)
+// share the key, so a group is never split between shards.
+__host__ __device__ __forceinline__ uint32_t seed_shard(uint32_t ei, uint32_t x, uint32_t num_shards) {
+    uint64_t z = ((uint64_t)ei << 32 | x) + 0x9e3779b97f4a7c15ull;
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+    z ^= z >> 31;
+    return (uint32_t)(z % num_shards);
+}
+
 // s_cand entries: vertex id (< 2^27) | offset of the candidate in the
 // generator chunk it came from << 27
 constexpr uint32_t kCandBits = 27;
 constexpr uint32_t kCandMask = (1u << kCandBits) - 1u;
 
+// kMulti = false: one query, plans in constant memory (c_plan), seed table
+// in shared memory.  kMulti = true: the plans of every registered query in
+// global memory (a.plans, one per (query, edge); a.qe of them), seed table
+// searched in global memory, each warp's current plan copied to shared
+// memory when its unit changes plan.
+template <bool kMulti>
 __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
     __shared__ uint32_t s_cand[kDfsWarps][kMaxQV][32];
     __shared__ uint4 s_bn[kDfsWarps][kMaxBN];
     __shared__ uint32_t s_rbs[kDfsWarps][kMaxBN];  // run bit-set slot of each resolved record
     __shared__ uint32_t s_m[kDfsWarps][kMaxQV];
     __shared__ unsigned long long s_tc[kDfsWarps][kMaxQV * 8];
-    __shared__ uint32_t s_pre[kMaxQE + 1];
-    __shared__ uint32_t s_lo[kMaxQE];
+    __shared__ uint32_t s_pre[kMulti ? 1 : kMaxQE + 1];
+    __shared__ uint32_t s_lo[kMulti ? 1 : kMaxQE];
+    __shared__ __align__(16) EdgePlan s_plan[kMulti ? kDfsWarps : 1];
 
     const uint32_t lane = threadIdx.x & 31;
     const uint32_t w = threadIdx.x >> 5;
     const bool self_loops = *(const volatile unsigned int*)a.self_seen != 0;
-    if (threadIdx.x <= a.qe) s_pre[threadIdx.x] = a.seed_pre[threadIdx.x];
-    if (threadIdx.x < a.qe) s_lo[threadIdx.x] = a.seed_lo[threadIdx.x];
+    // launch tag of the task ring: a kernel argument, or (in a replayed CUDA
+    // graph, whose arguments are fixed) a device word bumped before the launch
+    const uint32_t epoch = a.epoch_ptr ? *(const volatile unsigned int*)a.epoch_ptr : a.epoch;
+    if (!kMulti) {
+        if (threadIdx.x <= a.qe) s_pre[threadIdx.x] = a.seed_pre[threadIdx.x];
+        if (threadIdx.x < a.qe) s_lo[threadIdx.x] = a.seed_lo[threadIdx.x];
+    }
     __syncthreads();
-    // seeds of this shard: global seed i = shard + local * num_shards
-    const uint32_t all_seeds = s_pre[a.qe];
-    const uint32_t total = all_seeds > a.shard ? (all_seeds - a.shard + a.num_shards - 1) / a.num_shards : 0;
+    auto pre_at = [&](uint32_t e) -> uint32_t { return kMulti ? __ldg(a.seed_pre + e) : s_pre[e]; };
+    auto lo_at = [&](uint32_t e) -> uint32_t { return kMulti ? __ldg(a.seed_lo + e) : s_lo[e]; };
+    auto grouped_at = [&](uint32_t e) -> bool { return kMulti ? a.plans[e].grouped != 0 : c_plan[e].grouped != 0; };
+    int plan_in_smem = -1;  // kMulti: plan held in s_plan[w]
+    // every engine walks all seeds; a sharded one skips the groups of other shards
+    const uint32_t total = pre_at(a.qe);
     const uint64_t vmask = (1ull << a.B) - 1ull;
     uint32_t* m = s_m[w];
     uint4* bn = s_bn[w];
@@ -874,7 +1145,7 @@ __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
                 // no seed left: hold one ticket of the task ring and wait for its task
                 if (ticket == kNoTicket) ticket = atomicAdd((unsigned int*)&a.qctr[1], 1u);
                 const volatile uint32_t* tk = a.tasks + (size_t)(ticket & (a.task_cap - 1u)) * kTaskWords;
-                if (tk[3] == task_tag(a.epoch, ticket)) {
+                if (tk[3] == task_tag(epoch, ticket)) {
                     kind = 2;
                     item = ticket;
                     ticket = kNoTicket;
@@ -903,22 +1174,36 @@ __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
         int ei = 0;
         uint32_t jbase = 2, tgen = 0, tlo = 0, thi = 0;
         if (kind == 1) {
-            item = a.shard + item * a.num_shards;
-            while (ei + 1 < (int)a.qe && s_pre[ei + 1] <= item) ++ei;
-            const uint64_t key = a.dkeys[s_lo[ei] + (item - s_pre[ei])];
+            if (kMulti) {
+                // last plan whose seeds start at or before item (empty plans skipped)
+                uint32_t lo = 0, hi = a.qe;
+                while (hi - lo > 1) {
+                    const uint32_t mid = (lo + hi) >> 1;
+                    if (pre_at(mid) <= item) lo = mid; else hi = mid;
+                }
+                ei = (int)lo;
+            } else {
+                while (ei + 1 < (int)a.qe && s_pre[ei + 1] <= item) ++ei;
+            }
+            const uint32_t e_pre = pre_at(ei), e_lo = lo_at(ei);
+            const uint64_t key = a.dkeys[e_lo + (item - e_pre)];
             ++n_seeds;
-            if (c_plan[ei].grouped && item > s_pre[ei]) {
+            if (grouped_at(ei) && item > e_pre) {
                 // a grouped edge runs one DFS per first vertex: only the first
                 // seed of each run of equal first vertices starts one
-                const uint64_t prev = a.dkeys[s_lo[ei] + (item - s_pre[ei]) - 1];
+                const uint64_t prev = a.dkeys[e_lo + (item - e_pre) - 1];
                 if (((prev ^ key) >> a.B & vmask) == 0) {
                     if (lane == 0) add_release((unsigned int*)&a.qctr[3], 1u);
                     continue;
                 }
             }
+            if (a.num_shards > 1 && seed_shard((uint32_t)ei, (uint32_t)((key >> a.B) & vmask), a.num_shards) != a.shard) {
+                if (lane == 0) add_release((unsigned int*)&a.qctr[3], 1u);
+                continue;
+            }
             if (lane == 0) {
                 m[0] = (uint32_t)((key >> a.B) & vmask);
-                m[1] = c_plan[ei].grouped ? kNoVertex : (uint32_t)(key & vmask);
+                m[1] = grouped_at(ei) ? kNoVertex : (uint32_t)(key & vmask);
                 n_bytes += 8;
             }
         } else {
@@ -927,9 +1212,9 @@ __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
             __threadfence();
             const uint32_t wv = lane < kTaskWords ? tk[lane] : 0;
             const uint32_t w0 = __shfl_sync(kFull, wv, 0);
-            ei = (int)(w0 & 0xffu);
-            jbase = (w0 >> 8) & 0xffu;
-            tgen = (w0 >> 16) & 0xffu;
+            ei = (int)(w0 & 0xffffu);
+            jbase = (w0 >> 16) & 0xffu;
+            tgen = (w0 >> 24) & 0xffu;
             tlo = __shfl_sync(kFull, wv, 1);
             thi = __shfl_sync(kFull, wv, 2);
             if (lane >= 4 && lane < 4 + kMaxQV) m[lane - 4] = wv;
@@ -942,7 +1227,15 @@ __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
             cnt = 0;
             cur_ei = ei;
         }
-        const EdgePlan& P = c_plan[ei];
+        if (kMulti && plan_in_smem != ei) {
+            const uint32_t* src = reinterpret_cast<const uint32_t*>(a.plans + ei);
+            uint32_t* dst = reinterpret_cast<uint32_t*>(&s_plan[w]);
+            for (uint32_t t = lane; t < sizeof(EdgePlan) / 4; t += 32) dst[t] = __ldg(src + t);
+            __syncwarp();
+            plan_in_smem = ei;
+        }
+        const EdgePlan& P = kMulti ? s_plan[w] : c_plan[ei];
+        const bool tail_cache = a.tail_cache && !(P.flags & cgb::kPlanNoTailCache);
         const uint32_t nc = P.n_core;
         const bool has_tail = nc < P.n;
         SeedGroup X{nullptr, 0u, kNoVertex};
@@ -1069,14 +1362,14 @@ __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
                             const uint32_t gd = __shfl_sync(kFull, st_gen, d);
                             uint32_t* tk = a.tasks + (size_t)(slot & (a.task_cap - 1u)) * kTaskWords;
                             uint32_t v = 0;
-                            if (lane == 0) v = (uint32_t)ei | (d << 8) | (gd << 16);
+                            if (lane == 0) v = (uint32_t)ei | (d << 16) | (gd << 24);
                             else if (lane == 1) v = lo;
                             else if (lane == 2) v = hi;
                             else if (lane >= 4 && lane < 4 + kMaxQV) v = (lane - 4 < d) ? m[lane - 4] : 0u;
                             if (lane < kTaskWords && lane != 3) tk[lane] = v;
                             __threadfence();
                             __syncwarp();
-                            if (lane == 0) *(volatile uint32_t*)(tk + 3) = task_tag(a.epoch, slot);
+                            if (lane == 0) *(volatile uint32_t*)(tk + 3) = task_tag(epoch, slot);
                             if (lane == d) {
                                 if (d == j) st_len = gnext + 32u;
                                 else { st_len = st_next; st_ncand = st_pos; }
@@ -1127,7 +1420,7 @@ __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
                     // multiplicity of its hit-position vertices
                     const uint32_t hs = P.grouped ? __shfl_sync(kFull, st_hs, j) : 0u;
                     const bool hit_last = P.grouped && ((P.hit_mask >> j) & 1u);
-                    if (has_tail && P.tail_const && a.tail_cache) {
+                    if (has_tail && P.tail_const && tail_cache) {
                         // the tail count depends on the prefix only: one value per prefix
                         const uint32_t bal = __ballot_sync(kFull, ok);
                         if (bal) {
@@ -1143,7 +1436,7 @@ __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
                             }
                             if (lane == 0) { cnt += wsum * tail_const; n_tail += __popc(bal); }
                         }
-                    } else if (has_tail && P.tail_lane && a.tail_cache && !hit_last) {
+                    } else if (has_tail && P.tail_lane && tail_cache && !hit_last) {
                         // the tail depends on the candidate only through prefix-only
                         // lists: every lane counts its own candidate's tail
                         const uint32_t bal = __ballot_sync(kFull, ok);
@@ -1164,7 +1457,7 @@ __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
                             const int l = __ffs(bal) - 1;
                             bal &= bal - 1;
                             const uint32_t cl = __shfl_sync(kFull, c, l);
-                            if (dirty <= P.tail_dep && a.tail_cache) {
+                            if (dirty <= P.tail_dep && tail_cache) {
                                 // first embedding since the prefix changed: recount the stale prefix-only subsets
                                 tail_prepare(P, m, bn, s_tc[w], dirty, a.rec, a.dvcap, a.pool, a.dval, self_loops, lane, n_bytes, rb);
                             }
@@ -1172,7 +1465,7 @@ __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
                             if (lane == 0) m[j] = cl;
                             __syncwarp();
                             const unsigned long long tc =
-                                a.tail_cache
+                                tail_cache
                                     ? tail_eval(P, m, bn, s_tc[w], a.rec, a.dvcap, a.pool, a.dval, self_loops, lane,
                                                 n_bytes, rb)
                                     : tail_count_warp(P, m, bn, a.rec, a.dvcap, a.pool, a.dval, self_loops, lane,
@@ -1401,6 +1694,8 @@ struct cgb_handle {
     uint64_t* d_edits = nullptr; uint64_t* d_edits_alt = nullptr; size_t edits_cap = 0;
     uint32_t* d_du = nullptr; uint32_t* d_run_du = nullptr; uint32_t* d_run_len = nullptr;
     uint32_t* d_run_off = nullptr; size_t runs_cap = 0;
+    uint32_t* d_small_runs = nullptr; uint32_t* d_big_runs = nullptr;  // merge lists (k_merge_classify)
+    unsigned int* d_list_ctr = nullptr;  // [0] small, [1] big
     int* d_num_runs = nullptr;
     uint64_t* d_dkeys = nullptr; uint64_t* d_dkeys_alt = nullptr; size_t dkeys_cap = 0;
     uint32_t* d_dval = nullptr;
@@ -1415,13 +1710,26 @@ struct cgb_handle {
     unsigned long long last_stats[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     void* d_temp = nullptr; size_t temp_cap = 0;
 
-    // run bit sets (per batch)
+    // run bit sets: built in full on the first matched batch (and after the
+    // record table grows), then kept current by every merge
     uint32_t* d_rb_slot = nullptr; size_t rb_slot_cap = 0;  // [nd][dvcap]
     uint32_t* d_rb_sel = nullptr; size_t rb_sel_cap = 0;
     uint32_t* d_rb_bits = nullptr; size_t rb_bits_cap = 0;
-    unsigned int* d_rb_ctr = nullptr;
-    uint32_t rb_words = 0;
+    uint32_t* d_rb_new = nullptr; size_t rb_new_cap = 0;    // slots claimed by the last merge
+    unsigned int* d_rb_ctr = nullptr;  // [0] slots claimed, [1] claimed by the last merge
+    uint32_t rb_words = 0;             // words per bit set: (dvcap + 31) / 32
+    uint32_t rb_cap = 0;               // bit sets the budget holds
+    bool rb_valid = false;             // slot table and bit sets match the index
     uint32_t rb_min_len = kRunBitsMinLen;
+    uint8_t* d_rev = nullptr;          // reverse direction of each direction
+
+    // label-keyed mode (the multi-query engine's data-graph index): the
+    // "direction" of a key is the label of its target vertex, the delta keys
+    // carry the source vertex's label (lb bits) between direction and source
+    bool mq = false;
+    uint32_t lb = 0;
+    uint8_t* d_vlabel = nullptr;       // [dv] vertex labels
+    unsigned int* d_epoch = nullptr;   // DFS launch tag read by replayed graphs
 
     // valid bits
     uint32_t vb_start[2] = {0, 0};   // starting edge (SelectStartingEdge)
@@ -1503,6 +1811,7 @@ cgb_status ensure_dvcap(cgb_handle* h, uint32_t dv) {
     }
     h->rec = nr;
     h->dvcap = nc;
+    h->rb_valid = false;  // the slot table and the bit sets follow the record layout
     return CGB_OK;
 }
 
@@ -1608,8 +1917,11 @@ cgb_status ensure_edit_buffers(cgb_handle* h, uint64_t n) {
     if (n <= h->edits_cap && h->d_edits) return CGB_OK;
     size_t nc = std::max<size_t>(n + n / 2, 1 << 16);
     CK(cudaStreamSynchronize(h->stream));
-    void* olds[] = {h->d_edits, h->d_edits_alt, h->d_du, h->d_run_du, h->d_run_len, h->d_run_off};
+    void* olds[] = {h->d_edits, h->d_edits_alt, h->d_du, h->d_run_du, h->d_run_len, h->d_run_off,
+                    h->d_small_runs, h->d_big_runs};
     for (void* p : olds) if (p) CK(cudaFree(p));
+    CK(cudaMalloc(&h->d_small_runs, nc * sizeof(uint32_t)));
+    CK(cudaMalloc(&h->d_big_runs, nc * sizeof(uint32_t)));
     CK(cudaMalloc(&h->d_edits, nc * sizeof(uint64_t)));
     CK(cudaMalloc(&h->d_edits_alt, nc * sizeof(uint64_t)));
     CK(cudaMalloc(&h->d_du, nc * sizeof(uint32_t)));
@@ -1647,7 +1959,7 @@ cgb_status apply_edits(cgb_handle* h, const uint64_t* adds0, uint64_t n0, const 
     cgb_status s;
     if ((s = reserve_pool(h, n)) != CGB_OK) return s;
     if ((s = ensure_edit_buffers(h, n)) != CGB_OK) return s;
-    PackInfo pi{bits_for(h->dv), h->nd, h->dv};
+    PackInfo pi{bits_for(h->dv), h->nd, h->dv, h->mq ? 1u : 0u};
     unsigned int* d_err = (unsigned int*)(h->d_scal + 2);
     if (n0) { k_pack_edits<<<grid_for(h, n0), 256, 0, h->stream>>>(adds0, n0, 0, pi, h->d_edits, d_err, h->d_self); LAUNCHED(); }
     if (n1) { k_pack_edits<<<grid_for(h, n1), 256, 0, h->stream>>>(adds1, n1, 0, pi, h->d_edits + n0, d_err, h->d_self); LAUNCHED(); }
@@ -1670,13 +1982,70 @@ cgb_status apply_edits(cgb_handle* h, const uint64_t* adds0, uint64_t n0, const 
     ma.run_len = h->d_run_len;
     ma.run_off = h->d_run_off;
     ma.num_runs = h->d_num_runs;
+    ma.small_runs = h->d_small_runs;
+    ma.big_runs = h->d_big_runs;
+    ma.list_ctr = h->d_list_ctr;
     ma.B = pi.B;
     ma.err = d_err;
     ma.stats = h->d_stats;
+    // bit sets are kept current by the merge once built (k_rb_fill_new, k_rb_edits)
+    const bool rb = h->rb_valid && !(h->cfg.flags & CGB_FLAG_NO_RUN_BITS);
+    ma.rb_slot = rb ? h->d_rb_slot : nullptr;
+    ma.rb_sel = h->d_rb_sel;
+    ma.rb_ctr = h->d_rb_ctr;
+    ma.rb_new = h->d_rb_new;
+    ma.rb_cap = h->rb_cap;
+    ma.rb_min_len = h->rb_min_len;
+    if (rb) {
+        if ((s = grow(h, h->d_rb_new, h->rb_new_cap, std::max<size_t>(h->rb_cap, 1))) != CGB_OK) return s;
+        ma.rb_new = h->d_rb_new;
+        CK(cudaMemsetAsync(h->d_rb_ctr + 1, 0, sizeof(unsigned int), h->stream));
+    }
+    CK(cudaMemsetAsync(h->d_list_ctr, 0, 2 * sizeof(unsigned int), h->stream));
+    k_merge_classify<<<grid_for(h, n), 256, 0, h->stream>>>(ma);
+    LAUNCHED();
     const int mg = std::max(1, std::min<int>((int)((n * 32 + 255) / 256), h->num_sms * 16));
     k_merge_runs<<<mg, 256, 0, h->stream>>>(ma);
     LAUNCHED();
+    // hub runs: one CTA each (at most n / kBigRun of them)
+    const int bg = (int)std::max<uint64_t>(1, std::min<uint64_t>(n / kBigRun + 1, (uint64_t)h->num_sms * 2));
+    k_merge_big<<<bg, kMergeWarps * 32, 0, h->stream>>>(ma);
+    LAUNCHED();
+    if (rb) {
+        k_rb_fill_new<<<h->num_sms * 4, 256, 0, h->stream>>>(h->rec, h->dvcap, h->pool, h->d_rb_sel, h->d_rb_new,
+                                                           h->d_rb_ctr, h->d_rb_bits, h->rb_words);
+        LAUNCHED();
+        k_rb_edits<<<grid_for(h, n), 256, 0, h->stream>>>(h->d_edits, n, pi.B, h->dvcap, h->d_rb_slot,
+                                                           h->d_rb_bits, h->rb_words);
+        LAUNCHED();
+    }
     CK(cudaGetLastError());
+    return CGB_OK;
+}
+
+// Builds the run bit sets in full: a slot for every run of at least
+// rb_min_len entries while the budget lasts (later merges keep them current).
+cgb_status rebuild_run_bits(cgb_handle* h) {
+    cgb_status s;
+    h->rb_words = (h->dvcap + 31) / 32;
+    // as many bit sets as the budget holds, never more than records exist
+    h->rb_cap = (uint32_t)std::min<size_t>(kRunBitsBytes / 4 / std::max(h->rb_words, 1u),
+                                           std::max<size_t>((size_t)h->nd * h->dvcap, 1));
+    const uint32_t cap = h->rb_cap;
+    if ((s = grow(h, h->d_rb_slot, h->rb_slot_cap, (size_t)h->nd * h->dvcap)) != CGB_OK) return s;
+    if ((s = grow(h, h->d_rb_sel, h->rb_sel_cap, (size_t)cap)) != CGB_OK) return s;
+    if ((s = grow(h, h->d_rb_bits, h->rb_bits_cap, (size_t)cap * h->rb_words)) != CGB_OK) return s;
+    CK(cudaMemsetAsync(h->d_rb_ctr, 0, 2 * sizeof(unsigned int), h->stream));
+    k_rb_select<<<grid_for(h, (uint64_t)h->nd * h->dvcap), 256, 0, h->stream>>>(
+        h->rec, h->dvcap, h->nd, h->rb_min_len, cap, h->d_rb_slot, h->d_rb_sel, h->d_rb_ctr);
+    LAUNCHED();
+    k_rb_zero<<<h->num_sms * 8, 256, 0, h->stream>>>(h->d_rb_bits, h->rb_words, cap, h->d_rb_ctr);
+    LAUNCHED();
+    k_rb_fill<<<h->num_sms * 8, 256, 0, h->stream>>>(h->rec, h->dvcap, h->pool, h->d_rb_sel, cap, h->d_rb_ctr,
+                                                     h->d_rb_bits, h->rb_words);
+    LAUNCHED();
+    CK(cudaGetLastError());
+    h->rb_valid = true;
     return CGB_OK;
 }
 
@@ -1686,7 +2055,10 @@ cgb_status sync_scalars(cgb_handle* h) {
                        h->stream));
     CK(cudaMemcpyAsync(h->h_scal + 4 + kMaxQE, h->d_stats, 8 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
                        h->stream));
+    CK(cudaMemcpyAsync(h->h_scal + 12 + kMaxQE, h->d_rb_ctr, sizeof(unsigned int), cudaMemcpyDeviceToHost, h->stream));
     CK(cudaStreamSynchronize(h->stream));
+    // every slot claimed: rebuild on the next batch, so today's long runs get them
+    if (h->rb_valid && (uint32_t)h->h_scal[12 + kMaxQE] >= h->rb_cap) h->rb_valid = false;
     h->h_pool_top = h->h_scal[0];
     h->h_live = (long long)h->h_scal[1];
     return CGB_OK;
@@ -1733,8 +2105,12 @@ cgb_status cgb_create(const cgb_config* cfg, cgb_handle** out) {
     CKC(cudaMemset(h->d_scal, 0, 4 * sizeof(unsigned long long)));
     CKC(cudaMalloc(&h->d_self, sizeof(unsigned int)));
     CKC(cudaMemset(h->d_self, 0, sizeof(unsigned int)));
-    CKC(cudaMallocHost(&h->h_scal, (12 + kMaxQE) * sizeof(unsigned long long)));
+    CKC(cudaMallocHost(&h->h_scal, (16 + kMaxQE) * sizeof(unsigned long long)));
     CKC(cudaMalloc(&h->d_num_runs, 2 * sizeof(int)));
+    CKC(cudaMalloc(&h->d_list_ctr, 2 * sizeof(unsigned int)));
+    CKC(cudaMalloc(&h->d_rb_ctr, 2 * sizeof(unsigned int)));
+    CKC(cudaMemset(h->d_rb_ctr, 0, 2 * sizeof(unsigned int)));
+    CKC(cudaMalloc(&h->d_rev, kMaxDir));
     CKC(cudaMalloc(&h->d_seed, (3 * kMaxQE + 2) * sizeof(uint32_t)));
     CKC(cudaMalloc(&h->d_counts, kMaxQE * sizeof(unsigned long long)));
     CKC(cudaMalloc(&h->d_stats, 8 * sizeof(unsigned long long)));
@@ -1757,7 +2133,8 @@ void cgb_destroy(cgb_handle* h) {
                     h->d_edits_alt, h->d_du, h->d_run_du, h->d_run_len, h->d_run_off, h->d_num_runs,
                     h->d_dkeys, h->d_dkeys_alt, h->d_dval, h->d_ddu, h->d_drun_du, h->d_drun_len, h->d_drun_off,
                     h->d_seed, h->d_counts, h->d_stats, h->d_tasks, h->d_qctr, h->d_temp, h->d_qe_dirs, h->d_edge_ok,
-                    h->d_vb, h->d_rb_slot, h->d_rb_sel, h->d_rb_bits, h->d_rb_ctr};
+                    h->d_vb, h->d_rb_slot, h->d_rb_sel, h->d_rb_bits, h->d_rb_ctr, h->d_rb_new, h->d_small_runs,
+                    h->d_big_runs, h->d_list_ctr, h->d_rev};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (h->h_scal) cudaFreeHost(h->h_scal);
@@ -1779,6 +2156,10 @@ cgb_status cgb_load_query(cgb_handle* h, uint32_t qv, const uint32_t* labels, ui
     for (uint32_t i = 0; i < h->q.qe; ++i) { dirs[2 * i] = h->q.qe_dir[i][0]; dirs[2 * i + 1] = h->q.qe_dir[i][1]; }
     CK(cudaSetDevice(h->device));
     CK(cudaMemcpy(h->d_qe_dirs, dirs, 2 * h->q.qe, cudaMemcpyHostToDevice));
+    uint8_t rev[kMaxDir];
+    std::memset(rev, 255, sizeof(rev));
+    for (uint32_t d = 0; d < h->q.nd; ++d) rev[d] = h->q.eidx[h->q.dir_dst[d] * kMaxQV + h->q.dir_src[d]];
+    CK(cudaMemcpy(h->d_rev, rev, kMaxDir, cudaMemcpyHostToDevice));
     h->have_query = true;
     return CGB_OK;
 }
@@ -1940,28 +2321,12 @@ cgb_status cgb_apply_batch_device(cgb_handle* h, uint32_t dv_count, const uint64
         }
         CK(cudaEventRecord(h->ev[2], h->stream));
 
-        // 2c. bit sets of the long old runs (this batch's index)
+        // 2c. bit sets of the long old runs (this batch's index): built in full
+        // once (and after the record table grows), since then kept current by
+        // every merge; rebuilt when the slots ran out so that the longest runs
+        // of today's index hold them
         const bool rb_on = !(h->cfg.flags & CGB_FLAG_NO_RUN_BITS);
-        if (rb_on) {
-            h->rb_words = (h->dv + 31) / 32;
-            // as many bit sets as the budget holds, never more than runs exist
-            const uint32_t cap = (uint32_t)std::min<size_t>(kRunBitsBytes / 4 / std::max(h->rb_words, 1u),
-                                                            std::max<size_t>((size_t)h->nd * h->dv, 1));
-            if ((s = grow(h, h->d_rb_slot, h->rb_slot_cap, (size_t)h->nd * h->dvcap)) != CGB_OK) return s;
-            if ((s = grow(h, h->d_rb_sel, h->rb_sel_cap, (size_t)cap)) != CGB_OK) return s;
-            if ((s = grow(h, h->d_rb_bits, h->rb_bits_cap, (size_t)cap * h->rb_words)) != CGB_OK) return s;
-            if (!h->d_rb_ctr) CK(cudaMalloc(&h->d_rb_ctr, sizeof(unsigned int)));
-            CK(cudaMemsetAsync(h->d_rb_ctr, 0, sizeof(unsigned int), h->stream));
-            k_rb_select<<<grid_for(h, (uint64_t)h->nd * h->dv), 256, 0, h->stream>>>(
-                h->rec, h->dvcap, h->dv, h->nd, h->rb_min_len, cap, h->d_rb_slot, h->d_rb_sel, h->d_rb_ctr);
-            LAUNCHED();
-            k_rb_zero<<<h->num_sms * 8, 256, 0, h->stream>>>(h->d_rb_bits, h->rb_words, cap, h->d_rb_ctr);
-            LAUNCHED();
-            k_rb_fill<<<h->num_sms * 8, 256, 0, h->stream>>>(h->rec, h->dvcap, h->pool, h->d_rb_sel, cap, h->d_rb_ctr,
-                                                             h->d_rb_bits, h->rb_words);
-            LAUNCHED();
-            CK(cudaGetLastError());
-        }
+        if (rb_on && !h->rb_valid && (s = rebuild_run_bits(h)) != CGB_OK) return s;
 
         // 3. matching
         DfsArgs da;
@@ -1997,17 +2362,19 @@ cgb_status cgb_apply_batch_device(cgb_handle* h, uint32_t dv_count, const uint64
         da.rb_slot = rb_on ? h->d_rb_slot : nullptr;
         da.rb_bits = h->d_rb_bits;
         da.rb_words = h->rb_words;
+        da.plans = nullptr;
+        da.epoch_ptr = nullptr;
         da.budget_ns = h->cfg.dfs_budget_ms ? (unsigned long long)h->cfg.dfs_budget_ms * 1000000ull
                                             : 600ull * 1000000000ull;
         // persistent grid: exactly the blocks that can be resident at once
         if (h->dfs_occupancy == 0) {
             int occ = 0;
-            CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_dfs_count, kDfsWarps * 32, 0));
+            CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_dfs_count<false>, kDfsWarps * 32, 0));
             h->dfs_occupancy = std::max(occ, 1);
         }
         int bps = h->dfs_occupancy;
         if (h->cfg.dfs_blocks_per_sm) bps = std::min(bps, (int)h->cfg.dfs_blocks_per_sm);
-        k_dfs_count<<<h->num_sms * bps, kDfsWarps * 32, 0, h->stream>>>(da);
+        k_dfs_count<false><<<h->num_sms * bps, kDfsWarps * 32, 0, h->stream>>>(da);
         LAUNCHED();
         CK(cudaGetLastError());
         CK(cudaEventRecord(h->ev[3], h->stream));
@@ -2036,6 +2403,7 @@ cgb_status cgb_apply_batch_device(cgb_handle* h, uint32_t dv_count, const uint64
     for (int i = 0; i < 8; ++i) h->last_stats[i] = h->h_scal[4 + kMaxQE + i];
     if (h->h_scal[2]) {
         h->n_pending = 0;
+        h->rb_valid = false;  // a rejected batch may have left runs and bit sets apart
         cgb_status st = (h->h_scal[2] & 24u) ? CGB_ERR_TIMEOUT : (h->h_scal[2] & 4u) ? CGB_ERR_OOM : CGB_ERR_ARG;
         return fail(h, st,
                     "batch rejected: error bits %llu (1/2 = key out of range, 4 = pool exhausted, "
@@ -2093,6 +2461,39 @@ cgb_status cgb_last_stats(const cgb_handle* h, uint64_t* out8) {
 }
 
 void* cgb_stream(const cgb_handle* h) { return h ? (void*)h->stream : nullptr; }
+
+cgb_status cgb_plan_anchor(const cgb_handle* h, uint32_t ei, uint32_t* qvertex) {
+    if (!h || !qvertex) return CGB_ERR_ARG;
+    if (!h->have_index) return CGB_ERR_STATE;
+    if (ei >= h->q.qe) return CGB_ERR_ARG;
+    *qvertex = h->plans[ei].vs[0];
+    return CGB_OK;
+}
+
+cgb_status cgb_check_symmetry(cgb_handle* h, uint64_t* n_asym) {
+    if (!h || !n_asym) return CGB_ERR_ARG;
+    *n_asym = 0;
+    if (!h->have_index) return fail(h, CGB_ERR_STATE, "no index");
+    CK(cudaSetDevice(h->device));
+    cgb_status s;
+    if ((s = flush_pending(h)) != CGB_OK) return s;
+    unsigned long long* d_bad = nullptr;
+    CK(cudaMalloc(&d_bad, sizeof(unsigned long long)));
+    CK(cudaMemsetAsync(d_bad, 0, sizeof(unsigned long long), h->stream));
+    const uint64_t n = (uint64_t)h->nd * h->dv;
+    if (n) {
+        k_asymmetry<<<grid_for(h, n * 32), 256, 0, h->stream>>>(h->rec, h->dvcap, h->dv, h->nd, h->pool, h->d_rev, d_bad);
+        LAUNCHED();
+    }
+    unsigned long long bad = 0;
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&bad, d_bad, sizeof(bad), cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    cudaFree(d_bad);
+    CK(e);
+    *n_asym = bad;
+    return CGB_OK;
+}
 
 cgb_status cgb_starting_edge(const cgb_handle* h, uint32_t* out2) {
     if (!h || !out2) return CGB_ERR_ARG;
@@ -2164,3 +2565,5 @@ cgb_status cgb_read_index(cgb_handle* h, uint64_t* out, uint64_t cap, uint64_t* 
 }
 
 }  // extern "C"
+
+#include "multiquery.cuh"

@@ -205,28 +205,21 @@ int write_graph(const char* path, const Workload& W, const std::vector<uint64_t>
     return 0;
 }
 
-}  // namespace
-
-extern "C" {
-
-// Generates a data graph + insertion stream + one query.
-//   kind: 0 = Erdos-Renyi (uniform pairs), 1 = R-MAT(a, b, c, 1-a-b-c)
-//   zipf_s <= 0: uniform labels, else P(k) ~ (k+1)^-zipf_s over num_labels
-//   holdout edges are chosen uniformly (seed_holdout) and written in shuffled order
-//   qshape: 0 = dense, 1 = sparse, 2 = tree; qsize vertices; queries sampled from
-//   the final graph; resampled until the query has <= max_qedges edges.
-// Returns 0 on success, <0 on failure; *out_qedges receives the query edge count.
-int cgbgen_workload(const char* graph_path, const char* update_path, const char* query_path,
-                    int kind, uint32_t n, uint64_t m, double a, double b, double c,
-                    uint32_t num_labels, double zipf_s, uint64_t holdout,
-                    uint64_t seed_graph, uint64_t seed_labels, uint64_t seed_holdout,
-                    int qshape, uint32_t qsize, uint32_t max_qedges, uint64_t seed_query,
-                    uint32_t* out_qedges) {
-    const bool query_only = graph_path == nullptr;  // graph/stream already written
+// Graph, labels and the held-out stream of one workload (the stream in its
+// shuffled order with the orientation the update file is written in).
+struct Generated {
     Workload W;
+    std::vector<uint64_t> initial;  // (min << 32) | max
+    std::vector<std::pair<uint32_t, uint32_t>> stream;
+    Adj final_adj;                  // initial + stream, for query sampling
+};
+
+void generate(Generated& G, int kind, uint32_t n, uint64_t m, double a, double b, double c, uint32_t num_labels,
+              double zipf_s, uint64_t holdout, uint64_t seed_graph, uint64_t seed_labels, uint64_t seed_holdout,
+              bool want_adj) {
+    Workload& W = G.W;
     gen_edges(W, n, m, kind, a, b, c, seed_graph);
     gen_labels(W, num_labels, zipf_s, seed_labels);
-
     // holdout: random subset, re-inserted in shuffled order
     std::vector<uint32_t> perm(W.edges.size());
     for (uint32_t i = 0; i < perm.size(); ++i) perm[i] = i;
@@ -237,28 +230,28 @@ int cgbgen_workload(const char* graph_path, const char* update_path, const char*
     std::vector<uint64_t> stream;
     stream.reserve(holdout);
     for (uint64_t i = 0; i < holdout; ++i) { held[perm[i]] = 1; stream.push_back(W.edges[perm[i]]); }
-    std::vector<uint64_t> initial;
-    initial.reserve(W.edges.size() - holdout);
+    G.initial.clear();
+    G.initial.reserve(W.edges.size() - holdout);
     for (size_t i = 0; i < W.edges.size(); ++i)
-        if (!held[i]) initial.push_back(W.edges[i]);
-
-    if (!query_only && write_graph(graph_path, W, initial) != 0) return -1;
-    if (!query_only) {
-        FILE* f = std::fopen(update_path, "w");
-        if (!f) return -2;
-        std::vector<char> buf(1 << 22);
-        std::setvbuf(f, buf.data(), _IOFBF, buf.size());
-        std::mt19937_64 dr(seed_holdout ^ 0x5bd1e995ull);
-        for (uint64_t e : stream) {
-            uint32_t x = (uint32_t)(e >> 32), y = (uint32_t)e;
-            if (dr() & 1) std::swap(x, y);  // random orientation, as an edge stream would have
-            std::fprintf(f, "e %u %u 0\n", x, y);
-        }
-        std::fclose(f);
+        if (!held[i]) G.initial.push_back(W.edges[i]);
+    std::mt19937_64 dr(seed_holdout ^ 0x5bd1e995ull);
+    G.stream.clear();
+    G.stream.reserve(stream.size());
+    for (uint64_t e : stream) {
+        uint32_t x = (uint32_t)(e >> 32), y = (uint32_t)e;
+        if (dr() & 1) std::swap(x, y);  // random orientation, as an edge stream would have
+        G.stream.emplace_back(x, y);
     }
+    if (want_adj) G.final_adj = build_adj(W.n, W.edges);
+}
 
-    // query from the final graph
-    Adj A = build_adj(W.n, W.edges);
+// Samples one query pattern from the final graph (see cgbgen_workload for the
+// shape rules).  Returns 0 and the pattern's vertices' data ids / local edges,
+// or < 0.
+int sample_query(const Generated& G, int qshape, uint32_t qsize, uint32_t max_qedges, uint64_t seed_query,
+                 std::vector<uint32_t>& out_vs, std::vector<std::pair<uint32_t, uint32_t>>& out_qe) {
+    const Workload& W = G.W;
+    const Adj& A = G.final_adj;
     std::mt19937_64 qr(seed_query);
     std::uniform_int_distribution<uint32_t> pick(0, W.n - 1);
     std::vector<uint32_t> vs;
@@ -271,12 +264,8 @@ int cgbgen_workload(const char* graph_path, const char* update_path, const char*
     const int budget = 20000;
     auto emit = [&](const std::vector<uint32_t>& V, std::vector<std::pair<uint32_t, uint32_t>> qe) {
         std::sort(qe.begin(), qe.end());
-        FILE* f = std::fopen(query_path, "w");
-        if (!f) return -3;
-        for (uint32_t i = 0; i < V.size(); ++i) std::fprintf(f, "v %u %u\n", i, W.labels[V[i]]);
-        for (auto& [x, y] : qe) std::fprintf(f, "e %u %u 0\n", x, y);
-        std::fclose(f);
-        if (out_qedges) *out_qedges = (uint32_t)qe.size();
+        out_vs = V;
+        out_qe = qe;
         return 0;
     };
     for (int attempt = 0; attempt < budget; ++attempt) {
@@ -315,6 +304,104 @@ int cgbgen_workload(const char* graph_path, const char* update_path, const char*
     }
     if (qshape == 0 && !best_vs.empty()) return emit(best_vs, best_qe);
     return -4;
+}
+
+}  // namespace
+
+extern "C" {
+
+// Generates a data graph + insertion stream + one query.
+//   kind: 0 = Erdos-Renyi (uniform pairs), 1 = R-MAT(a, b, c, 1-a-b-c)
+//   zipf_s <= 0: uniform labels, else P(k) ~ (k+1)^-zipf_s over num_labels
+//   holdout edges are chosen uniformly (seed_holdout) and written in shuffled order
+//   qshape: 0 = dense, 1 = sparse, 2 = tree; qsize vertices; queries sampled from
+//   the final graph; resampled until the query has <= max_qedges edges.
+// Returns 0 on success, <0 on failure; *out_qedges receives the query edge count.
+int cgbgen_workload(const char* graph_path, const char* update_path, const char* query_path,
+                    int kind, uint32_t n, uint64_t m, double a, double b, double c,
+                    uint32_t num_labels, double zipf_s, uint64_t holdout,
+                    uint64_t seed_graph, uint64_t seed_labels, uint64_t seed_holdout,
+                    int qshape, uint32_t qsize, uint32_t max_qedges, uint64_t seed_query,
+                    uint32_t* out_qedges) {
+    const bool query_only = graph_path == nullptr;  // graph/stream already written
+    Generated G;
+    generate(G, kind, n, m, a, b, c, num_labels, zipf_s, holdout, seed_graph, seed_labels, seed_holdout, true);
+    if (!query_only && write_graph(graph_path, G.W, G.initial) != 0) return -1;
+    if (!query_only) {
+        FILE* f = std::fopen(update_path, "w");
+        if (!f) return -2;
+        std::vector<char> buf(1 << 22);
+        std::setvbuf(f, buf.data(), _IOFBF, buf.size());
+        for (auto& [x, y] : G.stream) std::fprintf(f, "e %u %u 0\n", x, y);
+        std::fclose(f);
+    }
+    std::vector<uint32_t> vs;
+    std::vector<std::pair<uint32_t, uint32_t>> qe;
+    const int rc = sample_query(G, qshape, qsize, max_qedges, seed_query, vs, qe);
+    if (rc != 0) return rc;
+    FILE* f = std::fopen(query_path, "w");
+    if (!f) return -3;
+    for (uint32_t i = 0; i < vs.size(); ++i) std::fprintf(f, "v %u %u\n", i, G.W.labels[vs[i]]);
+    for (auto& [x, y] : qe) std::fprintf(f, "e %u %u 0\n", x, y);
+    std::fclose(f);
+    if (out_qedges) *out_qedges = (uint32_t)qe.size();
+    return 0;
+}
+
+// In-memory form of the same workloads: the graph, labels and stream as
+// arrays, and any number of query patterns sampled from one generated graph
+// (query seed s gives the same pattern as cgbgen_workload with seed_query s).
+void* cgbgen_open(int kind, uint32_t n, uint64_t m, double a, double b, double c, uint32_t num_labels,
+                  double zipf_s, uint64_t holdout, uint64_t seed_graph, uint64_t seed_labels,
+                  uint64_t seed_holdout) {
+    Generated* G = new Generated();
+    generate(*G, kind, n, m, a, b, c, num_labels, zipf_s, holdout, seed_graph, seed_labels, seed_holdout, true);
+    return G;
+}
+
+void cgbgen_close(void* h) { delete (Generated*)h; }
+
+// Sizes: out3[0] = vertices, out3[1] = initial edges, out3[2] = stream edges.
+void cgbgen_sizes(void* h, uint64_t* out3) {
+    const Generated* G = (const Generated*)h;
+    out3[0] = G->W.n;
+    out3[1] = G->initial.size();
+    out3[2] = G->stream.size();
+}
+
+// labels[n]; initial[2 * initial edges] as (min, max) pairs in generation
+// order; stream[2 * stream edges] as written to the update file.
+void cgbgen_copy(void* h, uint32_t* labels, uint32_t* initial, uint32_t* stream) {
+    const Generated* G = (const Generated*)h;
+    if (labels) std::memcpy(labels, G->W.labels.data(), G->W.labels.size() * 4);
+    if (initial)
+        for (size_t i = 0; i < G->initial.size(); ++i) {
+            initial[2 * i] = (uint32_t)(G->initial[i] >> 32);
+            initial[2 * i + 1] = (uint32_t)G->initial[i];
+        }
+    if (stream)
+        for (size_t i = 0; i < G->stream.size(); ++i) {
+            stream[2 * i] = G->stream[i].first;
+            stream[2 * i + 1] = G->stream[i].second;
+        }
+}
+
+// One query: labels_out[<= 12], edges_out[2 * <= 66]; *qv, *qe set.
+int cgbgen_query(void* h, int qshape, uint32_t qsize, uint32_t max_qedges, uint64_t seed_query,
+                 uint32_t* labels_out, uint32_t* edges_out, uint32_t* qv, uint32_t* qe) {
+    const Generated* G = (const Generated*)h;
+    std::vector<uint32_t> vs;
+    std::vector<std::pair<uint32_t, uint32_t>> e;
+    const int rc = sample_query(*G, qshape, qsize, max_qedges, seed_query, vs, e);
+    if (rc != 0) return rc;
+    for (uint32_t i = 0; i < vs.size(); ++i) labels_out[i] = G->W.labels[vs[i]];
+    for (size_t i = 0; i < e.size(); ++i) {
+        edges_out[2 * i] = e[i].first;
+        edges_out[2 * i + 1] = e[i].second;
+    }
+    *qv = (uint32_t)vs.size();
+    *qe = (uint32_t)e.size();
+    return 0;
 }
 
 }  // extern "C"

@@ -14,7 +14,8 @@
 //
 // Set-up: the scratch array's device address is obtained once per device with
 // cudaGetSymbolAddress, with that device current, on the first call made on
-// that device; make that first call before any stream capture.
+// that device (and again if that device's context was reset since); make that
+// first call before any stream capture.
 // Sharing: every call uses the same array and it keeps the last call's
 // contents; calls whose work overlaps on the GPU (different streams, or
 // different host threads, on one device) race on it and must be ordered by
@@ -32,6 +33,7 @@ namespace {
 constexpr uint64_t kMaxEdits = CGB_NOALLOC_MAX_EDITS;
 constexpr uint32_t kTile = 2048;           // merged positions per block and step
 constexpr uint32_t kMaxTiles = 1u << 16;   // per-tile counts kept in scratch
+constexpr uint64_t kMaxMerged = (uint64_t)kMaxTiles * kTile;  // old keys + edits per call (2^27)
 constexpr size_t kSortTempBytes = 6u << 20;
 constexpr size_t kScanTempBytes = 1u << 20;
 // layout: [edits A][edits B][sort temp][scan temp][tile counts + 1][error word]
@@ -46,7 +48,6 @@ constexpr size_t kScratchBytes = kOffErr + 256;
 __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
 std::mutex g_mu;
-unsigned char* g_scratch_addr[64] = {};
 
 __device__ __forceinline__ bool unpack_ext(uint64_t k, uint32_t dv, uint32_t& d, uint32_t& u, uint32_t& v) {
     d = (uint32_t)(k >> 59);
@@ -93,18 +94,6 @@ struct Merged {
         }
         return lo;
     }
-    // element k of the merge: value, whether it is a remove, and the next value
-    __device__ void at(uint64_t k, uint64_t& val, bool& rem, bool& last) const {
-        uint64_t i = split(k), j = k - i;
-        const bool fx = i < xl && (j >= yl || xv(i) <= yv(j));
-        if (fx) { val = xv(i); rem = false; ++i; }
-        else { val = yv(j); rem = (Y[j] & 1ull) != 0; ++j; }
-        last = true;
-        if (k + 1 < xl + yl) {
-            const uint64_t nv = (i < xl && (j >= yl || xv(i) <= yv(j))) ? xv(i) : yv(j);
-            last = nv != val;
-        }
-    }
 };
 
 __device__ __forceinline__ uint64_t to_ext(uint64_t p, uint32_t B) {
@@ -112,38 +101,81 @@ __device__ __forceinline__ uint64_t to_ext(uint64_t p, uint32_t B) {
     return ((p >> (2 * B)) << 59) | (((p >> B) & vm) << 32) | (p & vm);
 }
 
-// pass 1: per-tile number of emitted keys; pass 2: write them at scanned offsets
+constexpr uint32_t kThreads = 256;
+constexpr uint32_t kItems = kTile / kThreads;  // merged entries per thread
+constexpr uint64_t kEnd = ~0ull;               // beyond every packed value
+
+// Tiled merge path.  Block b merges the entries [b * kTile, (b + 1) * kTile):
+// two splits per tile (its ends), the tile's part of X and Y staged in
+// shared memory (X converted to the packed order, Y with its op bit), then
+// each thread splits its own kItems entries inside the tile and merges them
+// serially.  An entry is emitted when it is the last of its value group and
+// not a remove.  Pass 1 (kWrite = false) stores each tile's emitted count;
+// pass 2 writes the entries at the scanned tile offsets.
 template <bool kWrite>
-__global__ void k_na_merge(Merged M, uint64_t per_tile, unsigned long long* tile_cnt,
-                           const unsigned long long* tile_off, uint64_t* out) {
-    __shared__ unsigned int s_warp[32];
+__global__ void __launch_bounds__(kThreads) k_na_merge(Merged M, unsigned long long* tile_cnt,
+                                                      const unsigned long long* tile_off, uint64_t* out) {
+    using Scan = cub::BlockScan<uint32_t, kThreads>;
+    __shared__ uint64_t s_e[kTile];    // [0, nx): X (packed), [nx, nx + ny): Y (packed << 1 | op)
+    __shared__ uint64_t s_split[3];    // i0, i1, value of the entry after the tile
+    __shared__ typename Scan::TempStorage s_scan;
     const uint64_t total = M.xl + M.yl;
-    const uint64_t t0 = (uint64_t)blockIdx.x * per_tile;
-    const uint64_t t1 = t0 + per_tile < total ? t0 + per_tile : total;
-    unsigned long long base = kWrite ? tile_off[blockIdx.x] : 0;
-    const uint32_t lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    for (uint64_t k0 = t0; k0 < t1; k0 += blockDim.x) {
-        const uint64_t k = k0 + threadIdx.x;
-        bool emit = false;
-        uint64_t val = 0;
-        if (k < t1) {
-            bool rem, last;
-            M.at(k, val, rem, last);
-            emit = last && !rem && val != (~0ull >> 1);
-        }
-        const unsigned int bal = __ballot_sync(0xffffffffu, emit);
-        if (lane == 0) s_warp[wid] = __popc(bal);
-        __syncthreads();
-        unsigned int before = 0, sum = 0;
-        for (uint32_t w2 = 0; w2 < blockDim.x / 32; ++w2) {
-            if (w2 < wid) before += s_warp[w2];
-            sum += s_warp[w2];
-        }
-        if (kWrite && emit) out[base + before + __popc(bal & ((1u << lane) - 1u))] = to_ext(val, M.B);
-        base += sum;
-        __syncthreads();
+    const uint64_t k0 = (uint64_t)blockIdx.x * kTile;
+    const uint64_t k1 = k0 + kTile < total ? k0 + kTile : total;
+    if (threadIdx.x == 0) s_split[0] = M.split(k0);
+    if (threadIdx.x == 32) {
+        const uint64_t i1 = M.split(k1), j1 = k1 - i1;
+        s_split[1] = i1;
+        uint64_t nxt = kEnd;
+        if (i1 < M.xl) nxt = M.xv(i1);
+        if (j1 < M.yl && M.yv(j1) < nxt) nxt = M.yv(j1);
+        s_split[2] = nxt;
     }
-    if (!kWrite && threadIdx.x == 0) tile_cnt[blockIdx.x] = base;
+    __syncthreads();
+    const uint64_t i0 = s_split[0], i1 = s_split[1];
+    const uint64_t j0 = k0 - i0;
+    const uint32_t nx = (uint32_t)(i1 - i0), nt = (uint32_t)(k1 - k0), ny = nt - nx;
+    for (uint32_t t = threadIdx.x; t < nt; t += kThreads)
+        s_e[t] = t < nx ? M.xv(i0 + t) : M.Y[j0 + (t - nx)];
+    __syncthreads();
+    const uint64_t* sx = s_e;
+    const uint64_t* sy = s_e + nx;
+    // this thread's entries [a0, a1) of the tile
+    const uint32_t a0 = min(threadIdx.x * kItems, nt), a1 = min(a0 + kItems, nt);
+    uint32_t lo = a0 > ny ? a0 - ny : 0, hi = a0 < nx ? a0 : nx;
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (sx[mid] <= (sy[a0 - 1 - mid] >> 1)) lo = mid + 1;
+        else hi = mid;
+    }
+    uint32_t i = lo, j = a0 - lo;
+    uint64_t val[kItems + 1];
+    bool rem[kItems];
+#pragma unroll
+    for (uint32_t q = 0; q <= kItems; ++q) {
+        if (a0 + q < a1 || (q > 0 && a0 + q == a1 && a1 < nt)) {
+            const bool fx = i < nx && (j >= ny || sx[i] <= (sy[j] >> 1));
+            if (fx) { val[q] = sx[i++]; if (q < kItems) rem[q] = false; }
+            else { val[q] = sy[j] >> 1; if (q < kItems) rem[q] = (sy[j] & 1ull) != 0; ++j; }
+        } else {
+            val[q] = (a0 + q == nt) ? s_split[2] : kEnd;
+            if (q < kItems) rem[q] = true;
+        }
+    }
+    uint32_t cnt = 0;
+#pragma unroll
+    for (uint32_t q = 0; q < kItems; ++q)
+        cnt += (a0 + q < a1 && val[q] != val[q + 1] && !rem[q] && val[q] != (~0ull >> 1)) ? 1u : 0u;
+    uint32_t before = 0, all = 0;
+    Scan(s_scan).ExclusiveSum(cnt, before, all);
+    if (!kWrite) {
+        if (threadIdx.x == 0) tile_cnt[blockIdx.x] = all;
+        return;
+    }
+    uint64_t o = tile_off[blockIdx.x] + before;
+#pragma unroll
+    for (uint32_t q = 0; q < kItems; ++q)
+        if (a0 + q < a1 && val[q] != val[q + 1] && !rem[q] && val[q] != (~0ull >> 1)) out[o++] = to_ext(val[q], M.B);
 }
 
 __global__ void k_na_finish(const unsigned long long* tile_off, uint32_t tiles, const unsigned int* err,
@@ -157,6 +189,51 @@ inline uint32_t bits_for(uint32_t dv) {
     return b;
 }
 
+// Device address of the scratch array for the current device and context.
+// The host-side name g_noalloc_scratch is only a stand-in: the address must
+// be asked for with cudaGetSymbolAddress, with the device current.  It is
+// looked up again when the device's context changes (after a
+// cudaDeviceReset), which the driver's context id shows; that check makes no
+// allocation and no stream operation.
+typedef int (*CtxGetCurrentFn)(void**);
+typedef int (*CtxGetIdFn)(void*, unsigned long long*);
+
+bool current_context_id(unsigned long long* id) {
+    static CtxGetCurrentFn get_ctx = nullptr;
+    static CtxGetIdFn get_id = nullptr;
+    static bool looked_up = false;
+    if (!looked_up) {
+        looked_up = true;
+        cudaDriverEntryPointQueryResult q1, q2;
+        void* f1 = nullptr;
+        void* f2 = nullptr;
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &f1, 12000, cudaEnableDefault, &q1) == cudaSuccess &&
+            cudaGetDriverEntryPointByVersion("cuCtxGetId", &f2, 12000, cudaEnableDefault, &q2) == cudaSuccess &&
+            q1 == cudaDriverEntryPointSuccess && q2 == cudaDriverEntryPointSuccess) {
+            get_ctx = (CtxGetCurrentFn)f1;
+            get_id = (CtxGetIdFn)f2;
+        }
+    }
+    void* ctx = nullptr;
+    if (!get_ctx || !get_id || get_ctx(&ctx) != 0 || !ctx) return false;
+    return get_id(ctx, id) == 0;
+}
+
+unsigned char* scratch_address(int dev) {
+    static unsigned char* addr[64] = {};
+    static unsigned long long ctx_id[64] = {};
+    unsigned long long id = 0;
+    const bool have_id = current_context_id(&id);
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (!addr[dev] || (have_id && id != ctx_id[dev])) {
+        void* p = nullptr;
+        if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return nullptr;
+        addr[dev] = (unsigned char*)p;
+        ctx_id[dev] = have_id ? id : 0;
+    }
+    return addr[dev];
+}
+
 }  // namespace
 
 extern "C" cgb_status cgb_merge_keys_noalloc(const uint64_t* old_keys_device, uint64_t n_old,
@@ -166,59 +243,68 @@ extern "C" cgb_status cgb_merge_keys_noalloc(const uint64_t* old_keys_device, ui
     if (!out_device || !out_n_device || (n_old && !old_keys_device) || (n_ins && !ins_device) ||
         (n_del && !del_device))
         return CGB_ERR_ARG;
-    // more edits than the scratch array holds (tested without forming n_ins + n_del, which could wrap)
+    // more edits than the scratch array holds, or more merged keys than its
+    // tile counts cover (tested without forming sums that could wrap)
     if (n_ins > kMaxEdits || n_del > kMaxEdits - n_ins) return CGB_ERR_LIMIT;
+    if (n_old > kMaxMerged - (n_ins + n_del)) return CGB_ERR_LIMIT;
     if (dv_count == 0 || dv_count > CGB_MAX_VID) return CGB_ERR_ARG;
+    // an error left by earlier work on this thread is reported, not cleared
+    if (cudaPeekAtLastError() != cudaSuccess) return CGB_ERR_CUDA;
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return CGB_ERR_CUDA;
-    unsigned char* scratch = nullptr;
-    {
-        std::lock_guard<std::mutex> lk(g_mu);
-        if (!g_scratch_addr[dev]) {
-            // the host-side symbol is only a stand-in: the device address must be asked for
-            void* p = nullptr;
-            if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return CGB_ERR_CUDA;
-            g_scratch_addr[dev] = (unsigned char*)p;
-        }
-        scratch = g_scratch_addr[dev];
-    }
     cudaStream_t st = (cudaStream_t)stream;
+    const uint32_t B = bits_for(dv_count);
+    const uint64_t ne = n_ins + n_del;
+    const uint64_t total = n_old + ne;
+    const uint64_t ntiles = total ? (total + kTile - 1) / kTile : 1;
+    // temporary sizes first (host-only queries): every limit is checked before
+    // any work is enqueued
+    size_t sort_need = 0, scan_need = 0;
+    if (ne) {
+        cub::DoubleBuffer<uint64_t> probe(nullptr, nullptr);
+        if (cub::DeviceRadixSort::SortKeys(nullptr, sort_need, probe, (int64_t)ne, 0, (int)(2 * B + 7), st) !=
+            cudaSuccess)
+            return CGB_ERR_CUDA;
+        if (sort_need > kSortTempBytes) return CGB_ERR_LIMIT;
+    }
+    {
+        unsigned long long* none = nullptr;
+        if (cub::DeviceScan::ExclusiveSum(nullptr, scan_need, none, none, (int64_t)ntiles + 1, st) != cudaSuccess)
+            return CGB_ERR_CUDA;
+        if (scan_need > kScanTempBytes) return CGB_ERR_LIMIT;
+    }
+    unsigned char* scratch = scratch_address(dev);
+    if (!scratch) return CGB_ERR_CUDA;
     uint64_t* A = (uint64_t*)(scratch + kOffA);
     uint64_t* Bf = (uint64_t*)(scratch + kOffB);
     unsigned long long* tiles = (unsigned long long*)(scratch + kOffTiles);
     unsigned int* err = (unsigned int*)(scratch + kOffErr);
-    const uint32_t B = bits_for(dv_count);
-    const uint64_t ne = n_ins + n_del;
     if (cudaMemsetAsync(err, 0, sizeof(unsigned int), st) != cudaSuccess) return CGB_ERR_CUDA;
     if (ne) {
         k_na_pack<<<(int)((ne + 255) / 256 < 4096 ? (ne + 255) / 256 : 4096), 256, 0, st>>>(
             ins_device, n_ins, del_device, n_del, dv_count, B, A, err);
+        if (cudaGetLastError() != cudaSuccess) return CGB_ERR_CUDA;
         cub::DoubleBuffer<uint64_t> db(A, Bf);
-        size_t need = 0;
-        if (cub::DeviceRadixSort::SortKeys(nullptr, need, db, (int64_t)ne, 0, (int)(2 * B + 7), st) != cudaSuccess)
-            return CGB_ERR_CUDA;
-        if (need > kSortTempBytes) return CGB_ERR_LIMIT;
-        if (cub::DeviceRadixSort::SortKeys(scratch + kOffSort, need, db, (int64_t)ne, 0, (int)(2 * B + 7), st) !=
+        if (cub::DeviceRadixSort::SortKeys(scratch + kOffSort, sort_need, db, (int64_t)ne, 0, (int)(2 * B + 7), st) !=
             cudaSuccess)
             return CGB_ERR_CUDA;
         A = db.Current();
     }
-    const uint64_t total = n_old + ne;
-    uint64_t ntiles = (total + kTile - 1) / kTile;
-    if (ntiles == 0) ntiles = 1;
-    if (ntiles > kMaxTiles) ntiles = kMaxTiles;
-    const uint64_t per_tile = (total + ntiles - 1) / ntiles ? (total + ntiles - 1) / ntiles : 1;
     Merged M{old_keys_device, n_old, A, ne, B};
-    k_na_merge<false><<<(unsigned)ntiles, 256, 0, st>>>(M, per_tile, tiles, nullptr, nullptr);
-    size_t scan_need = 0;
-    if (cub::DeviceScan::ExclusiveSum(nullptr, scan_need, tiles, tiles, (int64_t)ntiles + 1, st) != cudaSuccess)
+    if (total) {
+        k_na_merge<false><<<(unsigned)ntiles, kThreads, 0, st>>>(M, tiles, nullptr, nullptr);
+        if (cudaGetLastError() != cudaSuccess) return CGB_ERR_CUDA;
+    } else if (cudaMemsetAsync(tiles, 0, sizeof(unsigned long long), st) != cudaSuccess) {
         return CGB_ERR_CUDA;
-    if (scan_need > kScanTempBytes) return CGB_ERR_LIMIT;
+    }
     if (cudaMemsetAsync(tiles + ntiles, 0, sizeof(unsigned long long), st) != cudaSuccess) return CGB_ERR_CUDA;
     if (cub::DeviceScan::ExclusiveSum(scratch + kOffScan, scan_need, tiles, tiles, (int64_t)ntiles + 1, st) !=
         cudaSuccess)
         return CGB_ERR_CUDA;
-    k_na_merge<true><<<(unsigned)ntiles, 256, 0, st>>>(M, per_tile, nullptr, tiles, out_device);
+    if (total) {
+        k_na_merge<true><<<(unsigned)ntiles, kThreads, 0, st>>>(M, nullptr, tiles, out_device);
+        if (cudaGetLastError() != cudaSuccess) return CGB_ERR_CUDA;
+    }
     k_na_finish<<<1, 1, 0, st>>>(tiles, (uint32_t)ntiles, err, out_n_device);
     return cudaGetLastError() == cudaSuccess ? CGB_OK : CGB_ERR_CUDA;
 }

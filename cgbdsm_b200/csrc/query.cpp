@@ -40,9 +40,12 @@ std::string parse_query_file(const std::string& path, std::vector<uint32_t>& lab
 }
 
 std::string build_query_meta(uint32_t qv, uint32_t qe, const uint32_t* edges, const uint32_t* labels,
-                             QueryMeta& q) {
+                             QueryMeta& q, uint32_t max_qe) {
     if (qv < 2 || qv > (uint32_t)kMaxQV) return "query must have 2..12 vertices";
-    if (qe == 0 || 2 * qe > (uint32_t)kMaxDir) return "query must have 1..16 edges (5-bit directed index)";
+    if (max_qe > (uint32_t)kMaxQE) max_qe = kMaxQE;
+    if (qe == 0 || qe > max_qe)
+        return max_qe == (uint32_t)kMaxQEKeyed ? "query must have 1..16 edges (5-bit directed index)"
+                                               : "query must have 1..32 edges";
     q = QueryMeta();
     q.qv = qv;
     if (labels) q.labels.assign(labels, labels + qv);

@@ -7,8 +7,13 @@
 namespace cgb {
 
 constexpr int kMaxQV = 12;   // utils/config.h:5 (MAX_VCOUNT)
-constexpr int kMaxDir = 32;  // 5-bit directed index in the key (calig_helper_gamma.cu:228)
-constexpr int kMaxQE = 16;
+// Query edges of a pattern.  The single-query engine's keys carry the directed
+// query-edge index in 5 bits (calig_helper_gamma.cu:228), so it takes at most
+// kMaxQEKeyed edges; the multi-query engine keys its index by data-vertex
+// label instead and takes up to kMaxQE (dense 11- and 12-vertex patterns).
+constexpr int kMaxQE = 32;
+constexpr int kMaxQEKeyed = 16;
+constexpr int kMaxDir = 2 * kMaxQE;
 constexpr int kMaxBN = 48;
 
 // Query graph metadata, numbered exactly as the reference numbers it:
@@ -72,7 +77,10 @@ struct EdgePlan {
     // reads (a list's owner or an excluded vertex); a prefix change at a
     // deeper position leaves every prefix-only tail count as it was.
     uint8_t tail_dep;
+    // kPlan* bits: per-plan schedule choices (the multi-query autotuner's)
+    uint8_t flags;
 };
+constexpr uint8_t kPlanNoTailCache = 0x1;  // recount every tail subset per core embedding
 
 // Valid-bit plan of one query edge ei (the reference's 1-bit support masks,
 // BuildLocalIndexBitAll, graph_gpu.cu:803-869): its indexing order (BFS from
@@ -99,9 +107,9 @@ void select_starting_edge(const QueryMeta& q, const uint64_t* card, const float*
 // (plan.cpp:1361-1366).
 std::string plan_valid_bits(const QueryMeta& q, const uint32_t start[2], VbPlan* plans);
 
-// Returns "" on success, else an error message.
+// Returns "" on success, else an error message; at most max_qe edges.
 std::string build_query_meta(uint32_t qv, uint32_t qe, const uint32_t* edges, const uint32_t* labels,
-                             QueryMeta& q);
+                             QueryMeta& q, uint32_t max_qe = kMaxQEKeyed);
 std::string parse_query_file(const std::string& path, std::vector<uint32_t>& labels,
                              std::vector<uint32_t>& edges, uint32_t& qv);
 // avg_deg[dir]: mean run length of direction dir in the initial index.

@@ -1,10 +1,13 @@
 """Multi-GPU plumbing: one process per GPU (launched by torchrun).
 
 Every rank keeps a full replica of the index and applies every batch; the
-matching of a batch is split by seed (delta edge): rank r expands the seeds
-i with i % world == r (cgb_config.shard_index / num_shards).  The batch
-count is the sum of the ranks' counts (one all-reduce of a u64 per batch, NCCL
-on GPUs, gloo on CPU), and a step's time is the maximum over ranks.
+matching of a batch is split by seed group: rank r expands the seeds whose
+group key (query edge, vertex at the plan's first position) hashes to r
+modulo the world size (cgb_config.shard_index / num_shards), so the seeds
+of one pendant group stay on one rank.  The batch count is the sum of the
+ranks' counts modulo 2^64 (the engine's u64 counter semantics; one
+all-reduce per batch, NCCL on GPUs, gloo on CPU), and a step's time is the
+maximum over ranks.
 """
 from __future__ import annotations
 
@@ -38,12 +41,20 @@ def _device():
 
 
 def sum_counts(counts: list[int]) -> list[int]:
-    """Element-wise sum over ranks of per-batch match counts (< 2^63 each)."""
+    """Element-wise sum over ranks of per-batch match counts, modulo 2^64.
+
+    Counts are u64 values (any value below 2^64, wrapped like the engine's
+    own counters).  Each is split into its low and high 32-bit halves, which
+    are summed as int64 (exact for up to 2^31 ranks) and recombined."""
+    counts = [int(c) % (1 << 64) for c in counts]
     if not dist.is_initialized():
-        return list(counts)
-    t = torch.tensor(counts, dtype=torch.int64, device=_device())
+        return counts
+    halves = [c & 0xFFFFFFFF for c in counts] + [c >> 32 for c in counts]
+    t = torch.tensor(halves, dtype=torch.int64, device=_device())
     dist.all_reduce(t, op=dist.ReduceOp.SUM)
-    return [int(x) for x in t.tolist()]
+    s = [int(x) for x in t.tolist()]
+    n = len(counts)
+    return [(s[i] + (s[n + i] << 32)) % (1 << 64) for i in range(n)]
 
 
 def max_value(x: float) -> float:

@@ -25,15 +25,22 @@ EXPORTS = [
     "cgb_default_config", "cgb_create", "cgb_destroy", "cgb_last_error", "cgb_load_query",
     "cgb_load_query_file", "cgb_query_dir", "cgb_build_index", "cgb_apply_batch",
     "cgb_apply_batch_device", "cgb_last_edge_counts", "cgb_read_index", "cgb_last_timings",
-    "cgb_kernel_launches", "cgb_last_stats", "cgb_stream", "cgb_producer_open", "cgb_producer_close", "cgb_producer_last_error",
+    "cgb_kernel_launches", "cgb_last_stats", "cgb_stream", "cgb_plan_anchor", "cgb_check_symmetry",
+    "cgb_producer_open", "cgb_producer_close", "cgb_producer_last_error",
     "cgb_producer_num_batches", "cgb_producer_initial", "cgb_producer_next", "cgb_producer_vertex_map",
     "cgb_merge_keys_noalloc", "cgb_valid_bits", "cgb_starting_edge",
     "cgb_gpma_create", "cgb_gpma_destroy", "cgb_gpma_last_error", "cgb_gpma_bulk_load", "cgb_gpma_batch_update",
     "cgb_gpma_extract", "cgb_gpma_stats",
+    "cgb_mq_default_config", "cgb_mq_create", "cgb_mq_destroy", "cgb_mq_last_error", "cgb_mq_load_graph",
+    "cgb_mq_register_query", "cgb_mq_unregister_query", "cgb_mq_apply_batch", "cgb_mq_apply_batch_device",
+    "cgb_mq_last_timings", "cgb_mq_last_stats", "cgb_mq_query_info", "cgb_mq_schedule", "cgb_mq_kernel_launches",
+    "cgb_mq_stream",
 ]
 
-# Edits one cgb_merge_keys_noalloc call accepts (CGB_NOALLOC_MAX_EDITS).
+# Edits one cgb_merge_keys_noalloc call accepts (CGB_NOALLOC_MAX_EDITS), and
+# old keys + edits (CGB_NOALLOC_MAX_KEYS).
 NOALLOC_MAX_EDITS = 1 << 18
+NOALLOC_MAX_KEYS = 1 << 27
 
 
 class CgbError(RuntimeError):
@@ -57,6 +64,17 @@ FLAG_VALID_BITS = 0x40
 FLAG_MASK_PRUNE = 0x80
 FLAG_NO_SEED_GROUPS = 0x100
 FLAG_NO_RUN_BITS = 0x200
+
+
+class MqConfig(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int), ("flags", _u32), ("dfs_budget_ms", _u32), ("dfs_blocks_per_sm", _u32),
+                ("pool_words", _u64)]
+
+
+MQ_FLAG_NO_AUTOTUNE = 0x1
+MQ_FLAG_NO_GRAPH = 0x2
+MQ_FLAG_NO_RUN_BITS = 0x4
+MQ_MAX_QUERIES = 256
 
 
 class BatchKeys(ctypes.Structure):
@@ -98,6 +116,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.cgb_last_stats.argtypes = [_vp, _vp]
     lib.cgb_stream.argtypes = [_vp]
     lib.cgb_stream.restype = _vp
+    lib.cgb_plan_anchor.argtypes = [_vp, _u32, ctypes.POINTER(_u32)]
+    lib.cgb_check_symmetry.argtypes = [_vp, ctypes.POINTER(_u64)]
     lib.cgb_producer_open.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, _u32, _u32,
                                       ctypes.POINTER(_vp)]
     lib.cgb_producer_close.argtypes = [_vp]
@@ -120,6 +140,24 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.cgb_gpma_batch_update.argtypes = [_vp, _vp, _u64, _vp, _u64]
     lib.cgb_gpma_extract.argtypes = [_vp, _u32, _vp, _u64, ctypes.POINTER(_u64)]
     lib.cgb_gpma_stats.argtypes = [_vp, _vp]
+    lib.cgb_mq_default_config.argtypes = [ctypes.POINTER(MqConfig)]
+    lib.cgb_mq_create.argtypes = [ctypes.POINTER(MqConfig), ctypes.POINTER(_vp)]
+    lib.cgb_mq_destroy.argtypes = [_vp]
+    lib.cgb_mq_last_error.argtypes = [_vp]
+    lib.cgb_mq_last_error.restype = ctypes.c_char_p
+    lib.cgb_mq_load_graph.argtypes = [_vp, _u32, _vp, _u64, _vp]
+    lib.cgb_mq_register_query.argtypes = [_vp, _u32, _vp, _u32, _vp, ctypes.POINTER(_u32)]
+    lib.cgb_mq_unregister_query.argtypes = [_vp, _u32]
+    lib.cgb_mq_apply_batch.argtypes = [_vp, _vp, _u64, _vp, _u64, _vp, _vp, _u32]
+    lib.cgb_mq_apply_batch_device.argtypes = [_vp, _vp, _u64, _vp, _u64, _vp, _vp, _vp, _u32]
+    lib.cgb_mq_last_timings.argtypes = [_vp, _vp]
+    lib.cgb_mq_last_stats.argtypes = [_vp, _vp]
+    lib.cgb_mq_query_info.argtypes = [_vp, _u32, ctypes.POINTER(_u32), ctypes.POINTER(ctypes.c_float)]
+    lib.cgb_mq_schedule.argtypes = [_vp, ctypes.POINTER(_u32), ctypes.POINTER(_u32)]
+    lib.cgb_mq_kernel_launches.argtypes = [_vp]
+    lib.cgb_mq_kernel_launches.restype = _u64
+    lib.cgb_mq_stream.argtypes = [_vp]
+    lib.cgb_mq_stream.restype = _vp
     for name in EXPORTS:
         getattr(lib, name)
     _lib_handle = lib
@@ -251,6 +289,18 @@ class Engine:
     def stream(self) -> int:
         return int(self.lib.cgb_stream(self.h) or 0)
 
+    def plan_anchor(self, ei: int) -> int:
+        """Query vertex at the first position of query edge ei's plan (keys the seed shard)."""
+        v = _u32(0)
+        self._check(self.lib.cgb_plan_anchor(self.h, ei, ctypes.byref(v)))
+        return v.value
+
+    def check_symmetry(self) -> int:
+        """Index entries whose mirror entry is missing (0 for a symmetric index)."""
+        n = _u64(0)
+        self._check(self.lib.cgb_check_symmetry(self.h, ctypes.byref(n)))
+        return n.value
+
     def kernel_launches(self) -> int:
         return int(self.lib.cgb_kernel_launches(self.h))
 
@@ -378,3 +428,108 @@ class Gpma:
         return {"slots": int(out[0]), "windows": int(out[1]), "rewritten": int(out[2]), "rebuilt": int(out[3]),
                 "device_us": int(out[4]), "keys": int(out[5])}
 
+
+
+def _pairs(edges) -> np.ndarray:
+    a = np.ascontiguousarray(np.asarray(edges, dtype=np.uint32).reshape(-1, 2))
+    return a
+
+
+class MultiQuery:
+    """Multi-query engine (cgb_mq_*): one device-resident data-graph index
+    shared by registered queries, all matched per batch in one launch."""
+
+    def __init__(self, device: int = 0, flags: int = 0, dfs_budget_ms: int = 0, dfs_blocks_per_sm: int = 0,
+                 pool_words: int = 0):
+        self.lib = load_library()
+        cfg = MqConfig(device, flags, dfs_budget_ms, dfs_blocks_per_sm, pool_words)
+        h = _vp()
+        st = self.lib.cgb_mq_create(ctypes.byref(cfg), ctypes.byref(h))
+        self.h = h.value
+        if st != 0:
+            msg = self.lib.cgb_mq_last_error(self.h).decode() if self.h else ""
+            self.close()
+            raise CgbError(st, msg)
+        self.ids: set[int] = set()
+
+    def _check(self, st: int) -> None:
+        if st != 0:
+            raise CgbError(st, self.lib.cgb_mq_last_error(self.h).decode())
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.lib.cgb_mq_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def load_graph(self, labels, edges) -> None:
+        lab = np.ascontiguousarray(labels, dtype=np.uint32)
+        e = _pairs(edges)
+        self._check(self.lib.cgb_mq_load_graph(self.h, len(lab), lab.ctypes.data, len(e),
+                                               e.ctypes.data if len(e) else None))
+
+    def register(self, qv: int, edges, labels) -> int:
+        e = np.ascontiguousarray(np.asarray(edges, dtype=np.uint32).reshape(-1))
+        lab = np.ascontiguousarray(labels, dtype=np.uint32)
+        qid = _u32(0)
+        self._check(self.lib.cgb_mq_register_query(self.h, qv, lab.ctypes.data, len(e) // 2, e.ctypes.data,
+                                                   ctypes.byref(qid)))
+        self.ids.add(qid.value)
+        return qid.value
+
+    def unregister(self, qid: int) -> None:
+        self._check(self.lib.cgb_mq_unregister_query(self.h, qid))
+        self.ids.discard(qid)
+
+    def apply_batch(self, ins=None, dele=None) -> tuple[np.ndarray, np.ndarray]:
+        """(positive, negative) counts per query id (arrays of MQ_MAX_QUERIES u64)."""
+        ins = _pairs(ins if ins is not None else np.zeros((0, 2)))
+        dele = _pairs(dele if dele is not None else np.zeros((0, 2)))
+        pos = np.zeros(MQ_MAX_QUERIES, dtype=np.uint64)
+        neg = np.zeros(MQ_MAX_QUERIES, dtype=np.uint64)
+        self._check(self.lib.cgb_mq_apply_batch(self.h, ins.ctypes.data if len(ins) else None, len(ins),
+                                                dele.ctypes.data if len(dele) else None, len(dele),
+                                                pos.ctypes.data, neg.ctypes.data, MQ_MAX_QUERIES))
+        return pos, neg
+
+    def apply_batch_device(self, ins_ptr: int, n_ins: int, del_ptr: int = 0, n_del: int = 0,
+                           stream: int = 0) -> tuple[np.ndarray, np.ndarray]:
+        pos = np.zeros(MQ_MAX_QUERIES, dtype=np.uint64)
+        neg = np.zeros(MQ_MAX_QUERIES, dtype=np.uint64)
+        self._check(self.lib.cgb_mq_apply_batch_device(self.h, ins_ptr or None, n_ins, del_ptr or None, n_del,
+                                                       stream or None, pos.ctypes.data, neg.ctypes.data,
+                                                       MQ_MAX_QUERIES))
+        return pos, neg
+
+    def timings(self) -> np.ndarray:
+        t = np.zeros(4, dtype=np.float32)
+        self._check(self.lib.cgb_mq_last_timings(self.h, t.ctypes.data))
+        return t
+
+    def stats(self) -> dict:
+        out = np.zeros(8, dtype=np.uint64)
+        self._check(self.lib.cgb_mq_last_stats(self.h, out.ctypes.data))
+        return {"seeds": int(out[0]), "chunks": int(out[1]), "tested": int(out[2]), "tails": int(out[3]),
+                "match_bytes": int(out[4]), "update_bytes": int(out[5]), "touched_runs": int(out[6]),
+                "stolen_tasks": int(out[7])}
+
+    def query_info(self, qid: int) -> tuple[int, float]:
+        v, ms = _u32(0), ctypes.c_float(0)
+        self._check(self.lib.cgb_mq_query_info(self.h, qid, ctypes.byref(v), ctypes.byref(ms)))
+        return v.value, float(ms.value)
+
+    def schedule(self) -> tuple[int, int]:
+        b, st = _u32(0), _u32(0)
+        self._check(self.lib.cgb_mq_schedule(self.h, ctypes.byref(b), ctypes.byref(st)))
+        return b.value, st.value
+
+    def kernel_launches(self) -> int:
+        return int(self.lib.cgb_mq_kernel_launches(self.h))
+
+    def stream(self) -> int:
+        return int(self.lib.cgb_mq_stream(self.h) or 0)

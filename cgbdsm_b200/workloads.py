@@ -7,6 +7,10 @@ the engine is measured on (seeds fixed so every run sees the same input):
   c1  Erdos-Renyi 10,000 vertices / 50,000 edges, 8 uniform labels,
       10% (5,000 edges) held out and re-inserted in batches of 1,000,
       5-vertex dense pattern (densest induced BFS sample, see gen.cpp).
+      With query seed 11 no batch has a positive match (the sampled
+      occurrence uses no held-out edge, and the pattern is rare at this
+      density); c1_q25 is the same graph and stream with query seed 25, the
+      first seed whose first two batches have positive matches (4 and 6).
   c2  R-MAT(0.57,0.19,0.19,0.05) 1,000,000 vertices / 10,000,000 edges,
       16 labels Zipf(1.2), 1,000,000 held out, batches of 100,000,
       9-vertex dense pattern with <= 16 edges.  Every sampled pattern is
@@ -58,6 +62,7 @@ class WorkloadSpec:
 
 SPECS = {
     "c1": WorkloadSpec("c1", 0, 10_000, 50_000, 8, 0.0, 5_000, 1_000, 0, 5, 1, 2, 3, 11),
+    "c1_q25": WorkloadSpec("c1_q25", 0, 10_000, 50_000, 8, 0.0, 5_000, 1_000, 0, 5, 1, 2, 3, 25),
     "c2": WorkloadSpec("c2", 1, 1_000_000, 10_000_000, 16, 1.2, 1_000_000, 100_000, 0, 9, 21, 22, 23, 41),
     "c3_tree": WorkloadSpec("c3_tree", 1, 4_000_000, 34_000_000, 32, 1.0, 3_400_000, 1_000_000, 2, 7,
                             31, 32, 33, 34),
@@ -117,6 +122,68 @@ def materialize_query(spec: WorkloadSpec, path: str, seed_query: int) -> int:
     if rc != 0:
         raise RuntimeError(f"query generation failed: rc={rc}")
     return qe.value
+
+
+class GraphData:
+    """A workload's graph in memory (cgbgen_open): labels, initial edges and
+    the held-out stream as (x, y) pairs, identical to what materialize()
+    writes, plus query patterns sampled from the final graph (query seed s
+    gives the pattern materialize() writes with seed_query s)."""
+
+    def __init__(self, spec: WorkloadSpec):
+        import numpy as np
+
+        lib = ctypes.CDLL(GEN_LIB)
+        lib.cgbgen_open.restype = ctypes.c_void_p
+        lib.cgbgen_open.argtypes = [ctypes.c_int, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_double, ctypes.c_double,
+                                    ctypes.c_double, ctypes.c_uint32, ctypes.c_double, ctypes.c_uint64,
+                                    ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64]
+        lib.cgbgen_close.argtypes = [ctypes.c_void_p]
+        lib.cgbgen_sizes.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        lib.cgbgen_copy.argtypes = [ctypes.c_void_p] * 4
+        lib.cgbgen_query.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_uint32, ctypes.c_uint32,
+                                     ctypes.c_uint64, ctypes.c_void_p, ctypes.c_void_p,
+                                     ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_uint32)]
+        self.lib = lib
+        self.spec = spec
+        self.h = lib.cgbgen_open(spec.kind, spec.n, spec.m, 0.57, 0.19, 0.19, spec.labels, spec.zipf, spec.holdout,
+                                 spec.seed_graph, spec.seed_labels, spec.seed_holdout)
+        sz = np.zeros(3, dtype=np.uint64)
+        lib.cgbgen_sizes(self.h, sz.ctypes.data)
+        self.n = int(sz[0])
+        self.labels = np.zeros(self.n, dtype=np.uint32)
+        self.initial = np.zeros((int(sz[1]), 2), dtype=np.uint32)
+        self.stream = np.zeros((int(sz[2]), 2), dtype=np.uint32)
+        lib.cgbgen_copy(self.h, self.labels.ctypes.data, self.initial.ctypes.data, self.stream.ctypes.data)
+
+    def query(self, shape: int, size: int, seed: int, max_qedges: int = 32):
+        """(labels, edges) of a pattern: shape 0 dense, 1 sparse, 2 tree; None if none was found."""
+        import numpy as np
+
+        lab = np.zeros(12, dtype=np.uint32)
+        edges = np.zeros(2 * 66, dtype=np.uint32)
+        qv, qe = ctypes.c_uint32(0), ctypes.c_uint32(0)
+        rc = self.lib.cgbgen_query(self.h, shape, size, max_qedges, seed, lab.ctypes.data, edges.ctypes.data,
+                                   ctypes.byref(qv), ctypes.byref(qe))
+        if rc != 0:
+            return None
+        return [int(x) for x in lab[: qv.value]], [(int(edges[2 * i]), int(edges[2 * i + 1])) for i in range(qe.value)]
+
+    def batches(self):
+        """The stream cut into the spec's batches."""
+        b = self.spec.batch_edges
+        return [self.stream[i:i + b] for i in range(0, len(self.stream), b)]
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.lib.cgbgen_close(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def read_query(path: str) -> tuple[list[int], list[tuple[int, int]]]:

@@ -48,10 +48,12 @@ typedef struct {
     uint32_t flags;          /* CGB_FLAG_* below                                           */
     uint32_t dfs_budget_ms;  /* wall-clock budget of one matching launch; past it the batch
                                 fails with CGB_ERR_TIMEOUT (count incomplete); 0 = 600 s   */
-    uint32_t shard_index;    /* multi-GPU: this engine matches the seeds (delta edges) i with */
-    uint32_t num_shards;     /* i % num_shards == shard_index; 0 or 1 = all seeds.  Every    */
-                             /* shard applies every batch to its own full index replica; the */
-                             /* batch count is the sum of the shards' counts.                */
+    uint32_t shard_index;    /* multi-GPU: this engine matches the seed groups whose key      */
+    uint32_t num_shards;     /* (query edge ei, vertex x at the edge plan's first position)  */
+                             /* hashes to shard_index (splitmix64 finaliser of ei << 32 | x,  */
+                             /* modulo num_shards); 0 or 1 = all seeds.  Every shard applies   */
+                             /* every batch to its own full index replica; the batch count is */
+                             /* the sum of the shards' counts modulo 2^64.                    */
 } cgb_config;
 
 #define CGB_FLAG_NO_MERGE_BACK_DEFER 0x1u /* apply the delta merge-back eagerly after matching */
@@ -164,6 +166,20 @@ cgb_status cgb_last_stats(const cgb_handle* h, uint64_t* out8);
 /* The engine's CUDA stream (a cudaStream_t) on which all its work runs. */
 void* cgb_stream(const cgb_handle* h);
 
+/* Query vertex at the first position of query edge ei's matching plan (one of
+ * ei's endpoints): the vertex whose data vertex keys the seed shard.  The
+ * reference plans one global order instead (plan.cpp:535-745).  Available
+ * after cgb_build_index. */
+cgb_status cgb_plan_anchor(const cgb_handle* h, uint32_t ei, uint32_t* qvertex);
+
+/* Index symmetry check (after any pending delta merge-back): *n_asym = number
+ * of index entries y in the list of (a -> b) at x whose mirror entry (x in
+ * the list of (b -> a) at y) is missing.  The matcher's per-edge seeding gives
+ * the reference's global-order counts when this is 0 (the reference builds
+ * both directions from one data edge, calig_helper_gamma.cu:248-277 and
+ * calig.cpp:776-804). */
+cgb_status cgb_check_symmetry(cgb_handle* h, uint64_t* n_asym);
+
 /* ------------------------------------------------------------------------
  * Stage-1 producer: the CaLiG candidate index on the host and the host
  * staging that turns its deltas into the keys above.  Replaces, per batch,
@@ -231,12 +247,18 @@ cgb_status cgb_producer_vertex_map(const cgb_producer* p, const uint32_t** new2o
  * that every GPU loading this library holds until the process exits; calls
  * keep their contents in it, so calls whose work overlaps on one GPU race and
  * must be ordered by the caller.  The first call on a device looks up the
- * array's device address (cudaGetSymbolAddress) with that device current:
- * make it before any stream capture.  Rejects more than CGB_NOALLOC_MAX_EDITS
- * edits (n_ins + n_del) with CGB_ERR_LIMIT, before touching the device.
- * Never calls cudaMalloc or cudaFree.
+ * array's device address (cudaGetSymbolAddress) with that device current,
+ * and looks it up again after that device's context was reset: make the
+ * first call before any stream capture.  Rejects more than
+ * CGB_NOALLOC_MAX_EDITS edits (n_ins + n_del), or more than
+ * CGB_NOALLOC_MAX_KEYS keys in all (n_old + n_ins + n_del), with
+ * CGB_ERR_LIMIT; every limit is checked before any work is enqueued.  An
+ * error already pending on the calling thread (cudaPeekAtLastError) makes the
+ * call return CGB_ERR_CUDA without enqueuing anything and without clearing
+ * it.  Never calls cudaMalloc or cudaFree.
  * ------------------------------------------------------------------------ */
 #define CGB_NOALLOC_MAX_EDITS (1u << 18)
+#define CGB_NOALLOC_MAX_KEYS (1ull << 27)
 cgb_status cgb_merge_keys_noalloc(const uint64_t* old_keys_device, uint64_t n_old,
                                   const uint64_t* ins_device, uint64_t n_ins,
                                   const uint64_t* del_device, uint64_t n_del, uint32_t dv_count,
@@ -283,6 +305,86 @@ cgb_status cgb_valid_bits(cgb_handle* h, uint32_t* out, uint64_t cap, uint64_t* 
  * use: out2[0], out2[1] = the first two vertices of the reference's global
  * order.  Available after cgb_build_index. */
 cgb_status cgb_starting_edge(const cgb_handle* h, uint32_t* out2);
+
+/* ------------------------------------------------------------------------
+ * Multi-query engine.  No single counterpart in the reference, which runs one
+ * query per process (main_calig.cpp:44-450: a CaLiG index, GAMMA staging
+ * and one MatchingBitAll per batch, graph_gpu.cu:1261-1480); this engine
+ * replaces N such processes on one device.
+ *
+ * One device-resident data-graph index, keyed by target-vertex label (the
+ * list of (label L, vertex x) = x's neighbours of label L, sorted), is shared
+ * by every registered query; all queries are matched per batch in one
+ * persistent launch (replayed as a CUDA graph while its arguments are
+ * unchanged), with the reference's count semantics per query: the
+ * embeddings that map some query edge to a batch edge, counted once at
+ * their largest such edge, edges before it matched to old-or-batch edges and
+ * after it to old edges (enumeration.cu:768, 797, 937).  For insertions this
+ * equals the CaLiG pipeline's positive matches (CaLiG's lists are these
+ * lists pruned by a filter every embedding passes, calig.cpp:358-408);
+ * deletions count the embeddings they destroy (negative matches), matched
+ * against the graph without the deleted edges, before any insertion.
+ * Queries: <= 12 vertices, <= 32 edges, labels < 32; registered or removed
+ * between batches.  An autotuner times, on the first batch a query sees,
+ * its plan variants (core order, tail counting cache, seed grouping) and
+ * the DFS grid size and work stealing for the whole set, and keeps the
+ * fastest (counts are identical across variants).
+ * ------------------------------------------------------------------------ */
+typedef struct cgb_mq cgb_mq;
+
+typedef struct {
+    int device;
+    uint32_t flags;             /* CGB_MQ_FLAG_* */
+    uint32_t dfs_budget_ms;     /* wall-clock budget of one matching launch; 0 = 600 s */
+    uint32_t dfs_blocks_per_sm; /* 0 = autotuned */
+    uint64_t pool_words;        /* neighbour-run pool capacity in u32 words; 0 = automatic */
+} cgb_mq_config;
+
+#define CGB_MQ_FLAG_NO_AUTOTUNE 0x1u  /* default plans and grid, no trials        */
+#define CGB_MQ_FLAG_NO_GRAPH 0x2u     /* launch the matching step directly         */
+#define CGB_MQ_FLAG_NO_RUN_BITS 0x4u  /* binary-search long runs (no bit sets)     */
+#define CGB_MQ_MAX_QUERIES 256
+#define CGB_MQ_MAX_LABELS 32
+
+void cgb_mq_default_config(cgb_mq_config* cfg);
+cgb_status cgb_mq_create(const cgb_mq_config* cfg, cgb_mq** out);
+void cgb_mq_destroy(cgb_mq* m);
+const char* cgb_mq_last_error(const cgb_mq* m);
+/* The data graph: n vertices with labels[n] (< 32), num_edges undirected
+ * edges as (x, y) pairs (no self-loops, no duplicates).  Host arrays. */
+cgb_status cgb_mq_load_graph(cgb_mq* m, uint32_t n, const uint32_t* labels, uint64_t num_edges,
+                             const uint32_t* edges);
+/* Registers a query (qv vertices with labels, qe edges as (a, b) pairs);
+ * *query_id indexes the count arrays.  Takes effect at the next batch. */
+cgb_status cgb_mq_register_query(cgb_mq* m, uint32_t qv, const uint32_t* labels, uint32_t qe,
+                                 const uint32_t* edges, uint32_t* query_id);
+cgb_status cgb_mq_unregister_query(cgb_mq* m, uint32_t query_id);
+/* One batch: n_del deleted and n_ins inserted undirected edges as (x, y)
+ * pairs (host arrays; edges absent from / already in the graph, and repeats,
+ * are ignored).  pos_counts[id] / neg_counts[id] (cap entries, optional)
+ * receive each registered query's positive / negative matches, modulo 2^64.
+ * Order: deletions (matched against the graph without them), then
+ * insertions (matched, joining the graph before the next batch). */
+cgb_status cgb_mq_apply_batch(cgb_mq* m, const uint32_t* ins_edges, uint64_t n_ins, const uint32_t* del_edges,
+                              uint64_t n_del, uint64_t* pos_counts, uint64_t* neg_counts, uint32_t cap);
+/* Same with the edge pairs in device memory; work enqueued after the
+ * caller's prior work on `stream` (NULL = none); returns with counts read. */
+cgb_status cgb_mq_apply_batch_device(cgb_mq* m, const uint32_t* ins_device, uint64_t n_ins,
+                                     const uint32_t* del_device, uint64_t n_del, void* stream,
+                                     uint64_t* pos_counts, uint64_t* neg_counts, uint32_t cap);
+/* Last batch, device milliseconds: t[0] index merge, t[1] delta preparation,
+ * t[2] matching (autotuner trials excluded), t[3] whole batch. */
+cgb_status cgb_mq_last_timings(const cgb_mq* m, float* t4);
+/* Work counters of the last batch (as cgb_last_stats). */
+cgb_status cgb_mq_last_stats(const cgb_mq* m, uint64_t* out8);
+/* Autotuned plan variant of a query (bit 0 plain core order, bit 1 no tail
+ * cache, bit 2 no seed groups) and its matching time alone on the tuning
+ * batch (ms; < 0 if not tuned). */
+cgb_status cgb_mq_query_info(const cgb_mq* m, uint32_t query_id, uint32_t* variant, float* tuned_ms);
+/* The DFS schedule in use: blocks per SM and whether work stealing is on. */
+cgb_status cgb_mq_schedule(const cgb_mq* m, uint32_t* blocks_per_sm, uint32_t* steal);
+uint64_t cgb_mq_kernel_launches(const cgb_mq* m);
+void* cgb_mq_stream(const cgb_mq* m);
 
 #ifdef __cplusplus
 }

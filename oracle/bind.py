@@ -20,20 +20,23 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_LIB = os.path.join(HERE, "_ref", "libcgbref.so")
 ORACLE_LIB = os.path.join(HERE, "liboracle.so")
-REF_TREE = os.environ.get("CGB_REFERENCE_TREE", "/root/reference")
+# The reference source tree, when this machine has one (only `build` reads it).
+REF_TREE = os.environ.get("CGB_REFERENCE_TREE", "")
 
 _u8p = ctypes.POINTER(ctypes.c_uint8)
 _u64p = ctypes.POINTER(ctypes.c_uint64)
 _u32, _u64, _vp = ctypes.c_uint32, ctypes.c_uint64, ctypes.c_void_p
 
-GLOBAL, PER_EDGE = 0, 1
+GLOBAL, PER_EDGE, TAIL = 0, 1, 2
 
 
-def build(ref: bool = True) -> None:
-    """Builds liboracle.so, and libcgbref.so when the reference tree is present."""
+def build(ref: bool = True, ref_tree: Optional[str] = None) -> None:
+    """Builds liboracle.so, and libcgbref.so when a reference source tree is
+    given (ref_tree, else $CGB_REFERENCE_TREE) and present on this machine."""
     subprocess.run(["make", "-s", "-C", HERE, "oracle"], check=True)
-    if ref and os.path.isdir(REF_TREE):
-        subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={REF_TREE}"], check=True)
+    tree = ref_tree or REF_TREE
+    if ref and tree and os.path.isdir(tree):
+        subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={tree}"], check=True)
 
 
 def have_ref() -> bool:
@@ -227,6 +230,7 @@ class Oracle:
         L.orc_valid_bits.restype = _u64
         L.orc_indexing_order.argtypes = [_vp, _u32, _u32, _u32, _vp, _vp, _vp, _vp]
         L.orc_indexing_order.restype = _u32
+        L.orc_set_shard.argtypes = [_vp, _u32, _u32, _vp]
         L.orc_bruteforce.restype = _u64
         L.orc_bruteforce.argtypes = [_u32, _vp, _vp, _vp, _u32, _vp, _u32, _vp]
         self.L = L
@@ -303,6 +307,13 @@ class Oracle:
         out = np.zeros(max(n, 1), np.uint32)
         self.L.orc_valid_bits(self.h, out.ctypes.data, n)
         return out[:n]
+
+    def set_shard(self, shard: int, num_shards: int, anchor=None) -> None:
+        """Counts only the seeds of one shard: those whose key (query edge ei,
+        data vertex at query vertex anchor[ei]; default ei's first endpoint)
+        hashes to `shard` like the engine's seed groups."""
+        a = None if anchor is None else np.ascontiguousarray(anchor, dtype=np.uint8)
+        self.L.orc_set_shard(self.h, shard, num_shards, a.ctypes.data if a is not None else None)
 
     def asymmetry(self) -> int:
         return int(self.L.orc_asymmetry(self.h))

@@ -36,6 +36,12 @@
  *               entries of ei; equal to ORC_GLOBAL whenever the index lists
  *               are symmetric ((a->b) contains y at x iff (b->a) contains x
  *               at y), which tests/ check as a property.
+ *   ORC_TAIL  per-edge seeding with an independent tail counted instead of
+ *             enumerated (see count_tail below): pins the engine's counted
+ *             tails on workloads too large to enumerate.
+ * Seeds may be restricted to one shard of the seed groups (orc_set_shard),
+ * keyed like the engine's: a splitmix64 finaliser of (ei << 32 | x), x the
+ * data vertex at a given query vertex of ei.
  * Plus an independent brute-force embedding counter for the incremental
  * identity  sum(batch counts) = |Emb(Q, G_after)| - |Emb(Q, G_before)|,
  * and the valid bits of BuildLocalIndexBitAll (graph_gpu.cu:803-869,
@@ -50,7 +56,7 @@
 #define ORC_MAXD 32
 #define ORC_MAXQE 16
 
-enum { ORC_GLOBAL = 0, ORC_PER_EDGE = 1 };
+enum { ORC_GLOBAL = 0, ORC_PER_EDGE = 1, ORC_TAIL = 2 };
 
 typedef struct {
     uint32_t* v;
@@ -68,6 +74,10 @@ typedef struct {
     uint64_t* pending;  /* delta keys of the last matched batch (merged before the next) */
     uint64_t n_pending;
     uint64_t last_edge_counts[ORC_MAXQE];
+    /* seed shard: keep seeds whose (ei, data vertex at query vertex
+     * shard_anchor[ei]) hashes to shard (num_shards <= 1: all seeds) */
+    uint32_t shard, num_shards;
+    uint8_t shard_anchor[ORC_MAXQE];
     /* valid bits (BuildLocalIndexBitAll) of the last matched batch */
     int vb_on;
     uint32_t vb_start[2];
@@ -233,6 +243,7 @@ typedef struct {
     uint8_t bn_pos[64], bn_dir[64];
     int seed_dirs[2];
     uint32_t m[ORC_MAXQV];
+    uint32_t ncore;  /* ORC_TAIL: positions >= ncore are counted, not enumerated */
 } Run;
 
 /* cpu_dfs.cpp:67-78: (base, app) of directed edge d at vertex x under ei. */
@@ -272,6 +283,225 @@ static uint64_t dfs(Run* r, uint32_t j) {
         }
     }
     return cnt;
+}
+
+/* ---- counted tails (ORC_TAIL) ----
+ * The tail positions T = [ncore, qv) hold pairwise non-adjacent query
+ * vertices whose neighbours are all core vertices, so once the core is
+ * matched each tail vertex p draws from a fixed candidate multiset: the
+ * entries of its first backward list (base and, when visible, delta part)
+ * that lie in every other backward list, weight w_p(c) = occurrences of c.
+ * The enumeration would count, over injective assignments f of T avoiding
+ * the core's vertices, the product of w_p(f(p)).  By Moebius inversion over
+ * the lattice of set partitions of T (a partition's blocks are the tail
+ * vertices that coincide), that is
+ *     sum over partitions P of prod over blocks B of  mu(B) * W(B),
+ *     mu(B) = (-1)^(|B|-1) (|B|-1)!,
+ *     W(B)  = sum over c in (common candidates of B) minus the core's
+ *             vertices of prod over p in B of w_p(c),
+ * evaluated with the subset recursion F(S) = sum over blocks B of S that
+ * contain S's lowest member of mu(B) W(B) F(S \ B), F(empty) = 1, in
+ * arithmetic modulo 2^64 (the counters' own). */
+typedef struct {
+    uint32_t* v;  /* sorted distinct values */
+    uint64_t* w;  /* product of the members' weights */
+    uint32_t n;
+} WSet;
+
+static uint32_t* cand_tmp(uint32_t n) { return (uint32_t*)malloc((n ? n : 1) * sizeof(uint32_t)); }
+
+/* Candidate multiset of tail position j as a weighted set. */
+static void tail_candidates(Run* r, uint32_t j, WSet* out) {
+    uint32_t b0 = r->bn_off[j], b1 = r->bn_off[j + 1];
+    const List *gb, *ga;
+    resolve(r, r->bn_dir[b0], r->m[r->bn_pos[b0]], &gb, &ga);
+    uint32_t n = gb->n + (ga ? ga->n : 0);
+    uint32_t* all = cand_tmp(n);
+    uint32_t k = 0;
+    for (int part = 0; part < 2; ++part) {
+        const List* L = part ? ga : gb;
+        if (!L) continue;
+        for (uint32_t t = 0; t < L->n; ++t) {
+            uint32_t c = L->v[t];
+            int ok = 1;
+            for (uint32_t q = b0 + 1; q < b1 && ok; ++q) {
+                const List *xb, *xa;
+                resolve(r, r->bn_dir[q], r->m[r->bn_pos[q]], &xb, &xa);
+                ok = list_has(xb, c) || (xa && list_has(xa, c));
+            }
+            if (ok) all[k++] = c;
+        }
+    }
+    /* sort (insertion sort is too slow for hubs: use qsort on u32) */
+    uint64_t* tmp = (uint64_t*)malloc((k ? k : 1) * 8);
+    for (uint32_t i = 0; i < k; ++i) tmp[i] = all[i];
+    qsort(tmp, k, 8, cmp_u64);
+    out->v = cand_tmp(k);
+    out->w = (uint64_t*)malloc((k ? k : 1) * 8);
+    out->n = 0;
+    for (uint32_t i = 0; i < k;) {
+        uint32_t e = i;
+        while (e < k && tmp[e] == tmp[i]) ++e;
+        out->v[out->n] = (uint32_t)tmp[i];
+        out->w[out->n] = e - i;
+        ++out->n;
+        i = e;
+    }
+    free(tmp);
+    free(all);
+}
+
+static void wset_intersect(const WSet* a, const WSet* b, WSet* out) {
+    uint32_t cap = a->n < b->n ? a->n : b->n;
+    out->v = cand_tmp(cap);
+    out->w = (uint64_t*)malloc((cap ? cap : 1) * 8);
+    out->n = 0;
+    uint32_t i = 0, j = 0;
+    while (i < a->n && j < b->n) {
+        if (a->v[i] < b->v[j]) ++i;
+        else if (b->v[j] < a->v[i]) ++j;
+        else { out->v[out->n] = a->v[i]; out->w[out->n++] = a->w[i] * b->w[j]; ++i; ++j; }
+    }
+}
+
+static uint64_t count_tail(Run* r) {
+    const uint32_t nt = r->o->qv - r->ncore;
+    const uint32_t ns = 1u << nt;
+    WSet* sets = (WSet*)calloc(ns, sizeof(WSet));
+    uint64_t* W = (uint64_t*)calloc(ns, 8);
+    for (uint32_t p = 0; p < nt; ++p) tail_candidates(r, r->ncore + p, &sets[1u << p]);
+    for (uint32_t S = 1; S < ns; ++S) {
+        uint32_t top = 31 - __builtin_clz(S);
+        if (S != (1u << top)) wset_intersect(&sets[S & ~(1u << top)], &sets[1u << top], &sets[S]);
+        uint64_t sum = 0;
+        for (uint32_t i = 0; i < sets[S].n; ++i) {
+            int core = 0;
+            for (uint32_t t = 0; t < r->ncore && !core; ++t) core = r->m[t] == sets[S].v[i];
+            if (!core) sum += sets[S].w[i];
+        }
+        W[S] = sum;
+    }
+    uint64_t* F = (uint64_t*)calloc(ns, 8);
+    F[0] = 1;
+    for (uint32_t S = 1; S < ns; ++S) {
+        const uint32_t low = S & (~S + 1u), rest = S & ~low;
+        uint64_t f = 0;
+        /* blocks B = low + any subset of rest */
+        for (uint32_t sub = rest;; sub = (sub - 1) & rest) {
+            const uint32_t B = low | sub;
+            const uint32_t k = (uint32_t)__builtin_popcount(B);
+            uint64_t mu = 1;
+            for (uint32_t t = 2; t < k; ++t) mu *= t;     /* (k-1)! */
+            if (k % 2 == 0) mu = (uint64_t)0 - mu;        /* (-1)^(k-1) */
+            f += mu * W[B] * F[S & ~B];
+            if (sub == 0) break;
+        }
+        F[S] = f;
+    }
+    uint64_t res = F[ns - 1];
+    for (uint32_t S = 1; S < ns; ++S) { free(sets[S].v); free(sets[S].w); }
+    free(sets);
+    free(W);
+    free(F);
+    return res;
+}
+
+static uint64_t dfs_tail(Run* r, uint32_t j) {
+    if (j == r->ncore) return count_tail(r);
+    const Orc* o = r->o;
+    uint32_t b0 = r->bn_off[j], b1 = r->bn_off[j + 1];
+    const List *gb, *ga;
+    resolve(r, r->bn_dir[b0], r->m[r->bn_pos[b0]], &gb, &ga);
+    uint64_t cnt = 0;
+    for (int part = 0; part < 2; ++part) {
+        const List* L = part ? ga : gb;
+        if (!L) continue;
+        for (uint32_t t = 0; t < L->n; ++t) {
+            uint32_t c = L->v[t];
+            int ok = 1;
+            for (uint32_t k = 0; k < j && ok; ++k) ok = (r->m[k] != c);
+            for (uint32_t k = b0 + 1; k < b1 && ok; ++k) {
+                const List *xb, *xa;
+                resolve(r, r->bn_dir[k], r->m[r->bn_pos[k]], &xb, &xa);
+                ok = list_has(xb, c) || (xa && list_has(xa, c));
+            }
+            if (!ok) continue;
+            r->m[j] = c;
+            cnt += dfs_tail(r, j + 1);
+        }
+    }
+    (void)o;
+    return cnt;
+}
+
+/* ORC_TAIL order: ei's endpoints; the tail = query vertices taken in id order
+ * while not adjacent to the tail so far and leaving the other vertices
+ * connected; the core in between by most visited neighbours. */
+static uint32_t tail_order(const Orc* o, uint32_t ei, uint8_t* vs) {
+    const uint32_t qv = o->qv, a = o->qe_u[ei], b = o->qe_v[ei];
+    uint8_t tail[ORC_MAXQV] = {0};
+    for (uint32_t u = 0; u < qv; ++u) {
+        if (u == a || u == b) continue;
+        int adjt = 0;
+        for (uint32_t w = 0; w < qv; ++w) adjt |= tail[w] && o->eidx[u * ORC_MAXQV + w] != 255;
+        if (adjt) continue;
+        tail[u] = 1;
+        /* the rest must stay connected */
+        uint8_t seen[ORC_MAXQV] = {0}, st[ORC_MAXQV];
+        uint32_t sp = 0, reached = 1, need = 0;
+        for (uint32_t w = 0; w < qv; ++w) need += !tail[w];
+        st[sp++] = (uint8_t)a;
+        seen[a] = 1;
+        while (sp) {
+            uint32_t x = st[--sp];
+            for (uint32_t w = 0; w < qv; ++w)
+                if (!tail[w] && !seen[w] && o->eidx[x * ORC_MAXQV + w] != 255) { seen[w] = 1; ++reached; st[sp++] = (uint8_t)w; }
+        }
+        if (reached != need) tail[u] = 0;
+    }
+    uint8_t vis[ORC_MAXQV] = {0};
+    uint32_t n = 0;
+    vs[n++] = (uint8_t)a;
+    vs[n++] = (uint8_t)b;
+    vis[a] = vis[b] = 1;
+    uint32_t ncore = 2;
+    for (uint32_t u = 0; u < qv; ++u) ncore += !tail[u] && u != a && u != b;
+    while (n < ncore) {
+        int best = -1, bn = -1;
+        for (uint32_t u = 0; u < qv; ++u) {
+            if (vis[u] || tail[u]) continue;
+            int c = 0;
+            for (uint32_t w = 0; w < qv; ++w) if (vis[w] && o->eidx[u * ORC_MAXQV + w] != 255) ++c;
+            if (c > bn) { bn = c; best = (int)u; }
+        }
+        vs[n++] = (uint8_t)best;
+        vis[best] = 1;
+    }
+    for (uint32_t u = 0; u < qv; ++u)
+        if (tail[u]) vs[n++] = (uint8_t)u;
+    return ncore;
+}
+
+/* splitmix64 finaliser of (ei << 32 | x), modulo num_shards. */
+static uint32_t seed_shard(uint32_t ei, uint32_t x, uint32_t num_shards) {
+    uint64_t z = (((uint64_t)ei << 32) | x) + 0x9e3779b97f4a7c15ull;
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+    z ^= z >> 31;
+    return (uint32_t)(z % num_shards);
+}
+
+static int seed_kept(const Orc* o, uint32_t ei, uint32_t xu, uint32_t xv) {
+    if (o->num_shards <= 1) return 1;
+    const uint32_t key = o->shard_anchor[ei] == o->qe_u[ei] ? xu : xv;
+    return seed_shard(ei, key, o->num_shards) == o->shard;
+}
+
+void orc_set_shard(void* h, uint32_t shard, uint32_t num_shards, const uint8_t* anchor) {
+    Orc* o = (Orc*)h;
+    o->shard = shard;
+    o->num_shards = num_shards;
+    for (uint32_t e = 0; e < o->qe; ++e) o->shard_anchor[e] = anchor ? anchor[e] : o->qe_u[e];
 }
 
 static void make_run(const Orc* o, Run* r, uint32_t ei, const uint8_t* order) {
@@ -323,9 +553,12 @@ static uint64_t count_batch(Orc* o, const uint8_t* edge_ok, int mode, const uint
         if (!edge_ok[ei]) continue;
         Run r;
         uint8_t vs[ORC_MAXQV];
+        uint32_t ncore = o->qv;
         if (mode == ORC_GLOBAL) memcpy(vs, global_order, o->qv);
+        else if (mode == ORC_TAIL) ncore = tail_order(o, ei, vs);
         else per_edge_order(o, ei, vs);
         make_run(o, &r, ei, vs);
+        r.ncore = ncore;
         uint64_t c = 0;
         if (mode == ORC_GLOBAL) {
             /* enumeration.cu:727-809 without masks: every dv, resolved first-edge list */
@@ -348,9 +581,11 @@ static uint64_t count_batch(Orc* o, const uint8_t* edge_ok, int mode, const uint
             for (uint32_t x = 0; x < o->dv; ++x) {
                 const List* L = &o->delta[(size_t)d0 * o->dvcap + x];
                 for (uint32_t t = 0; t < L->n; ++t) {
+                    if (!seed_kept(o, ei, x, L->v[t])) continue;
                     r.m[0] = x;
                     r.m[1] = L->v[t];
-                    c += (o->qv == 2) ? 1 : dfs(&r, 2);
+                    if (mode == ORC_TAIL) c += dfs_tail(&r, 2);
+                    else c += (o->qv == 2) ? 1 : dfs(&r, 2);
                 }
             }
         }

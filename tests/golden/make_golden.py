@@ -2,7 +2,7 @@
 path (oracle/_ref/libcgbref.so, built from the reference sources by
 oracle/Makefile).  Run in a container that holds the reference tree:
 
-    python tests/golden/make_golden.py
+    CGB_REFERENCE_TREE=/root/reference python tests/golden/make_golden.py
 
 For each workload it records what the reference computes on the seeded
 synthetic input (cgbdsm_b200/workloads.py):
@@ -38,7 +38,7 @@ from cgbdsm_b200.workloads import SPECS, materialize, write_binary_csr  # noqa: 
 from oracle import bind  # noqa: E402
 
 FULL = ["t_tiny"]
-HASHED = ["t_tiny", "t_er5", "t_er_tree", "t_er_sparse", "t_rmat"]
+HASHED = ["t_tiny", "t_er5", "t_er_tree", "t_er_sparse", "t_rmat", "c1", "c1_q25"]
 # binary CSR inputs (calig.cpp:218-323): workload -> number of vertex classes
 BINARY = {"t_er5": 4, "t_rmat": 10}
 
@@ -129,11 +129,14 @@ def main() -> None:
     bind.build(ref=True)
     if not bind.have_ref():
         raise SystemExit("oracle/_ref/libcgbref.so could not be built (reference tree absent)")
+    only = set(sys.argv[1:])  # optional: regenerate only these fixtures
     with tempfile.TemporaryDirectory() as d:
         for name in HASHED:
-            make(name, d)
+            if not only or name in only:
+                make(name, d)
         for name, nvcls in BINARY.items():
-            make_binary(name, nvcls, d)
+            if not only or f"{name}_csr" in only:
+                make_binary(name, nvcls, d)
 
 
 if __name__ == "__main__":

@@ -45,3 +45,7 @@ def test_noalloc_limits_checked_before_any_device_call():
         assert lib.cgb_merge_keys_noalloc(None, 0, p, n_ins, p, n_del, 10, p, p, None) == 4, (n_ins, n_del)
     assert lib.cgb_merge_keys_noalloc(None, 0, p, 1, p, 0, 10, None, p, None) == 1
     assert lib.cgb_merge_keys_noalloc(None, 5, p, 1, p, 0, 10, p, p, None) == 1
+    # old keys + edits beyond the tile counts the scratch holds (CGB_NOALLOC_MAX_KEYS)
+    keys = engine.NOALLOC_MAX_KEYS
+    for n_old, n_ins in ((keys, 1), (keys - 5, 6), (2**64 - 1, 1)):
+        assert lib.cgb_merge_keys_noalloc(p, n_old, p, n_ins, None, 0, 10, p, p, None) == 4, (n_old, n_ins)

@@ -21,7 +21,7 @@ from cgbdsm_b200.workloads import SPECS, materialize, read_query, write_binary_c
 from oracle import bind
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
-NAMES = ["t_tiny", "t_er5", "t_er_tree", "t_er_sparse", "t_rmat"]
+NAMES = ["t_tiny", "t_er5", "t_er_tree", "t_er_sparse", "t_rmat", "c1", "c1_q25"]
 BINARY = ["t_er5_csr", "t_rmat_csr"]
 
 

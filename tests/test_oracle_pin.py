@@ -11,7 +11,7 @@ import pytest
 from cgbdsm_b200.workloads import SPECS, materialize, read_query
 from oracle import bind
 
-PIN_CASES = ["t_tiny", "t_er5", "t_er6", "t_er_sparse", "t_er_tree"]
+PIN_CASES = ["t_tiny", "t_er5", "t_er6", "t_er_sparse", "t_er_tree", "c1", "c1_q25"]
 
 
 def _ref_or_skip():
@@ -26,9 +26,11 @@ def run_pin(name, workdir):
     qlabels, qedges = read_query(p["query"])
     glob = bind.Oracle(len(qlabels), qedges)
     per = bind.Oracle(len(qlabels), qedges)
+    tail = bind.Oracle(len(qlabels), qedges)
     init = ref.init_keys()
     glob.build(init, ref.dv_count)
     per.build(init, ref.dv_count)
+    tail.build(init, ref.dv_count)
     go = ref.global_order()
     counts = []
     while True:
@@ -40,6 +42,8 @@ def run_pin(name, workdir):
         cp = per.batch(r["dv"], r["ins"], r["del"], r["delta"], None, bind.PER_EDGE)
         assert cg == r["count"], f"{name} batch {b}: global-order restatement {cg} != reference {r['count']}"
         assert cp == r["count"], f"{name} batch {b}: per-edge restatement {cp} != reference {r['count']}"
+        ct = tail.batch(r["dv"], r["ins"], r["del"], r["delta"], None, bind.TAIL)
+        assert ct == r["count"], f"{name} batch {b}: counted-tail restatement {ct} != reference {r['count']}"
         assert per.asymmetry() == 0, f"{name} batch {b}: index lists not symmetric"
         counts.append(cp)
     # index contents after the last merge-back, compared in original vertex ids
