@@ -1,28 +1,44 @@
 #!/usr/bin/env python
-"""Headline benchmark: edge updates/sec and incremental matches/sec of the
-per-batch GPU pipeline (index update + delta lists + merged matching) on the
-R-MAT 1M-vertex / 10M-edge stream (batches of 100,000 insertions, 9-vertex
-dense pattern), with p50/p99 per-batch latency.
+"""Benchmarks: edge updates/sec and incremental matches/sec of the per-batch
+GPU pipeline, p50/p99 per-batch latency, on one B200.
 
-A step is one batch through the hot path.  The stream has 10 batches; steps
-cycle through them, rebuilding the initial index (untimed) when the cycle
-restarts, so every cycle sees identical work.
+Headline (the largest single-GPU configuration): R-MAT 4,000,000 vertices /
+34,000,000 edges, 32 labels Zipf(1.0), 3,400,000 insertions in batches of
+1,000,000, with a 7-vertex tree and a 7-vertex sparse pattern; each pattern
+has its own CaLiG index and engine (the plain one-query-per-launch pipeline),
+and a step is one batch applied to both (index update + delta lists +
+matching per pattern).  Stage 1 (the CaLiG producer that makes the keys)
+runs before timing.
 
-  value  keys already resident in HBM; time = sum of per-step device
-         intervals (CUDA events on the engine's stream), max over ranks
+  value  keys resident in HBM; step time = sum of the engines' device
+         intervals (CUDA events on the engine streams), max over ranks
   e2e    the same batches through the C-ABI call with host buffers
          (cgb_apply_batch: H2D of the keys, compute, D2H of the count)
-Stage 1 (the CaLiG producer that makes the keys) runs before timing.
+The stream has 4 batches; steps cycle through them, rebuilding the initial
+indexes (untimed) when the cycle restarts, so every cycle sees identical work.
+
+Further workloads ride in the same JSON line under "workloads" (each
+guarded: a failure there is reported and leaves the headline intact):
+  c2  R-MAT 1M/10M, 16 labels Zipf(1.2), batches of 100,000, 9-vertex dense
+      pattern, plain single-query pipeline
+  c4  the same stream with 64 registered queries (sizes 4-12; tree, sparse,
+      dense; cgbdsm_b200/data/queries_c2.json) in the multi-query engine, one
+      launch per batch, against the plain pipeline (CaLiG producer +
+      single-query engine per query) on the same batches
+  c5  the serving loop (cgbdsm_b200/serve.py) on the R-MAT 4M/34M graph
 
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-For N > 1 run under torchrun: every rank keeps a full index replica and
-applies every batch; the matching of each batch is split by seed (rank r
-expands delta edges i with i % N == r); counts are summed and step times
-maxed over ranks (NCCL).  Total work per batch is fixed: scaling "strong".
+                       [--workloads c2,c4,c5] [--quick]
+For N > 1 run under torchrun: every rank keeps full index replicas and
+applies every batch; the matching of each batch is split by seed group
+(rank r expands the groups whose key hashes to r); counts are summed and
+step times maxed over ranks (NCCL).  Total work per batch is fixed: scaling
+"strong".
 """
 from __future__ import annotations
 
 import argparse
+import hashlib
 import json
 import os
 import statistics
@@ -35,8 +51,13 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-WORKLOAD = "c2"
+HEADLINE = ["c3_tree", "c3_sparse"]
 L2_FLUSH_BYTES = 256 << 20  # > 126 MB L2
+METRIC = "edge updates/sec (and incremental matches/sec, p50/p99 batch latency) on 1 B200"
+C3_DESC = ("R-MAT 4,000,000 vertices / 34,000,000 edges, 32 labels Zipf(1.0), 3,400,000 insertions in batches "
+           "of 1,000,000, 7-vertex tree and 7-vertex sparse patterns (one engine each)")
+C2_DESC = ("R-MAT 1,000,000 vertices / 10,000,000 edges, 16 labels Zipf(1.2), 1,000,000 insertions in batches of "
+           "100,000, 9-vertex dense pattern")
 
 
 def _peaks():
@@ -48,18 +69,32 @@ def _peaks():
         return 6650.0, "fallback"
 
 
-def _profiled_traffic(kernel: str):
-    """DRAM bytes (read + write) of one launch of `kernel` on this workload, from
-    the committed ncu summary (profiles/<kernel>_rmat1m10m.md, a line
-    "traffic_bytes_per_launch: N"); None when there is no such capture."""
+def _engine_source_sha() -> str:
+    h = hashlib.sha256()
+    for f in ("engine.cu", "multiquery.cuh"):
+        with open(os.path.join(ROOT, "cgbdsm_b200", "csrc", f), "rb") as fh:
+            h.update(fh.read())
+    return h.hexdigest()[:16]
+
+
+def _profiled(kernel: str, workload: str):
+    """Per-launch DRAM bytes and L2 throughput of `kernel` from the committed
+    ncu summary profiles/<kernel>_<workload>.md, used only when the summary
+    was made from the current kernel sources (its "engine_sha16" line equals
+    the sources' hash); else (None, None, reason)."""
     import re
 
-    path = os.path.join(ROOT, "profiles", f"{kernel}_rmat1m10m.md")
+    path = os.path.join(ROOT, "profiles", f"{kernel}_{workload}.md")
     try:
-        m = re.search(r"traffic_bytes_per_launch:\s*(\d+)", open(path).read())
-        return (int(m.group(1)), os.path.relpath(path, ROOT)) if m else (None, None)
+        txt = open(path).read()
     except OSError:
-        return None, None
+        return None, None, "no ncu summary"
+    m = re.search(r"engine_sha16:\s*([0-9a-f]{16})", txt)
+    if not m or m.group(1) != _engine_source_sha():
+        return None, None, "ncu summary made from other kernel sources"
+    t = re.search(r"traffic_bytes_per_launch:\s*(\d+)", txt)
+    l2 = re.search(r"l2_throughput_pct:\s*([0-9.]+)", txt)
+    return (int(t.group(1)) if t else None), (float(l2.group(1)) if l2 else None), os.path.relpath(path, ROOT)
 
 
 class ClockSampler:
@@ -68,7 +103,7 @@ class ClockSampler:
     def __init__(self, index: int):
         self.index = index
         self.proc = None
-        self.path = os.path.join("/tmp", f"cgb_clocks_{os.getpid()}.csv")
+        self.path = os.path.join("/tmp", f"cgb_clocks_{os.getpid()}_{index}.csv")
 
     def __enter__(self):
         q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
@@ -119,184 +154,200 @@ def log(msg: str) -> None:
     print(f"[bench {time.strftime('%H:%M:%S')}] {msg}", file=sys.stderr, flush=True)
 
 
-def setup_workload(rank: int):
-    from cgbdsm_b200 import Producer
-    from cgbdsm_b200.workloads import SPECS, materialize, read_query
+def pct(values, p):
+    lat = sorted(values)
+    return lat[min(len(lat) - 1, int(round(p / 100.0 * (len(lat) - 1))))] if lat else None
 
-    spec = SPECS[WORKLOAD]
-    log(f"generating workload {spec.name}")
+
+# ---------------------------------------------------------------------------
+# plain single-query pipeline (CaLiG producer + engine per pattern)
+# ---------------------------------------------------------------------------
+def produce(spec, rank: int):
+    """Stage 1 for every batch: the product's CaLiG producer (keys, vertex counts)."""
+    from cgbdsm_b200 import Producer
+    from cgbdsm_b200.workloads import materialize, read_query
+
     paths = materialize(spec, os.environ.get("CGB_BENCH_DIR", f"/tmp/cgb_bench_r{rank}"))
-    log("stage 1 (CaLiG producer) for every batch")
     t0 = time.perf_counter()
     prod = Producer(paths["query"], paths["data"], paths["update"], spec.cli_batch_size)
     init, dv0 = prod.initial()
-    batches = [prod.next() for _ in range(prod.num_batches)]
-    s1_s = time.perf_counter() - t0
-    log(f"stage 1 done in {s1_s:.1f} s: {len(init)} initial keys, {len(batches)} batches")
+    t_init = time.perf_counter() - t0
+    batches, s1 = [], []
+    for _ in range(prod.num_batches):
+        t1 = time.perf_counter()
+        batches.append(prod.next())
+        s1.append((time.perf_counter() - t1) * 1e3)
     ql, qe = read_query(paths["query"])
     prod.close()
-    return spec, paths, ql, qe, init, dv0, batches, s1_s
+    return {"spec": spec, "paths": paths, "ql": ql, "qe": qe, "init": init, "dv0": dv0, "batches": batches,
+            "stage1_init_s": t_init, "stage1_ms": s1}
 
 
-def run_ours(args) -> None:
+def run_pipelines(names: list[str], args, rank: int, world: int, local: int, footprint: bool = True) -> dict:
+    """Plain pipeline on the patterns `names` (same graph and stream): a step is
+    one batch applied to every pattern's engine."""
     import torch
 
     from cgbdsm_b200 import Engine, dist
+    from cgbdsm_b200.engine import FLAG_FOOTPRINT
+    from cgbdsm_b200.workloads import SPECS
 
-    rank, world, local = dist.env()
-    torch.cuda.set_device(local)
-    dist.init("nccl", timeout_s=600)
+    t0 = time.perf_counter()
+    W = []
+    for n in names:
+        log(f"stage 1 (CaLiG producer) for {n}")
+        W.append(produce(SPECS[n], rank))
+    setup_s = time.perf_counter() - t0
+    nb = len(W[0]["batches"])
+    dev = f"cuda:{local}"
 
-    spec, paths, ql, qe, init, dv0, batches, s1_s = setup_workload(rank)
-    nb = len(batches)
-
-    def new_engine():
-        e = Engine(device=local, dfs_budget_ms=args.budget_ms, shard_index=rank, num_shards=world)
-        e.load_query(len(ql), qe, ql)
-        e.build_index(init, dv0)
+    def new_engine(w, flags=0):
+        e = Engine(device=local, dfs_budget_ms=args.budget_ms, shard_index=rank, num_shards=world, flags=flags)
+        e.load_query(len(w["ql"]), w["qe"], w["ql"])
+        e.build_index(w["init"], w["dv0"])
         return e
 
-    # device-resident keys per batch: [ins | del | delta]
-    dev = []
-    for b in batches:
-        cat = np.concatenate([b["ins"], b["del"], b["delta"]]).view(np.int64)
-        t = torch.from_numpy(cat).to(f"cuda:{local}")
-        dev.append((t, len(b["ins"]), len(b["del"]), len(b["delta"])))
-    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.int32, device=f"cuda:{local}")
+    # device-resident keys per pattern and batch: [ins | del | delta]
+    dkeys = []
+    for w in W:
+        row = []
+        for b in w["batches"]:
+            cat = np.concatenate([b["ins"], b["del"], b["delta"]]).view(np.int64)
+            row.append((torch.from_numpy(cat).to(dev), len(b["ins"]), len(b["del"]), len(b["delta"])))
+        dkeys.append(row)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.int32, device=dev)
     torch.cuda.synchronize()
+    state = {"eng": [new_engine(w) for w in W], "pos": 0}
 
-    eng = new_engine()
-    state = {"eng": eng, "pos": 0}
+    def restart():
+        for e in state["eng"]:
+            e.close()
+        state["eng"] = [new_engine(w) for w in W]
+        state["pos"] = 0
 
     def one_step(device_keys: bool):
-        if state["pos"] == nb:  # restart the stream: fresh index (untimed)
-            state["eng"].close()
-            state["eng"] = new_engine()
-            state["pos"] = 0
+        if state["pos"] == nb:  # restart the stream: fresh indexes (untimed)
+            restart()
         b = state["pos"]
-        e = state["eng"]
-        l0 = e.kernel_launches()
-        if device_keys:
-            flush.zero_()  # evict L2 between steps (outside the engine's timed interval)
+        rec = {"batch": b, "ms": 0.0, "count": 0, "phase": np.zeros(3), "launches": 0, "stats": []}
+        for k, (w, e) in enumerate(zip(W, state["eng"])):
+            l0 = e.kernel_launches()
+            flush.zero_()  # evict L2 before each engine's batch (outside its timed interval)
             torch.cuda.synchronize()
-            t, ni, nd, nD = dev[b]
-            base = t.data_ptr()
-            c = e.apply_batch_device(batches[b]["dv"], base, ni, base + 8 * ni, nd, base + 8 * (ni + nd), nD)
-            ms = float(e.timings()[3])
-        else:
-            bb = batches[b]
-            t0 = time.perf_counter()
-            c = e.apply_batch(bb["dv"], bb["ins"], bb["del"], bb["delta"], bb["edge_ok"])
-            ms = (time.perf_counter() - t0) * 1e3
-        tm = e.timings()
-        st = e.stats()
-        st["launches"] = e.kernel_launches() - l0
+            if device_keys:
+                t, ni, nd, nD = dkeys[k][b]
+                base = t.data_ptr()
+                c = e.apply_batch_device(w["batches"][b]["dv"], base, ni, base + 8 * ni, nd, base + 8 * (ni + nd), nD)
+                ms = float(e.timings()[3])
+            else:
+                bb = w["batches"][b]
+                t1 = time.perf_counter()
+                c = e.apply_batch(bb["dv"], bb["ins"], bb["del"], bb["delta"], bb["edge_ok"])
+                ms = (time.perf_counter() - t1) * 1e3
+            tm = e.timings()
+            rec["ms"] += ms
+            rec["count"] = (rec["count"] + c) % (1 << 64)
+            rec["phase"] += np.array([float(x) for x in tm[:3]])
+            rec["launches"] += e.kernel_launches() - l0
+            rec["stats"].append(e.stats())
         state["pos"] += 1
-        log(f"batch {b} ({'device' if device_keys else 'host'} keys): {ms:.1f} ms, count {c}, "
-            f"phases {[round(float(x), 2) for x in tm[:3]]}")
-        return b, c, ms, tm, st
+        log(f"batch {b} ({'device' if device_keys else 'host'} keys): {rec['ms']:.1f} ms, count {rec['count']}, "
+            f"phases {[round(x, 2) for x in rec['phase']]}")
+        return rec
 
     for _ in range(args.warmup):
         one_step(True)
     dist.barrier()
     torch.cuda.synchronize()
-    recs = []
     with ClockSampler(local) as clk:
-        for _ in range(args.steps):
-            recs.append(one_step(True))
+        recs = [one_step(True) for _ in range(args.steps)]
     torch.cuda.synchronize()
     dist.barrier()
-    launches = sum(r[4]["launches"] for r in recs)
-
-    step_ms = dist.max_values([r[2] for r in recs])          # max over ranks, per step
-    counts = dist.sum_counts([int(r[1]) for r in recs])       # shard counts summed, per step
+    step_ms = dist.max_values([r["ms"] for r in recs])
+    counts = dist.sum_counts([r["count"] for r in recs])
     total_ms = sum(step_ms)
-    edges = sum(batches[r[0]]["num_edges"] for r in recs)     # every rank sees the same batches
-    matches = sum(counts)
+    edges = sum(W[0]["batches"][r["batch"]]["num_edges"] for r in recs)
 
-    # e2e through the host-buffer C-ABI call (same batches, same cycle)
-    state["eng"].close()
-    state["eng"] = new_engine()
-    state["pos"] = 0
+    restart()
     if args.quick:
         e2e_recs = recs
     else:
         for _ in range(args.warmup):
             one_step(False)
         e2e_recs = [one_step(False) for _ in range(args.steps)]
-    e2e_ms = sum(dist.max_values([r[2] for r in e2e_recs]))
-    e2e_edges = sum(batches[r[0]]["num_edges"] for r in e2e_recs)
-    h2d = sum(8 * (len(batches[r[0]]["ins"]) + len(batches[r[0]]["del"]) + len(batches[r[0]]["delta"]))
-              + len(batches[r[0]]["edge_ok"]) for r in e2e_recs) / len(e2e_recs)
+    e2e_ms = sum(dist.max_values([r["ms"] for r in e2e_recs]))
+    e2e_edges = sum(W[0]["batches"][r["batch"]]["num_edges"] for r in e2e_recs)
+    h2d = sum(sum(8 * (len(w["batches"][r["batch"]]["ins"]) + len(w["batches"][r["batch"]]["del"])
+                       + len(w["batches"][r["batch"]]["delta"])) + len(w["batches"][r["batch"]]["edge_ok"])
+                  for w in W) for r in e2e_recs) / len(e2e_recs)
 
-    # roofline of the dominant kernel (by time over the timed steps)
-    match_ms = sum(float(r[3][2]) for r in recs)
-    upd_ms = sum(float(r[3][0]) for r in recs)
-    match_bytes = sum(r[4]["match_bytes"] for r in recs)
-    upd_bytes = sum(r[4]["update_bytes"] for r in recs)
-    peak, peak_kind = _peaks()
-    if match_ms >= upd_ms:
-        kname, kbytes, kms = "k_dfs_count (matching)", match_bytes, match_ms
-    else:
-        kname, kbytes, kms = "k_merge_runs (index update)", upd_bytes, upd_ms
-    traffic, traffic_src = _profiled_traffic(kname.split()[0])
-    achieved = (kbytes / 1e9) / (kms / 1e3) if kms > 0 else 0.0
-    upd_achieved = (upd_bytes / 1e9) / (upd_ms / 1e3) if upd_ms > 0 else 0.0
-    lat = sorted(step_ms)
-
-    def pct(p):
-        return lat[min(len(lat) - 1, int(round(p / 100.0 * (len(lat) - 1))))]
-
-    line = {
-        "metric": "edge updates/sec (and incremental matches/sec, p50/p99 batch latency) on 1 B200",
+    # roofline: the dominant kernel by device time over the timed steps
+    match_ms = sum(r["phase"][2] for r in recs)
+    upd_ms = sum(r["phase"][0] for r in recs)
+    upd_bytes = sum(st["update_bytes"] for r in recs for st in r["stats"])
+    out = {
         "value": edges / (total_ms / 1e3) if total_ms > 0 else 0.0,
-        "unit": "edge updates/s",
-        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": total_ms / max(1, len(recs)),
-        "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
-        "dtype": "u32/u64 integer", "data": "synthetic (seeded R-MAT stand-in for the public graphs)",
-        "config": {"workload": "R-MAT 1,000,000 vertices / 10,000,000 edges, 16 labels Zipf(1.2), "
-                               "1,000,000 insertions in batches of 100,000, 9-vertex dense pattern",
-                   "batch_edges": spec.batch_edges, "batches_in_stream": nb,
-                   "query_vertices": len(ql), "query_edges": len(qe),
-                   "l2": "flushed between steps (256 MiB write)",
-                   "parallelism": f"{world} GPU(s): index replicated, seeds sharded"},
-        "matches_per_s": matches / (total_ms / 1e3) if total_ms > 0 else 0.0,
-        "matches_per_batch": matches / max(1, len(recs)),
-        "latency_ms": {"p50": pct(50), "p99": pct(99), "max": lat[-1]},
+        "matches_per_s": sum(counts) / (total_ms / 1e3) if total_ms > 0 else 0.0,
+        "matches_per_batch": sum(counts) / max(1, len(recs)),
+        "latency_ms": {"p50": pct(step_ms, 50), "p99": pct(step_ms, 99), "max": max(step_ms)},
         "phase_ms_per_step": {"index_update": upd_ms / len(recs),
-                              "delta_lists": sum(float(r[3][1]) for r in recs) / len(recs),
+                              "delta_lists": sum(r["phase"][1] for r in recs) / len(recs),
                               "matching": match_ms / len(recs)},
-        "work_per_step": {k: sum(r[4][k] for r in recs) / len(recs)
-                          for k in ("seeds", "chunks", "tested", "tails", "stolen_tasks", "touched_runs")},
         "e2e": {"value": e2e_edges / (e2e_ms / 1e3) if e2e_ms > 0 else 0.0, "unit": "edge updates/s",
-                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": 8 * (4 + 16 + 8)},
-        "gpu_launches": launches,
-        "roofline": {"kernel": kname, "bound": "hbm", "achieved": achieved, "peak": peak,
-                     "unit": "GB/s", "frac": achieved / peak if peak else None, "peak_source": peak_kind,
-                     "algorithmic_bytes_per_step": kbytes / len(recs), "traffic": traffic,
-                     "traffic_source": traffic_src,
-                     "index_update_achieved_gbs": upd_achieved},
+                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": 8 * (4 + 16 + 8) * len(W)},
+        "gpu_launches": sum(r["launches"] for r in recs),
+        "batches_in_stream": nb,
+        "patterns": [{"name": w["spec"].name, "query_vertices": len(w["ql"]), "query_edges": len(w["qe"]),
+                      "stage1_init_s": round(w["stage1_init_s"], 2),
+                      "stage1_ms_per_batch": round(float(np.mean(w["stage1_ms"])), 2)} for w in W],
+        "setup_s": round(setup_s, 1),
         "clocks": clk.summary(),
-        "stage1_setup_s": round(s1_s, 2),
     }
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        from oracle import bind
+    peak, peak_kind = _peaks()
+    upd_gbs = (upd_bytes / 1e9) / (upd_ms / 1e3) if upd_ms > 0 else 0.0
+    if footprint and match_ms >= upd_ms:
+        # matching footprint: one untimed run of each pattern on batch 0 with
+        # the record bit set on (bytes of the distinct records and lists resolved)
+        fp_bytes, fp_ms = 0, 0.0
+        for k, w in enumerate(W):
+            e = new_engine(w, FLAG_FOOTPRINT)
+            t, ni, nd, nD = dkeys[k][0]
+            base = t.data_ptr()
+            e.apply_batch_device(w["batches"][0]["dv"], base, ni, base + 8 * ni, nd, base + 8 * (ni + nd), nD)
+            fp_bytes += e.stats()["match_bytes"]
+            e.close()
+            fp_ms += float(np.mean([r["phase"][2] for r in recs if r["batch"] == 0] or [match_ms / len(recs)]))
+        achieved = (fp_bytes / 1e9) / (fp_ms / 1e3) if fp_ms > 0 else 0.0
+        kname = "k_dfs_count"
+        traffic, l2pct, src = _profiled(kname, names[0])
+        out["roofline"] = {"kernel": f"{kname} (matching)", "bound": "hbm", "achieved": achieved, "peak": peak,
+                           "unit": "GB/s", "frac": achieved / peak if peak else None, "peak_source": peak_kind,
+                           "algorithmic_bytes": "footprint: 16 B per distinct record resolved + 4 B per entry of "
+                                                "its old and delta lists, batch 0",
+                           "algorithmic_bytes_per_launch": fp_bytes, "traffic": traffic, "traffic_source": src,
+                           "l2_throughput_pct_ncu": l2pct, "index_update_achieved_gbs": upd_gbs,
+                           "index_update_frac": upd_gbs / peak if peak else None}
+    else:
+        traffic, l2pct, src = _profiled("k_merge_runs", names[0])
+        out["roofline"] = {"kernel": "k_merge_runs / k_merge_big (index update)", "bound": "hbm",
+                           "achieved": upd_gbs, "peak": peak, "unit": "GB/s",
+                           "frac": upd_gbs / peak if peak else None, "peak_source": peak_kind,
+                           "algorithmic_bytes": "8 B per edit + 4 B per old and new run word + 32 B per record",
+                           "algorithmic_bytes_per_step": upd_bytes / len(recs), "traffic": traffic,
+                           "traffic_source": src}
+    for e in state["eng"]:
+        e.close()
+    out["_W"] = W
+    return out
 
-        if bind.have_ref():
-            log("cpu baseline: reference CPU path on batch 0")
-            line["cpu_baseline"] = reference_sample(paths, spec, args.cpu_budget_s, batches)
-        else:
-            line["cpu_baseline"] = {"unavailable": "oracle/_ref/libcgbref.so was not built (no reference tree)"}
-    if rank == 0:
-        print(json.dumps(line), flush=True)
-    state["eng"].close()
-    dist.finish()
 
-
-def reference_sample(paths, spec, budget_s: float, batches=None) -> dict:
+# ---------------------------------------------------------------------------
+# reference CPU path (oracle/_ref): cpu_baseline and the reference arm
+# ---------------------------------------------------------------------------
+def reference_sample(paths, spec, budget_s: float) -> dict:
     """The reference's own CPU path (oracle/_ref: CaLiG + staging + CPUIndexMirror +
-    cpu_dfs) on batch 0 of the same stream with all host threads.  Stage 1,
+    cpu_dfs) on batch 0 of the stream with all host threads.  Stage 1,
     staging and the index mirror update run fully; the count (the reference
     enumerates every embedding, mask-free seeding) runs for budget_s in a
     supervised child process and is extrapolated by rows counted / rows total.
@@ -314,15 +365,102 @@ def reference_sample(paths, spec, budget_s: float, batches=None) -> dict:
         count_ms, kind = r["count_ms"] * r["rows_total"] / r["rows_done"], "extrapolated"
     else:
         count_ms, kind = r["count_ms"] * max(1, r["rows_total"]), "lower bound (no row finished)"
-    batch_ms = fixed_ms + count_ms
-    value = spec.batch_edges / (batch_ms / 1e3) if batch_ms > 0 else 0.0
-    return {"value": value, "unit": "edge updates/s", "cores": threads, "kind": "reference",
-            "sample": (f"batch 0 of the stream: Stage 1 {r['s1_ms']:.0f} ms + staging {r['staging_ms']:.0f} ms + "
-                       f"index mirror {r['mirror_ms']:.0f} ms measured; mask-free cpu_dfs count: "
-                       f"{r['rows_done']} of {r['rows_total']} seed rows in {r['count_ms']/1e3:.1f} s, "
-                       f"count time {kind}: {count_ms/1e3:.3g} s"
-                       + ("; value is an upper bound" if kind.startswith("lower") else "")),
-            "stage1_ms": r["s1_ms"], "count_time_kind": kind, "wall_s": round(r["wall_s"], 1)}
+    return {"batch_ms": fixed_ms + count_ms, "threads": threads, "kind": kind, "r": r, "count_ms": count_ms,
+            "spec": spec.name}
+
+
+def reference_line(names: list[str], budget_s: float, workdir: str) -> dict:
+    from cgbdsm_b200.workloads import SPECS, materialize
+
+    parts = []
+    for n in names:
+        spec = SPECS[n]
+        parts.append(reference_sample(materialize(spec, workdir), spec, budget_s))
+    spec0 = SPECS[names[0]]
+    batch_ms = sum(p["batch_ms"] for p in parts)
+    value = spec0.batch_edges / (batch_ms / 1e3) if batch_ms > 0 else 0.0
+    sample = "; ".join(
+        f"{p['spec']} batch 0: Stage 1 {p['r']['s1_ms']:.0f} ms + staging {p['r']['staging_ms']:.0f} ms + index "
+        f"mirror {p['r']['mirror_ms']:.0f} ms measured, mask-free cpu_dfs count {p['r']['rows_done']} of "
+        f"{p['r']['rows_total']} seed rows in {p['r']['count_ms'] / 1e3:.1f} s, count time {p['kind']}: "
+        f"{p['count_ms'] / 1e3:.3g} s" for p in parts)
+    return {"value": value, "unit": "edge updates/s", "cores": parts[0]["threads"], "kind": "reference",
+            "sample": sample + ("; value is an upper bound" if any(p["kind"].startswith("lower") for p in parts)
+                                else ""),
+            "count_time_kind": sorted(set(p["kind"] for p in parts))}
+
+
+# ---------------------------------------------------------------------------
+# extra workloads
+# ---------------------------------------------------------------------------
+def bench_c2(args, rank, world, local) -> dict:
+    r = run_pipelines(["c2"], args, rank, world, local)
+    r.pop("_W")
+    r["config"] = {"workload": C2_DESC}
+    r["unit"] = "edge updates/s"
+    return r
+
+
+def bench_c4(args, rank, world, local) -> dict:
+    from cgbdsm_b200 import multiq
+
+    return multiq.bench(args, local, log)
+
+
+def bench_c5(args, rank, world, local) -> dict:
+    from cgbdsm_b200 import serve
+
+    return serve.bench(args, local, log)
+
+
+def run_ours(args) -> None:
+    import torch
+
+    from cgbdsm_b200 import dist
+
+    rank, world, local = dist.env()
+    torch.cuda.set_device(local)
+    dist.init("nccl", timeout_s=900)
+    head = run_pipelines(HEADLINE, args, rank, world, local)
+    W = head.pop("_W")
+    line = {
+        "metric": METRIC, "value": head.pop("value"), "unit": "edge updates/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": head.pop("ms_per_step"),
+        "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+        "dtype": "u32/u64 integer", "data": "synthetic (seeded R-MAT stand-in for the public graphs)",
+        "config": {"workload": C3_DESC, "batch_edges": W[0]["spec"].batch_edges,
+                   "batches_in_stream": head.pop("batches_in_stream"), "patterns": head.pop("patterns"),
+                   "l2": "flushed before every engine call (256 MiB write); index > 126 MB L2",
+                   "parallelism": f"{world} GPU(s): index replicated, seed groups sharded"},
+    }
+    line.update(head)
+    line["stage1_setup_s"] = line.pop("setup_s")
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from oracle import bind
+
+        if bind.have_ref():
+            log("cpu baseline: reference CPU path on batch 0 of each pattern")
+            line["cpu_baseline"] = reference_line(HEADLINE, args.cpu_budget_s,
+                                                  os.environ.get("CGB_BENCH_DIR", "/tmp/cgb_bench_r0"))
+        else:
+            line["cpu_baseline"] = {"unavailable": "oracle/_ref/libcgbref.so was not built (no reference tree)"}
+    extras = {}
+    for name in [w for w in args.workloads.split(",") if w] if world == 1 else []:
+        fn = {"c2": bench_c2, "c4": bench_c4, "c5": bench_c5}.get(name)
+        if fn is None:
+            continue
+        log(f"workload {name}")
+        try:
+            extras[name] = fn(args, rank, world, local)
+        except Exception as e:  # reported, the headline stands
+            extras[name] = {"error": f"{type(e).__name__}: {e}"}
+            log(f"workload {name} failed: {e}")
+        torch.cuda.synchronize()
+    if extras:
+        line["workloads"] = extras
+    if rank == 0:
+        print(json.dumps(line, default=float), flush=True)
+    dist.finish()
 
 
 def run_reference(args) -> None:
@@ -330,33 +468,28 @@ def run_reference(args) -> None:
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    from cgbdsm_b200.workloads import SPECS, materialize
-
-    spec = SPECS[WORKLOAD]
-    paths = materialize(spec, os.environ.get("CGB_BENCH_DIR", "/tmp/cgb_bench_r0"))
     from oracle import bind
 
     if not bind.have_ref():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libcgbref.so was not built"}))
         return
-    vals = []
-    cb = None
+    workdir = os.environ.get("CGB_BENCH_DIR", "/tmp/cgb_bench_r0")
+    vals, cb = [], None
     per_step_budget = max(2.0, min(args.cpu_budget_s, 150.0 / max(1, args.steps + args.warmup)))
     for i in range(args.warmup + args.steps):
-        cb = reference_sample(paths, spec, per_step_budget)
+        cb = reference_line(HEADLINE, per_step_budget, workdir)
         if i >= args.warmup:
             vals.append(cb["value"])
     v = statistics.median(vals) if vals else 0.0
     cb["value"] = v
+    from cgbdsm_b200.workloads import SPECS
+
     print(json.dumps({
-        "impl": "reference",
-        "metric": "edge updates/sec (and incremental matches/sec, p50/p99 batch latency) on 1 B200",
-        "value": v, "unit": "edge updates/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": (spec.batch_edges / v * 1e3) if v else None, "higher_is_better": True, "scaling": "strong",
-        "vs_baseline": None, "dtype": "u32/u64 integer", "data": "synthetic (seeded R-MAT)",
-        "config": {"workload": "R-MAT 1,000,000 vertices / 10,000,000 edges, 16 labels Zipf(1.2), "
-                               "1,000,000 insertions in batches of 100,000, 9-vertex dense pattern"},
-        "cpu_baseline": cb,
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "edge updates/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": (SPECS[HEADLINE[0]].batch_edges / v * 1e3) if v else None, "higher_is_better": True,
+        "scaling": "strong", "vs_baseline": None, "dtype": "u32/u64 integer", "data": "synthetic (seeded R-MAT)",
+        "config": {"workload": C3_DESC}, "cpu_baseline": cb,
         "e2e": {"value": v, "unit": "edge updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }), flush=True)
 
@@ -368,13 +501,15 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--budget-ms", type=int, default=120000, help="matching time budget per batch")
-    ap.add_argument("--cpu-budget-s", type=float, default=15.0)
+    ap.add_argument("--cpu-budget-s", type=float, default=8.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workloads", default="c2,c4,c5", help="further workloads in the same JSON line")
     ap.add_argument("--quick", action="store_true",
-                    help="profiling run: 1 warm-up + 1 step, no e2e leg, no CPU baseline (not a benchmark)")
+                    help="profiling run: 1 warm-up + 1 step, no e2e leg, no CPU baseline, no further workloads "
+                         "(not a benchmark)")
     args = ap.parse_args()
     if args.quick:
-        args.steps, args.warmup, args.no_cpu_baseline = 1, 1, True
+        args.steps, args.warmup, args.no_cpu_baseline, args.workloads = 1, 1, True, ""
     elif args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":

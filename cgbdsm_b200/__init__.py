@@ -3,4 +3,4 @@
 Native code lives in libcgbdsm.so (C ABI: include/cgbdsm.h); this package
 holds the build script, a ctypes binding and the synthetic workloads.
 """
-from .engine import CgbError, Engine, Gpma, MultiQuery, Producer, load_library  # noqa: F401
+from .engine import CgbError, Engine, Gpma, MultiQuery, Producer, Server, load_library  # noqa: F401

@@ -24,7 +24,7 @@ CXX = "/usr/bin/g++"  # system compiler: dynamic libstdc++ (safe to load into Py
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 ENGINE_CU = ["engine.cu", "noalloc.cu", "gpma.cu"]
-ENGINE_CPP = ["query.cpp", "calig.cpp", "pipeline.cpp"]
+ENGINE_CPP = ["query.cpp", "calig.cpp", "pipeline.cpp", "server.cpp"]
 GEN_CPP = ["gen.cpp"]
 
 

@@ -612,7 +612,23 @@ struct DfsArgs {
     uint32_t rb_words;
     const EdgePlan* plans;       // k_dfs_count<true>: every registered query's plans
     const unsigned int* epoch_ptr;  // non-null: the launch tag is read here (k_epoch_bump)
+    uint32_t* touched;           // footprint runs: bit per record resolved (nullptr: off)
 };
+
+// Footprint of a matching launch: the bytes of every distinct record it
+// resolved (16 B) and of that record's whole old and delta lists (4 B per
+// entry), each counted once.  Added to *out.
+__global__ void k_footprint(const uint4* __restrict__ rec, uint64_t n, const uint32_t* __restrict__ touched,
+                            unsigned long long* out) {
+    unsigned long long b = 0;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        if ((touched[i >> 5] >> (i & 31)) & 1u) {
+            const uint4 r = rec[i];
+            b += 16ull + 4ull * ((unsigned long long)r.y + r.w);
+        }
+    for (int o = 16; o > 0; o >>= 1) b += __shfl_xor_sync(kFull, b, o);
+    if ((threadIdx.x & 31) == 0 && b) atomicAdd(out, b);
+}
 
 // Next launch tag for a DFS launch that reads it from memory; the low 20
 // bits (the tag's epoch field) are never 0.
@@ -658,13 +674,17 @@ __device__ __forceinline__ bool list_contains(const uint32_t* __restrict__ pool,
 // Bit sets of the long old runs (rebuilt each batch): slot[(dir, vertex)]
 // names a bit set over the compressed ids, or kNoSlot; a warp keeps the slot
 // of every resolved record bn[k] in bslot[k].  slot == nullptr: none.
+// touched (non-null in footprint runs): one bit per record, set for every
+// record the matching resolves.
 struct RunBits {
     const uint32_t* slot;
     const uint32_t* bits;
     uint32_t words;
     uint32_t* bslot;
+    uint32_t* touched;
     __device__ __forceinline__ void note(uint32_t k, size_t at) const {
         if (slot) bslot[k] = __ldg(slot + at);
+        if (touched) atomicOr(touched + (at >> 5), 1u << (at & 31));
     }
     // x in the resolved list bn[k] = r: one bit test for a long old run
     __device__ __forceinline__ bool has(uint32_t k, const uint4& r, const uint32_t* __restrict__ pool,
@@ -1114,7 +1134,7 @@ __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
     const uint64_t vmask = (1ull << a.B) - 1ull;
     uint32_t* m = s_m[w];
     uint4* bn = s_bn[w];
-    const RunBits rb{a.rb_slot, a.rb_bits, a.rb_words, s_rbs[w]};
+    const RunBits rb{a.rb_slot, a.rb_bits, a.rb_words, s_rbs[w], a.touched};
     volatile unsigned int* vq = a.qctr;  // [0] tasks reserved, [1] tickets issued, [3] completed, [6] seeds
 
     // per-depth state held by lane == depth
@@ -1240,7 +1260,9 @@ __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
         const bool has_tail = nc < P.n;
         SeedGroup X{nullptr, 0u, kNoVertex};
         if (P.grouped) {
-            const uint4 xr = a.rec[(size_t)P.seed_dir * a.dvcap + m[0]];
+            const size_t xat = (size_t)P.seed_dir * a.dvcap + m[0];
+            const uint4 xr = a.rec[xat];
+            if (a.touched && lane == 0) atomicOr(a.touched + (xat >> 5), 1u << (xat & 31));
             X.x = a.dval + xr.z;
             X.n = xr.w;
             if (X.n <= 32 && lane < X.n) X.xv = __ldg(X.x + lane);
@@ -1722,6 +1744,7 @@ struct cgb_handle {
     bool rb_valid = false;             // slot table and bit sets match the index
     uint32_t rb_min_len = kRunBitsMinLen;
     uint8_t* d_rev = nullptr;          // reverse direction of each direction
+    uint32_t* d_touched = nullptr; size_t touched_cap = 0;  // footprint runs: record bit set
 
     // label-keyed mode (the multi-query engine's data-graph index): the
     // "direction" of a key is the label of its target vertex, the delta keys
@@ -2134,7 +2157,7 @@ void cgb_destroy(cgb_handle* h) {
                     h->d_dkeys, h->d_dkeys_alt, h->d_dval, h->d_ddu, h->d_drun_du, h->d_drun_len, h->d_drun_off,
                     h->d_seed, h->d_counts, h->d_stats, h->d_tasks, h->d_qctr, h->d_temp, h->d_qe_dirs, h->d_edge_ok,
                     h->d_vb, h->d_rb_slot, h->d_rb_sel, h->d_rb_bits, h->d_rb_ctr, h->d_rb_new, h->d_small_runs,
-                    h->d_big_runs, h->d_list_ctr, h->d_rev};
+                    h->d_big_runs, h->d_list_ctr, h->d_rev, h->d_touched};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (h->h_scal) cudaFreeHost(h->h_scal);
@@ -2364,6 +2387,14 @@ cgb_status cgb_apply_batch_device(cgb_handle* h, uint32_t dv_count, const uint64
         da.rb_words = h->rb_words;
         da.plans = nullptr;
         da.epoch_ptr = nullptr;
+        da.touched = nullptr;
+        const bool footprint = (h->cfg.flags & CGB_FLAG_FOOTPRINT) != 0;
+        const uint64_t nrec = (uint64_t)h->nd * h->dvcap;
+        if (footprint) {
+            if ((s = grow(h, h->d_touched, h->touched_cap, (size_t)(nrec + 31) / 32)) != CGB_OK) return s;
+            CK(cudaMemsetAsync(h->d_touched, 0, ((nrec + 31) / 32) * sizeof(uint32_t), h->stream));
+            da.touched = h->d_touched;
+        }
         da.budget_ns = h->cfg.dfs_budget_ms ? (unsigned long long)h->cfg.dfs_budget_ms * 1000000ull
                                             : 600ull * 1000000000ull;
         // persistent grid: exactly the blocks that can be resident at once
@@ -2378,6 +2409,11 @@ cgb_status cgb_apply_batch_device(cgb_handle* h, uint32_t dv_count, const uint64
         LAUNCHED();
         CK(cudaGetLastError());
         CK(cudaEventRecord(h->ev[3], h->stream));
+        if (footprint) {  // stats[4] := the launch's footprint (bytes of distinct records and lists)
+            CK(cudaMemsetAsync(h->d_stats + 4, 0, sizeof(unsigned long long), h->stream));
+            k_footprint<<<grid_for(h, nrec), 256, 0, h->stream>>>(h->rec, nrec, h->d_touched, h->d_stats + 4);
+            LAUNCHED();
+        }
 
         // 4. clear delta records; this delta becomes the pending merge-back
         k_delta_recs<<<grid_for(h, n_delta), 256, 0, h->stream>>>(h->rec, h->dvcap, h->d_drun_du, h->d_drun_len,

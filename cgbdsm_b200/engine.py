@@ -35,6 +35,9 @@ EXPORTS = [
     "cgb_mq_register_query", "cgb_mq_unregister_query", "cgb_mq_apply_batch", "cgb_mq_apply_batch_device",
     "cgb_mq_last_timings", "cgb_mq_last_stats", "cgb_mq_query_info", "cgb_mq_schedule", "cgb_mq_kernel_launches",
     "cgb_mq_stream",
+    "cgb_server_default_config", "cgb_server_create", "cgb_server_destroy", "cgb_server_last_error",
+    "cgb_server_submit_batch", "cgb_server_submit_register", "cgb_server_submit_unregister", "cgb_server_wait",
+    "cgb_server_stats",
 ]
 
 # Edits one cgb_merge_keys_noalloc call accepts (CGB_NOALLOC_MAX_EDITS), and
@@ -64,6 +67,7 @@ FLAG_VALID_BITS = 0x40
 FLAG_MASK_PRUNE = 0x80
 FLAG_NO_SEED_GROUPS = 0x100
 FLAG_NO_RUN_BITS = 0x200
+FLAG_FOOTPRINT = 0x400
 
 
 class MqConfig(ctypes.Structure):
@@ -75,6 +79,19 @@ MQ_FLAG_NO_AUTOTUNE = 0x1
 MQ_FLAG_NO_GRAPH = 0x2
 MQ_FLAG_NO_RUN_BITS = 0x4
 MQ_MAX_QUERIES = 256
+
+
+class ServerConfig(ctypes.Structure):
+    _fields_ = [("mq", MqConfig), ("hbm_budget_bytes", _u64), ("staging_bytes", _u64), ("max_pending", _u32)]
+
+
+class ServerResult(ctypes.Structure):
+    _fields_ = [("ticket", _u64), ("kind", _u32), ("status", ctypes.c_int32), ("query_id", _u32),
+                ("live_queries", _u32), ("t_submit_ms", ctypes.c_double), ("t_staged_ms", ctypes.c_double),
+                ("t_start_ms", ctypes.c_double), ("t_done_ms", ctypes.c_double), ("device_ms", ctypes.c_float)]
+
+
+SERVER_BATCH, SERVER_REGISTER, SERVER_UNREGISTER = 0, 1, 2
 
 
 class BatchKeys(ctypes.Structure):
@@ -158,6 +175,16 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.cgb_mq_kernel_launches.restype = _u64
     lib.cgb_mq_stream.argtypes = [_vp]
     lib.cgb_mq_stream.restype = _vp
+    lib.cgb_server_default_config.argtypes = [ctypes.POINTER(ServerConfig)]
+    lib.cgb_server_create.argtypes = [ctypes.POINTER(ServerConfig), _u32, _vp, _u64, _vp, ctypes.POINTER(_vp)]
+    lib.cgb_server_destroy.argtypes = [_vp]
+    lib.cgb_server_last_error.argtypes = [_vp]
+    lib.cgb_server_last_error.restype = ctypes.c_char_p
+    lib.cgb_server_submit_batch.argtypes = [_vp, _vp, _u64, _vp, _u64, ctypes.POINTER(_u64)]
+    lib.cgb_server_submit_register.argtypes = [_vp, _u32, _vp, _u32, _vp, ctypes.POINTER(_u64)]
+    lib.cgb_server_submit_unregister.argtypes = [_vp, _u32, ctypes.POINTER(_u64)]
+    lib.cgb_server_wait.argtypes = [_vp, _u64, _u32, ctypes.POINTER(ServerResult), _vp, _vp, _u32]
+    lib.cgb_server_stats.argtypes = [_vp, _vp]
     for name in EXPORTS:
         getattr(lib, name)
     _lib_handle = lib
@@ -533,3 +560,88 @@ class MultiQuery:
 
     def stream(self) -> int:
         return int(self.lib.cgb_mq_stream(self.h) or 0)
+
+
+class Server:
+    """Serving loop (cgb_server_*): graph, index and queries resident on the
+    device; update batches and query registrations submitted from any thread,
+    applied in submission order, results collected per ticket."""
+
+    def __init__(self, labels, edges, device: int = 0, hbm_budget_bytes: int = 0, staging_bytes: int = 0,
+                 max_pending: int = 0, mq_flags: int = 0, dfs_budget_ms: int = 0):
+        self.lib = load_library()
+        cfg = ServerConfig()
+        self.lib.cgb_server_default_config(ctypes.byref(cfg))
+        cfg.mq.device = device
+        cfg.mq.flags = mq_flags
+        cfg.mq.dfs_budget_ms = dfs_budget_ms
+        cfg.hbm_budget_bytes = hbm_budget_bytes
+        cfg.staging_bytes = staging_bytes
+        cfg.max_pending = max_pending
+        lab = np.ascontiguousarray(labels, dtype=np.uint32)
+        e = _pairs(edges)
+        h = _vp()
+        st = self.lib.cgb_server_create(ctypes.byref(cfg), len(lab), lab.ctypes.data, len(e),
+                                        e.ctypes.data if len(e) else None, ctypes.byref(h))
+        self.h = h.value
+        if st != 0:
+            msg = self.lib.cgb_server_last_error(self.h).decode() if self.h else ""
+            self.close()
+            raise CgbError(st, msg)
+
+    def _check(self, st: int) -> None:
+        if st != 0:
+            raise CgbError(st, self.lib.cgb_server_last_error(self.h).decode())
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.lib.cgb_server_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def submit_batch(self, ins=None, dele=None) -> int:
+        ins = _pairs(ins if ins is not None else np.zeros((0, 2)))
+        dele = _pairs(dele if dele is not None else np.zeros((0, 2)))
+        t = _u64(0)
+        self._check(self.lib.cgb_server_submit_batch(self.h, ins.ctypes.data if len(ins) else None, len(ins),
+                                                     dele.ctypes.data if len(dele) else None, len(dele),
+                                                     ctypes.byref(t)))
+        return t.value
+
+    def submit_register(self, qv: int, edges, labels) -> int:
+        e = np.ascontiguousarray(np.asarray(edges, dtype=np.uint32).reshape(-1))
+        lab = np.ascontiguousarray(labels, dtype=np.uint32)
+        t = _u64(0)
+        self._check(self.lib.cgb_server_submit_register(self.h, qv, lab.ctypes.data, len(e) // 2, e.ctypes.data,
+                                                        ctypes.byref(t)))
+        return t.value
+
+    def submit_unregister(self, qid: int) -> int:
+        t = _u64(0)
+        self._check(self.lib.cgb_server_submit_unregister(self.h, qid, ctypes.byref(t)))
+        return t.value
+
+    def wait(self, ticket: int, timeout_ms: int = 600000) -> dict:
+        """Result of a request: status, timestamps, query id (registrations),
+        counts per query id (batches)."""
+        res = ServerResult()
+        pos = np.zeros(MQ_MAX_QUERIES, dtype=np.uint64)
+        neg = np.zeros(MQ_MAX_QUERIES, dtype=np.uint64)
+        self._check(self.lib.cgb_server_wait(self.h, ticket, timeout_ms, ctypes.byref(res), pos.ctypes.data,
+                                             neg.ctypes.data, MQ_MAX_QUERIES))
+        return {"ticket": res.ticket, "kind": res.kind, "status": res.status, "query_id": res.query_id,
+                "live_queries": res.live_queries, "t_submit_ms": res.t_submit_ms, "t_staged_ms": res.t_staged_ms,
+                "t_start_ms": res.t_start_ms, "t_done_ms": res.t_done_ms, "device_ms": res.device_ms,
+                "pos": pos, "neg": neg}
+
+    def stats(self) -> dict:
+        out = np.zeros(8, dtype=np.uint64)
+        self._check(self.lib.cgb_server_stats(self.h, out.ctypes.data))
+        keys = ["batches_done", "edges_done", "rejected", "live_queries", "queued", "staging_bytes",
+                "hbm_budget_bytes", "busy_us"]
+        return {k: int(v) for k, v in zip(keys, out)}

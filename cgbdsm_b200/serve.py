@@ -1,0 +1,138 @@
+"""Serving workload: the R-MAT 4M/34M graph resident on the device, update
+batches arriving as a seeded Poisson process with sizes drawn log-uniform
+from 1,000 to 1,000,000 insertions (cut consecutively from the held-out
+stream), and query registrations arriving during the run, drawn from the
+64-query mix (sizes 4-12; tree / sparse / dense) sampled on the same graph.
+
+The server (cgb_server_*, native) admits and applies the requests in order;
+the client here submits each request at its arrival time from its own
+thread and collects the results.  Reported: edge updates/s and matches/s
+over the run (first arrival to last completion), per-batch latency p50/p99
+(arrival to counts available), queueing delay, device busy fraction.
+
+Offered load: the mean inter-arrival time is set from a short calibration
+(the mean service time of batches of the same size distribution) so that the
+device is busy about 80% of the time.
+"""
+from __future__ import annotations
+
+import threading
+import time
+
+import numpy as np
+
+SEED_BATCHES, SEED_QUERIES = 51, 52
+
+
+def cut_batches(stream: np.ndarray, seed: int, lo: int = 1000, hi: int = 1_000_000, limit=None):
+    """Consecutive cuts of the stream with log-uniform sizes in [lo, hi]."""
+    rng = np.random.default_rng(seed)
+    out, pos = [], 0
+    while pos < len(stream) and (limit is None or len(out) < limit):
+        k = int(np.exp(rng.uniform(np.log(lo), np.log(hi))))
+        out.append(stream[pos:pos + k])
+        pos += k
+    return out
+
+
+def run_schedule(server, events, collect_timeout_ms: int = 600000):
+    """Submits events [(t_s, kind, payload)] at their times (one client thread)
+    and waits for every result; returns the results in submission order."""
+    tickets = []
+    t0 = time.perf_counter()
+
+    def client():
+        for t, kind, payload in events:
+            dt = t - (time.perf_counter() - t0)
+            if dt > 0:
+                time.sleep(dt)
+            if kind == "batch":
+                tickets.append(("batch", server.submit_batch(ins=payload)))
+            elif kind == "register":
+                ql, qe = payload
+                tickets.append(("register", server.submit_register(len(ql), qe, ql)))
+            else:
+                tickets.append(("unregister", server.submit_unregister(payload)))
+
+    th = threading.Thread(target=client)
+    th.start()
+    results, i = [], 0
+    while th.is_alive() or i < len(tickets):
+        if i < len(tickets):
+            kind, tk = tickets[i]
+            r = server.wait(tk, collect_timeout_ms)
+            r["what"] = kind
+            results.append(r)
+            i += 1
+        else:
+            time.sleep(0.0005)
+    th.join()
+    return results
+
+
+def bench(args, local: int, log) -> dict:
+    from . import queryset
+    from .engine import Server
+    from .workloads import SPECS, GraphData
+
+    spec = SPECS["c3_tree"]
+    g = GraphData(spec)
+    try:
+        qpool = queryset.load("c3")
+    except OSError:
+        qpool = queryset.load("c2")  # fall back to the R-MAT 1M/10M mix's shapes (labels are shared)
+    rng = np.random.default_rng(SEED_QUERIES)
+    n_initial, n_arriving = 8, 8
+    order = rng.permutation(len(qpool))
+    initial = [qpool[i] for i in order[:n_initial]]
+    arriving = [qpool[i] for i in order[n_initial:n_initial + n_arriving]]
+    batches = cut_batches(g.stream, SEED_BATCHES)
+    log(f"c5: {len(batches)} batches, {sum(len(b) for b in batches)} edges, {n_initial}+{n_arriving} queries")
+
+    server = Server(g.labels, g.initial, device=local, staging_bytes=256 << 20, dfs_budget_ms=args.budget_ms)
+    # the initial queries, then a calibration of the service time on the first batches' sizes
+    for q in initial:
+        r = server.wait(server.submit_register(q["qv"], [tuple(e) for e in q["edges"]], q["labels"]))
+        assert r["status"] == 0
+    n_cal = 3
+    cal = run_schedule(server, [(0.0, "batch", b) for b in batches[:n_cal]])
+    svc_ms_per_edge = sum(r["t_done_ms"] - r["t_start_ms"] for r in cal) / sum(len(b) for b in batches[:n_cal])
+    mean_size = float(np.mean([len(b) for b in batches]))
+    mean_gap_s = svc_ms_per_edge * mean_size / 1e3 / 0.8  # about 80% busy
+    arng = np.random.default_rng(SEED_BATCHES + 1000)
+    t, events = 0.0, []
+    for b in batches[n_cal:]:
+        t += float(arng.exponential(mean_gap_s))
+        events.append((t, "batch", b))
+    horizon = t
+    qt = np.sort(np.random.default_rng(SEED_QUERIES + 1000).uniform(0, horizon, n_arriving))
+    for tq, q in zip(qt, arriving):
+        events.append((float(tq), "register", (q["labels"], [tuple(e) for e in q["edges"]])))
+    events.sort(key=lambda e: e[0])
+    log(f"c5: mean inter-arrival {mean_gap_s * 1e3:.1f} ms (service {svc_ms_per_edge * 1e3:.3f} us/edge)")
+    res = run_schedule(server, events)
+    st = server.stats()
+    server.close()
+    br = [r for r in res if r["what"] == "batch"]
+    ok = [r for r in br if r["status"] == 0]
+    lat = [r["t_done_ms"] - r["t_submit_ms"] for r in ok]
+    queue = [r["t_start_ms"] - r["t_submit_ms"] for r in ok]
+    span_s = (max(r["t_done_ms"] for r in br) - min(r["t_submit_ms"] for r in res)) / 1e3
+    edges = sum(len(e[2]) for e in events if e[1] == "batch")
+    matches = sum(int(r["pos"].sum(dtype=np.uint64)) for r in ok)
+    return {
+        "metric": "served edge updates/sec and matches/sec under Poisson arrivals; p50/p99 batch latency",
+        "value": edges / span_s, "unit": "edge updates/s",
+        "config": {"workload": "R-MAT 4,000,000 / 34,000,000, 32 labels Zipf(1.0); Poisson batch arrivals "
+                               "(seed 51), sizes log-uniform 1,000-1,000,000 cut from the held-out stream; "
+                               f"{n_initial} queries registered at start, {n_arriving} arriving (seed 52)",
+                   "batches": len(br), "edges": edges, "mean_interarrival_ms": mean_gap_s * 1e3,
+                   "calibration_batches": n_cal},
+        "matches_per_s": matches / span_s,
+        "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                       "max": float(max(lat))},
+        "queue_ms": {"p50": float(np.percentile(queue, 50)), "p99": float(np.percentile(queue, 99))},
+        "device_busy_frac": sum(r["device_ms"] for r in ok) / 1e3 / span_s,
+        "rejected": len(br) - len(ok),
+        "live_queries_at_end": st["live_queries"],
+    }

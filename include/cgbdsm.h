@@ -66,6 +66,7 @@ typedef struct {
 #define CGB_FLAG_MASK_PRUNE 0x80u         /* valid bits, and skip core candidates whose bit is clear    */
 #define CGB_FLAG_NO_SEED_GROUPS 0x100u    /* one DFS per seed even where a pendant endpoint allows one per group */
 #define CGB_FLAG_NO_RUN_BITS 0x200u       /* binary-search long runs instead of testing their per-batch bit sets */
+#define CGB_FLAG_FOOTPRINT 0x400u         /* measure the matching footprint (cgb_last_stats[4]); slower   */
 
 /* Limits (reference: utils/config.h:5-6; key layout calig_helper_gamma.cu:228-229). */
 #define CGB_MAX_QV 12
@@ -157,8 +158,11 @@ uint64_t cgb_kernel_launches(const cgb_handle* h);
 
 /* Work counters of the last batch (8 entries): [0] seeds (delta edges
  * expanded), [1] 32-candidate chunks evaluated, [2] candidates tested,
- * [3] tail counts, [4] matching algorithmic bytes (seed keys 8 B, list records
- * 16 B, candidate words 4 B, one 32 B sector per binary-search step),
+ * [3] tail counts, [4] matching bytes: with CGB_FLAG_FOOTPRINT the footprint
+ * (16 B per distinct record resolved plus 4 B per entry of its old and delta
+ * lists, each record counted once), else a probe estimate (seed keys 8 B,
+ * list records 16 B, candidate words 4 B, one 32 B sector per binary-search
+ * step),
  * [5] index-update algorithmic bytes (edits 8 B, old and new run words 4 B,
  * record 32 B per touched run), [6] touched runs, [7] reserved. */
 cgb_status cgb_last_stats(const cgb_handle* h, uint64_t* out8);
@@ -385,6 +389,64 @@ cgb_status cgb_mq_query_info(const cgb_mq* m, uint32_t query_id, uint32_t* varia
 cgb_status cgb_mq_schedule(const cgb_mq* m, uint32_t* blocks_per_sm, uint32_t* steal);
 uint64_t cgb_mq_kernel_launches(const cgb_mq* m);
 void* cgb_mq_stream(const cgb_mq* m);
+
+/* ------------------------------------------------------------------------
+ * Serving loop over the multi-query engine.  No counterpart in the
+ * reference (one query and one update file per process, main_calig.cpp).
+ * The graph, its index and every registered query stay on the device while
+ * requests arrive from any thread: update batches (result: every registered
+ * query's positive / negative matches for that batch), query registrations
+ * (joining the running query set at the next batch boundary; result: the
+ * query id) and removals.  Requests take effect in submission order.
+ * Admission by HBM budget: an update batch's edge pairs must fit a device
+ * staging ring (they are copied as soon as space frees, on a copy stream, so
+ * the copies of waiting batches overlap the running batch), and its working
+ * set must fit the budget (else its result is CGB_ERR_LIMIT).
+ * ------------------------------------------------------------------------ */
+typedef struct cgb_server cgb_server;
+
+typedef struct {
+    cgb_mq_config mq;
+    uint64_t hbm_budget_bytes;  /* device memory the server may add after loading the graph; 0 = 90% of free */
+    uint64_t staging_bytes;     /* staging ring for edge pairs; 0 = 64 MiB                                 */
+    uint32_t max_pending;       /* requests queued at once; 0 = 4096                                      */
+} cgb_server_config;
+
+#define CGB_SERVER_BATCH 0u
+#define CGB_SERVER_REGISTER 1u
+#define CGB_SERVER_UNREGISTER 2u
+
+typedef struct {
+    uint64_t ticket;
+    uint32_t kind;          /* CGB_SERVER_* */
+    int32_t status;         /* cgb_status of the request */
+    uint32_t query_id;      /* registrations */
+    uint32_t live_queries;  /* batches: queries registered when it ran */
+    double t_submit_ms, t_staged_ms, t_start_ms, t_done_ms;  /* since the server started */
+    float device_ms;        /* batches: device time of the batch */
+} cgb_server_result;
+
+void cgb_server_default_config(cgb_server_config* cfg);
+/* Loads the graph (as cgb_mq_load_graph) and starts the server's threads. */
+cgb_status cgb_server_create(const cgb_server_config* cfg, uint32_t n, const uint32_t* labels, uint64_t num_edges,
+                             const uint32_t* edges, cgb_server** out);
+/* Stops the threads (queued requests are dropped) and frees everything. */
+void cgb_server_destroy(cgb_server* s);
+const char* cgb_server_last_error(const cgb_server* s);
+/* Requests (host arrays, copied before returning); *ticket identifies the result. */
+cgb_status cgb_server_submit_batch(cgb_server* s, const uint32_t* ins, uint64_t n_ins, const uint32_t* del,
+                                   uint64_t n_del, uint64_t* ticket);
+cgb_status cgb_server_submit_register(cgb_server* s, uint32_t qv, const uint32_t* labels, uint32_t qe,
+                                      const uint32_t* edges, uint64_t* ticket);
+cgb_status cgb_server_submit_unregister(cgb_server* s, uint32_t query_id, uint64_t* ticket);
+/* Waits up to timeout_ms for a request; fills *res and, for batches, the
+ * counts per query id (cap entries).  A ticket is collected once.
+ * CGB_ERR_TIMEOUT if it has not completed. */
+cgb_status cgb_server_wait(cgb_server* s, uint64_t ticket, uint32_t timeout_ms, cgb_server_result* res,
+                           uint64_t* pos, uint64_t* neg, uint32_t cap);
+/* [0] batches done, [1] edges done, [2] rejected, [3] live queries, [4] queued,
+ * [5] staging ring bytes, [6] HBM budget bytes, [7] device busy microseconds. */
+cgb_status cgb_server_stats(const cgb_server* s, uint64_t* out8);
 
 #ifdef __cplusplus
 }

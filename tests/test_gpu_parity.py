@@ -11,7 +11,7 @@ import pytest
 
 from cgbdsm_b200 import CgbError, Engine
 from cgbdsm_b200.engine import (FLAG_ENUMERATE_TAIL, FLAG_FORCE_SPLIT, FLAG_MASK_PRUNE, FLAG_NO_RUN_BITS,
-                                FLAG_NO_SEED_GROUPS, FLAG_NO_TAIL_CACHE, FLAG_VALID_BITS)
+                                FLAG_NO_SEED_GROUPS, FLAG_NO_TAIL_CACHE, FLAG_PLAIN_CORE_ORDER, FLAG_VALID_BITS)
 from cgbdsm_b200.workloads import SPECS, materialize, read_query
 from oracle import bind
 
@@ -25,9 +25,9 @@ def _key(d, u, v):
 
 
 @pytest.mark.parametrize("flags", [0, FLAG_ENUMERATE_TAIL, FLAG_FORCE_SPLIT | FLAG_ENUMERATE_TAIL, FLAG_FORCE_SPLIT,
-                                   FLAG_NO_TAIL_CACHE, FLAG_NO_SEED_GROUPS, FLAG_NO_RUN_BITS],
+                                   FLAG_NO_TAIL_CACHE, FLAG_NO_SEED_GROUPS, FLAG_NO_RUN_BITS, FLAG_PLAIN_CORE_ORDER],
                          ids=["counted_tail", "enumerated_tail", "stolen_enumerated", "stolen_counted",
-                              "counted_no_prefix_cache", "seed_per_dfs", "searched_runs"])
+                              "counted_no_prefix_cache", "seed_per_dfs", "searched_runs", "greedy_core_order"])
 @pytest.mark.parametrize("name", PIPELINE_CASES)
 def test_engine_matches_reference_cpu_path(name, flags, workdir):
     if not bind.have_ref():
