@@ -304,6 +304,14 @@ def run_pipelines(names: list[str], args, rank: int, world: int, local: int, foo
         "setup_s": round(setup_s, 1),
         "clocks": clk.summary(),
     }
+    # the reference's Bottleneck = max(S1, S2) view (main_calig.cpp:435-437):
+    # Stage 1 (host producer) of batch b+1 overlaps Stage 2 of batch b
+    s1_batch = [sum(w["stage1_ms"][r["batch"]] for w in W) for r in recs]
+    bneck_ms = sum(max(a, b) for a, b in zip(s1_batch, step_ms))
+    out["with_stage1"] = {"value": edges / (bneck_ms / 1e3) if bneck_ms > 0 else 0.0, "unit": "edge updates/s",
+                          "stage1_ms_per_batch": float(np.mean(s1_batch)),
+                          "stage2_ms_per_batch": float(np.mean(step_ms)),
+                          "view": "sum over batches of max(Stage 1, Stage 2)"}
     peak, peak_kind = _peaks()
     upd_gbs = (upd_bytes / 1e9) / (upd_ms / 1e3) if upd_ms > 0 else 0.0
     if footprint and match_ms >= upd_ms:
@@ -413,6 +421,43 @@ def bench_c5(args, rank, world, local) -> dict:
     return serve.bench(args, local, log)
 
 
+def index_layouts(W, local: int) -> dict:
+    """The update layouts on the headline's first pattern (R-MAT 4M/34M, 7-vertex
+    tree, batches of 1,000,000): per batch, the pool layout's fused merge
+    (index update phase of the engine, pending delta + ins - del) against the
+    packed-memory array (cgb_gpma_batch_update with the same edits), device
+    time of each."""
+    import torch
+
+    from cgbdsm_b200 import Engine, Gpma
+
+    w = W[0]
+    dev = f"cuda:{local}"
+    e = Engine(device=local)
+    e.load_query(len(w["ql"]), w["qe"], w["ql"])
+    e.build_index(w["init"], w["dv0"])
+    gp = Gpma(num_dirs=2 * len(w["qe"]), device=local)
+    gp.bulk_load(w["init"])
+    pool_ms, gpma_ms, edits = [], [], []
+    pending = np.zeros(0, np.uint64)
+    for b in w["batches"]:
+        e.apply_batch(b["dv"], b["ins"], b["del"], b["delta"], b["edge_ok"])
+        pool_ms.append(float(e.timings()[0]))
+        ins = np.concatenate([pending, b["ins"]])
+        gp.batch_update(ins, b["del"])
+        gpma_ms.append(gp.stats()["device_us"] / 1e3)
+        edits.append(int(len(ins) + len(b["del"])))
+        pending = b["delta"]
+    torch.cuda.synchronize()
+    same = bool(np.array_equal(np.sort(e.read_index()), np.sort(np.concatenate(
+        [(np.uint64(d) << np.uint64(59)) | gp.extract(d) for d in range(2 * len(w["qe"]))]))))
+    e.close()
+    gp.close()
+    return {"workload": w["spec"].name, "edits_per_batch": edits, "pool_merge_ms": pool_ms, "gpma_update_ms": gpma_ms,
+            "gpma_over_pool": float(np.sum(gpma_ms) / max(np.sum(pool_ms), 1e-9)),
+            "same_contents_after_stream": same}
+
+
 def run_ours(args) -> None:
     import torch
 
@@ -421,14 +466,16 @@ def run_ours(args) -> None:
     rank, world, local = dist.env()
     torch.cuda.set_device(local)
     dist.init("nccl", timeout_s=900)
-    head = run_pipelines(HEADLINE, args, rank, world, local)
+    names = args.headline.split(",")
+    head = run_pipelines(names, args, rank, world, local)
     W = head.pop("_W")
     line = {
         "metric": METRIC, "value": head.pop("value"), "unit": "edge updates/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": head.pop("ms_per_step"),
         "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
         "dtype": "u32/u64 integer", "data": "synthetic (seeded R-MAT stand-in for the public graphs)",
-        "config": {"workload": C3_DESC, "batch_edges": W[0]["spec"].batch_edges,
+        "config": {"workload": C3_DESC if names == HEADLINE else f"{names} (profiling run)",
+                   "batch_edges": W[0]["spec"].batch_edges,
                    "batches_in_stream": head.pop("batches_in_stream"), "patterns": head.pop("patterns"),
                    "l2": "flushed before every engine call (256 MiB write); index > 126 MB L2",
                    "parallelism": f"{world} GPU(s): index replicated, seed groups sharded"},
@@ -440,11 +487,16 @@ def run_ours(args) -> None:
 
         if bind.have_ref():
             log("cpu baseline: reference CPU path on batch 0 of each pattern")
-            line["cpu_baseline"] = reference_line(HEADLINE, args.cpu_budget_s,
+            line["cpu_baseline"] = reference_line(names, args.cpu_budget_s,
                                                   os.environ.get("CGB_BENCH_DIR", "/tmp/cgb_bench_r0"))
         else:
             line["cpu_baseline"] = {"unavailable": "oracle/_ref/libcgbref.so was not built (no reference tree)"}
     extras = {}
+    if world == 1 and not args.quick:
+        try:
+            line["index_layouts"] = index_layouts(W, local)
+        except Exception as e:
+            line["index_layouts"] = {"error": f"{type(e).__name__}: {e}"}
     for name in [w for w in args.workloads.split(",") if w] if world == 1 else []:
         fn = {"c2": bench_c2, "c4": bench_c4, "c5": bench_c5}.get(name)
         if fn is None:
@@ -504,6 +556,8 @@ def main():
     ap.add_argument("--cpu-budget-s", type=float, default=8.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workloads", default="c2,c4,c5", help="further workloads in the same JSON line")
+    ap.add_argument("--headline", default=",".join(HEADLINE),
+                    help="patterns of the timed pipeline (profiling runs use a smaller workload, e.g. c2)")
     ap.add_argument("--quick", action="store_true",
                     help="profiling run: 1 warm-up + 1 step, no e2e leg, no CPU baseline, no further workloads "
                          "(not a benchmark)")

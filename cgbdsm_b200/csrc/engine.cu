@@ -32,6 +32,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "cgbdsm.h"
@@ -135,6 +136,7 @@ __global__ void k_extract_du(const uint64_t* __restrict__ in, uint64_t n, uint32
 // fused edit merge of every touched (d, u): warp per run below kBigRun merged
 // entries, CTA per longer (hub) run
 // ---------------------------------------------------------------------------
+constexpr uint32_t kTinyRun = 32;        // merged entries up to which one lane merges the run
 constexpr uint32_t kBigRun = 4096;       // merged entries (old run + edits) from which a CTA merges the run
 constexpr uint32_t kMergeWarps = 8;      // warps of a CTA merge
 constexpr uint32_t kSegWindows = 8;      // 32-entry windows a CTA warp merges per round
@@ -152,9 +154,10 @@ struct MergeArgs {
     const uint32_t* run_len;
     const uint32_t* run_off;
     const int* num_runs;
-    uint32_t* small_runs;        // run ids merged by a warp / by a CTA (k_merge_classify)
+    uint32_t* small_runs;        // run ids merged by a warp / by a CTA / by a lane (k_merge_classify)
     uint32_t* big_runs;
-    unsigned int* list_ctr;      // [0] small, [1] big
+    uint32_t* tiny_runs;
+    unsigned int* list_ctr;      // [0] small, [1] big, [2] tiny
     uint32_t B;
     unsigned int* err;
     unsigned long long* stats;   // [5] merge bytes (edits 8 B, old run 4 B/word, new run 4 B/word, record 32 B), [6] runs
@@ -250,8 +253,10 @@ __global__ void k_merge_classify(MergeArgs a) {
         const uint32_t du = a.run_du[r];
         if (du == 0xffffffffu) continue;  // invalid keys
         const uint32_t xl = a.rec[(size_t)(du >> a.B) * a.dvcap + (du & vmask)].y;
-        if (xl + a.run_len[r] >= kBigRun) a.big_runs[atomicAdd(a.list_ctr + 1, 1u)] = (uint32_t)r;
-        else a.small_runs[atomicAdd(a.list_ctr + 0, 1u)] = (uint32_t)r;
+        const uint32_t total = xl + a.run_len[r];
+        if (total >= kBigRun) a.big_runs[atomicAdd(a.list_ctr + 1, 1u)] = (uint32_t)r;
+        else if (total > kTinyRun) a.small_runs[atomicAdd(a.list_ctr + 0, 1u)] = (uint32_t)r;
+        else a.tiny_runs[atomicAdd(a.list_ctr + 2, 1u)] = (uint32_t)r;
     }
 }
 
@@ -265,15 +270,37 @@ __device__ __forceinline__ unsigned long long pool_alloc(const MergeArgs& a, uin
     return off;
 }
 
-// Record update and accounting after a run was merged (one thread).
-__device__ __forceinline__ void merge_done(const MergeArgs& a, uint4* recp, uint4 old, unsigned long long off,
-                                           uint32_t outn, uint32_t yl, uint32_t d, uint32_t u) {
+// Accounting of the runs one warp merged, added to the launch's counters
+// once per warp (per-run atomics on these few words serialised the merge).
+struct MergeAcc {
+    unsigned long long bytes = 0, runs = 0;
+    long long live = 0;
+    __device__ __forceinline__ void add(uint32_t xl, uint32_t yl, uint32_t outn) {
+        bytes += 8ull * yl + 4ull * xl + 4ull * outn + 32ull;
+        runs += 1;
+        live += (long long)round4(outn) - (long long)round4(xl);
+    }
+    // every lane of the warp calls it; lane sums are combined
+    __device__ __forceinline__ void flush(const MergeArgs& a, uint32_t lane) {
+        for (int o = 16; o > 0; o >>= 1) {
+            bytes += __shfl_xor_sync(kFull, bytes, o);
+            runs += __shfl_xor_sync(kFull, runs, o);
+            live += __shfl_xor_sync(kFull, live, o);
+        }
+        if (lane == 0) {
+            if (bytes) atomicAdd(a.stats + 5, bytes);
+            if (runs) atomicAdd(a.stats + 6, runs);
+            if (live) atomicAdd((unsigned long long*)a.live_words, (unsigned long long)live);
+        }
+    }
+};
+
+// Record update after a run was merged (one thread); a run that reached the
+// bit-set length without a bit set claims one.  The unused tail of the
+// allocation is dead space until compaction.
+__device__ __forceinline__ void merge_record(const MergeArgs& a, uint4* recp, uint4 old, unsigned long long off,
+                                             uint32_t outn, uint32_t d, uint32_t u) {
     *recp = make_uint4((uint32_t)off, outn, old.z, old.w);
-    atomicAdd(a.stats + 5, 8ull * yl + 4ull * old.y + 4ull * outn + 32ull);
-    atomicAdd(a.stats + 6, 1ull);
-    long long dl = (long long)round4(outn) - (long long)round4(old.y);
-    if (dl) atomicAdd((unsigned long long*)a.live_words, (unsigned long long)dl);
-    // unused tail of the allocation is dead space until compaction
     if (a.rb_slot && outn >= a.rb_min_len) {
         uint32_t* sp = a.rb_slot + (size_t)d * a.dvcap + u;
         if (*sp == kNoVal) {
@@ -287,6 +314,70 @@ __device__ __forceinline__ void merge_done(const MergeArgs& a, uint4* recp, uint
     }
 }
 
+// Lane per run for runs of at most kTinyRun merged entries (most runs of a
+// batch touch a handful of entries): a serial merge per lane, one pool
+// allocation per warp step (a warp prefix over the lanes' bounds).
+__global__ void k_merge_tiny(MergeArgs a) {
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t n = a.list_ctr[2];
+    const uint32_t vmask = (1u << a.B) - 1u;
+    const uint64_t emask = (1ull << a.B) - 1ull;
+    const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+    MergeAcc acc;
+    for (uint32_t base = gw * 32; base < n; base += nw * 32) {
+        const uint32_t q = base + lane;
+        const bool on = q < n;
+        uint32_t r = 0, d = 0, u = 0, yl = 0;
+        uint4 old = make_uint4(0, 0, 0, 0);
+        uint4* recp = nullptr;
+        if (on) {
+            r = a.tiny_runs[q];
+            const uint32_t du = a.run_du[r];
+            d = du >> a.B;
+            u = du & vmask;
+            yl = a.run_len[r];
+            recp = a.rec + (size_t)d * a.dvcap + u;
+            old = *recp;
+        }
+        const uint32_t bound = on ? round4(old.y + yl) : 0u;
+        uint32_t pre = bound;  // inclusive prefix over the lanes
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t v = __shfl_up_sync(kFull, pre, o);
+            if (lane >= (uint32_t)o) pre += v;
+        }
+        const uint32_t total = __shfl_sync(kFull, pre, 31);
+        unsigned long long wbase = 0;
+        if (lane == 0 && total) {
+            wbase = atomicAdd(a.pool_top, (unsigned long long)total);
+            if (wbase + total > a.pool_cap) {
+                atomicOr(a.err, 4u);
+                wbase = ~0ull;
+            }
+        }
+        wbase = __shfl_sync(kFull, wbase, 0);
+        if (!on || wbase == ~0ull) continue;  // pool exhausted: runs left unchanged, error raised
+        const unsigned long long off = wbase + pre - bound;
+        const uint32_t* X = a.pool + old.x;
+        const uint64_t* Y = a.edits + a.run_off[r];
+        uint32_t* C = a.pool + off;
+        uint32_t i = 0, j = 0, outn = 0;
+        while (i < old.y || j < yl) {
+            const uint32_t xv = i < old.y ? X[i] : kNoVal;
+            const uint32_t yv = j < yl ? (uint32_t)((Y[j] >> 1) & emask) : kNoVal;
+            const uint32_t v = min(xv, yv);
+            bool present = false;
+            if (xv == v) { present = true; ++i; }
+            // the value's edits in order (adds before removes): the last decides
+            while (j < yl && (uint32_t)((Y[j] >> 1) & emask) == v) { present = (Y[j] & 1ull) == 0; ++j; }
+            if (present) C[outn++] = v;
+        }
+        merge_record(a, recp, old, off, outn, d, u);
+        acc.add(old.y, yl, outn);
+    }
+    acc.flush(a, lane);
+}
+
 // Warp per run: 32 merged entries per step from two coalesced windows.
 __global__ void k_merge_runs(MergeArgs a) {
     __shared__ uint32_t s_win[8][32];
@@ -296,6 +387,7 @@ __global__ void k_merge_runs(MergeArgs a) {
     const uint32_t nruns = a.list_ctr[0];
     const uint64_t vmask = (1ull << a.B) - 1ull;
     uint32_t* sbuf = s_win[(threadIdx.x >> 5) & 7];
+    MergeAcc acc;
     for (uint32_t q = gw; q < nruns; q += nw) {
         const uint32_t r = a.small_runs[q];
         const uint32_t du = a.run_du[r];
@@ -321,8 +413,12 @@ __global__ void k_merge_runs(MergeArgs a) {
             if (emit) C[outn + __popc(bal & ((1u << lane) - 1u))] = val;
             outn += __popc(bal);
         }
-        if (lane == 0) merge_done(a, recp, old, off, outn, yl, d, u);
+        if (lane == 0) {
+            merge_record(a, recp, old, off, outn, d, u);
+            acc.add(xl, yl, outn);
+        }
     }
+    acc.flush(a, lane);
 }
 
 // CTA per long run: each round, warp w merges the 256 entries from diagonal
@@ -337,6 +433,7 @@ __global__ void __launch_bounds__(kMergeWarps * 32) k_merge_big(MergeArgs a) {
     const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const uint32_t nruns = a.list_ctr[1];
     const uint64_t vmask = (1ull << a.B) - 1ull;
+    MergeAcc acc;
     for (uint32_t q = blockIdx.x; q < nruns; q += gridDim.x) {
         const uint32_t r = a.big_runs[q];
         const uint32_t du = a.run_du[r];
@@ -383,9 +480,13 @@ __global__ void __launch_bounds__(kMergeWarps * 32) k_merge_big(MergeArgs a) {
             outn += all;
             __syncthreads();
         }
-        if (threadIdx.x == 0) merge_done(a, recp, old, off, outn, yl, d, u);
+        if (threadIdx.x == 0) {
+            merge_record(a, recp, old, off, outn, d, u);
+            acc.add(xl, yl, outn);
+        }
         __syncthreads();
     }
+    if (threadIdx.x < 32) acc.flush(a, lane);
 }
 
 // ---------------------------------------------------------------------------
@@ -674,17 +775,13 @@ __device__ __forceinline__ bool list_contains(const uint32_t* __restrict__ pool,
 // Bit sets of the long old runs (rebuilt each batch): slot[(dir, vertex)]
 // names a bit set over the compressed ids, or kNoSlot; a warp keeps the slot
 // of every resolved record bn[k] in bslot[k].  slot == nullptr: none.
-// touched (non-null in footprint runs): one bit per record, set for every
-// record the matching resolves.
 struct RunBits {
     const uint32_t* slot;
     const uint32_t* bits;
     uint32_t words;
     uint32_t* bslot;
-    uint32_t* touched;
     __device__ __forceinline__ void note(uint32_t k, size_t at) const {
         if (slot) bslot[k] = __ldg(slot + at);
-        if (touched) atomicOr(touched + (at >> 5), 1u << (at & 31));
     }
     // x in the resolved list bn[k] = r: one bit test for a long old run
     __device__ __forceinline__ bool has(uint32_t k, const uint4& r, const uint32_t* __restrict__ pool,
@@ -700,6 +797,17 @@ struct RunBits {
     }
 };
 
+// Footprint runs (a separate instantiation of the DFS, so that the timed
+// kernel carries no trace of it): also sets the bit of every record resolved
+// in touched (one bit per record).
+struct RunBitsCount : RunBits {
+    uint32_t* touched;
+    __device__ __forceinline__ void note(uint32_t k, size_t at) const {
+        RunBits::note(k, at);
+        atomicOr(touched + (at >> 5), 1u << (at & 31));
+    }
+};
+
 
 // Number of x in the intersection of the resolved lists bn[ids[0..nl)] with x
 // not among the matched core vertices m[t], t in the bit set excl (positions
@@ -707,10 +815,11 @@ struct RunBits {
 // warp-uniform.  One list: its length minus the excluded vertices it holds.
 // Several: the shortest list is scanned 32 elements at a time and each
 // element probed in the others.
+template <class RB>
 __device__ unsigned long long isect_count(const uint4* bn, const uint8_t* ids, uint32_t nl, const uint32_t* m,
                                           uint32_t excl, const uint32_t* __restrict__ pool,
                                           const uint32_t* __restrict__ dval, uint32_t lane,
-                                          unsigned long long& bytes, const RunBits& rb) {
+                                          unsigned long long& bytes, const RB& rb) {
     if (nl == 1) {
         const uint4 r = bn[ids[0]];
         bool in = false;
@@ -770,10 +879,11 @@ __device__ __forceinline__ unsigned long long group_count(const unsigned long lo
 // m[0..n_core): per label group, inclusion-exclusion over the sizes of the
 // members' candidate sets and of their intersections (core vertices
 // excluded); groups multiply.  Warp-cooperative, warp-uniform result.
+template <class RB>
 __device__ unsigned long long tail_count_warp(const EdgePlan& P, const uint32_t* m, uint4* bn, const uint4* rec,
                                               uint32_t dvcap, const uint32_t* __restrict__ pool,
                                               const uint32_t* __restrict__ dval, bool self_loops, uint32_t lane,
-                                              unsigned long long& bytes, const RunBits& rb) {
+                                              unsigned long long& bytes, const RB& rb) {
     const uint32_t nc = P.n_core, n = P.n;
     // resolve every tail BN record once
     for (uint32_t k = P.bn_off[nc] + lane; k < P.bn_off[n]; k += 32) {
@@ -822,10 +932,11 @@ constexpr uint32_t kClean = 0xffu;  // tail cache up to date
 // depends on the positions of its lists' backward neighbours and of the
 // excluded core vertices, so e.g. a subset hanging off positions 0 and 1
 // is counted once per (m[0], m[1]), not once per prefix.
+template <class RB>
 __device__ void tail_prepare(const EdgePlan& P, const uint32_t* m, uint4* bn, unsigned long long* cache,
                              uint32_t dirty, const uint4* rec, uint32_t dvcap, const uint32_t* __restrict__ pool,
                              const uint32_t* __restrict__ dval, bool self_loops, uint32_t lane,
-                             unsigned long long& bytes, const RunBits& rb) {
+                             unsigned long long& bytes, const RB& rb) {
     const uint32_t nc = P.n_core, n = P.n, j = nc - 1;
     for (uint32_t k = P.bn_off[nc] + lane; k < P.bn_off[n]; k += 32) {
         if (P.bn_pos[k] >= j || P.bn_pos[k] < dirty) continue;  // records of unchanged owners are current
@@ -865,11 +976,12 @@ __device__ void tail_prepare(const EdgePlan& P, const uint32_t* m, uint4* bn, un
 }
 
 // Tail count for the core embedding m[0..n_core) (m[j] = the candidate).
+template <class RB>
 __device__ unsigned long long tail_eval(const EdgePlan& P, const uint32_t* m, uint4* bn,
                                         const unsigned long long* cache, const uint4* rec, uint32_t dvcap,
                                         const uint32_t* __restrict__ pool, const uint32_t* __restrict__ dval,
                                         bool self_loops, uint32_t lane, unsigned long long& bytes,
-                                        const RunBits& rb) {
+                                        const RB& rb) {
     const uint32_t nc = P.n_core, n = P.n, j = nc - 1;
     const uint32_t c = m[j];
     for (uint32_t k = P.bn_off[nc] + lane; k < P.bn_off[n]; k += 32) {
@@ -922,9 +1034,10 @@ __device__ unsigned long long tail_eval(const EdgePlan& P, const uint32_t* m, ui
 // and c is removed from it when c lies in all of the subset's lists (only
 // for groups sharing the last core vertex's label).  Lanes diverge only in
 // the searches.
+template <class RB>
 __device__ unsigned long long tail_eval_lane(const EdgePlan& P, const uint4* bn, const unsigned long long* cache,
                                              const uint32_t* __restrict__ pool, const uint32_t* __restrict__ dval,
-                                             uint32_t c, unsigned long long& bytes, const RunBits& rb) {
+                                             uint32_t c, unsigned long long& bytes, const RB& rb) {
     const uint32_t nc = P.n_core, n = P.n, j = nc - 1;
     unsigned long long prod = 1;
     uint32_t t = nc;
@@ -1103,7 +1216,7 @@ constexpr uint32_t kCandMask = (1u << kCandBits) - 1u;
 // global memory (a.plans, one per (query, edge); a.qe of them), seed table
 // searched in global memory, each warp's current plan copied to shared
 // memory when its unit changes plan.
-template <bool kMulti>
+template <bool kMulti, bool kFoot = false>
 __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
     __shared__ uint32_t s_cand[kDfsWarps][kMaxQV][32];
     __shared__ uint4 s_bn[kDfsWarps][kMaxBN];
@@ -1134,7 +1247,13 @@ __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
     const uint64_t vmask = (1ull << a.B) - 1ull;
     uint32_t* m = s_m[w];
     uint4* bn = s_bn[w];
-    const RunBits rb{a.rb_slot, a.rb_bits, a.rb_words, s_rbs[w], a.touched};
+    using RB = typename std::conditional<kFoot, RunBitsCount, RunBits>::type;
+    RB rb;
+    rb.slot = a.rb_slot;
+    rb.bits = a.rb_bits;
+    rb.words = a.rb_words;
+    rb.bslot = s_rbs[w];
+    if constexpr (kFoot) rb.touched = a.touched;
     volatile unsigned int* vq = a.qctr;  // [0] tasks reserved, [1] tickets issued, [3] completed, [6] seeds
 
     // per-depth state held by lane == depth
@@ -1262,7 +1381,7 @@ __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
         if (P.grouped) {
             const size_t xat = (size_t)P.seed_dir * a.dvcap + m[0];
             const uint4 xr = a.rec[xat];
-            if (a.touched && lane == 0) atomicOr(a.touched + (xat >> 5), 1u << (xat & 31));
+            if (kFoot && lane == 0) atomicOr(a.touched + (xat >> 5), 1u << (xat & 31));
             X.x = a.dval + xr.z;
             X.n = xr.w;
             if (X.n <= 32 && lane < X.n) X.xv = __ldg(X.x + lane);
@@ -1717,7 +1836,8 @@ struct cgb_handle {
     uint32_t* d_du = nullptr; uint32_t* d_run_du = nullptr; uint32_t* d_run_len = nullptr;
     uint32_t* d_run_off = nullptr; size_t runs_cap = 0;
     uint32_t* d_small_runs = nullptr; uint32_t* d_big_runs = nullptr;  // merge lists (k_merge_classify)
-    unsigned int* d_list_ctr = nullptr;  // [0] small, [1] big
+    uint32_t* d_tiny_runs = nullptr;
+    unsigned int* d_list_ctr = nullptr;  // [0] small, [1] big, [2] tiny
     int* d_num_runs = nullptr;
     uint64_t* d_dkeys = nullptr; uint64_t* d_dkeys_alt = nullptr; size_t dkeys_cap = 0;
     uint32_t* d_dval = nullptr;
@@ -1941,8 +2061,9 @@ cgb_status ensure_edit_buffers(cgb_handle* h, uint64_t n) {
     size_t nc = std::max<size_t>(n + n / 2, 1 << 16);
     CK(cudaStreamSynchronize(h->stream));
     void* olds[] = {h->d_edits, h->d_edits_alt, h->d_du, h->d_run_du, h->d_run_len, h->d_run_off,
-                    h->d_small_runs, h->d_big_runs};
+                    h->d_small_runs, h->d_big_runs, h->d_tiny_runs};
     for (void* p : olds) if (p) CK(cudaFree(p));
+    CK(cudaMalloc(&h->d_tiny_runs, nc * sizeof(uint32_t)));
     CK(cudaMalloc(&h->d_small_runs, nc * sizeof(uint32_t)));
     CK(cudaMalloc(&h->d_big_runs, nc * sizeof(uint32_t)));
     CK(cudaMalloc(&h->d_edits, nc * sizeof(uint64_t)));
@@ -2007,6 +2128,7 @@ cgb_status apply_edits(cgb_handle* h, const uint64_t* adds0, uint64_t n0, const 
     ma.num_runs = h->d_num_runs;
     ma.small_runs = h->d_small_runs;
     ma.big_runs = h->d_big_runs;
+    ma.tiny_runs = h->d_tiny_runs;
     ma.list_ctr = h->d_list_ctr;
     ma.B = pi.B;
     ma.err = d_err;
@@ -2024,8 +2146,10 @@ cgb_status apply_edits(cgb_handle* h, const uint64_t* adds0, uint64_t n0, const 
         ma.rb_new = h->d_rb_new;
         CK(cudaMemsetAsync(h->d_rb_ctr + 1, 0, sizeof(unsigned int), h->stream));
     }
-    CK(cudaMemsetAsync(h->d_list_ctr, 0, 2 * sizeof(unsigned int), h->stream));
+    CK(cudaMemsetAsync(h->d_list_ctr, 0, 3 * sizeof(unsigned int), h->stream));
     k_merge_classify<<<grid_for(h, n), 256, 0, h->stream>>>(ma);
+    LAUNCHED();
+    k_merge_tiny<<<grid_for(h, n), 256, 0, h->stream>>>(ma);
     LAUNCHED();
     const int mg = std::max(1, std::min<int>((int)((n * 32 + 255) / 256), h->num_sms * 16));
     k_merge_runs<<<mg, 256, 0, h->stream>>>(ma);
@@ -2130,7 +2254,7 @@ cgb_status cgb_create(const cgb_config* cfg, cgb_handle** out) {
     CKC(cudaMemset(h->d_self, 0, sizeof(unsigned int)));
     CKC(cudaMallocHost(&h->h_scal, (16 + kMaxQE) * sizeof(unsigned long long)));
     CKC(cudaMalloc(&h->d_num_runs, 2 * sizeof(int)));
-    CKC(cudaMalloc(&h->d_list_ctr, 2 * sizeof(unsigned int)));
+    CKC(cudaMalloc(&h->d_list_ctr, 3 * sizeof(unsigned int)));
     CKC(cudaMalloc(&h->d_rb_ctr, 2 * sizeof(unsigned int)));
     CKC(cudaMemset(h->d_rb_ctr, 0, 2 * sizeof(unsigned int)));
     CKC(cudaMalloc(&h->d_rev, kMaxDir));
@@ -2157,7 +2281,7 @@ void cgb_destroy(cgb_handle* h) {
                     h->d_dkeys, h->d_dkeys_alt, h->d_dval, h->d_ddu, h->d_drun_du, h->d_drun_len, h->d_drun_off,
                     h->d_seed, h->d_counts, h->d_stats, h->d_tasks, h->d_qctr, h->d_temp, h->d_qe_dirs, h->d_edge_ok,
                     h->d_vb, h->d_rb_slot, h->d_rb_sel, h->d_rb_bits, h->d_rb_ctr, h->d_rb_new, h->d_small_runs,
-                    h->d_big_runs, h->d_list_ctr, h->d_rev, h->d_touched};
+                    h->d_big_runs, h->d_tiny_runs, h->d_list_ctr, h->d_rev, h->d_touched};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (h->h_scal) cudaFreeHost(h->h_scal);
@@ -2405,7 +2529,8 @@ cgb_status cgb_apply_batch_device(cgb_handle* h, uint32_t dv_count, const uint64
         }
         int bps = h->dfs_occupancy;
         if (h->cfg.dfs_blocks_per_sm) bps = std::min(bps, (int)h->cfg.dfs_blocks_per_sm);
-        k_dfs_count<false><<<h->num_sms * bps, kDfsWarps * 32, 0, h->stream>>>(da);
+        if (footprint) k_dfs_count<false, true><<<h->num_sms * bps, kDfsWarps * 32, 0, h->stream>>>(da);
+        else k_dfs_count<false><<<h->num_sms * bps, kDfsWarps * 32, 0, h->stream>>>(da);
         LAUNCHED();
         CK(cudaGetLastError());
         CK(cudaEventRecord(h->ev[3], h->stream));

@@ -232,6 +232,7 @@ struct cgb_mq {
     // schedule (autotuned)
     bool tuned_global = false;
     bool tuned_now = false;  // the current batch ran the autotuner
+    uint32_t tuned_plans = 0;  // plan count when the grid was last tuned
     int bps = 0;        // DFS blocks per SM
     bool steal = true;
 
@@ -530,8 +531,9 @@ cgb_status mq_sync(cgb_mq* m) {
 
 // Autotuner, run on the first matched batch after the query set changed:
 // every new query alone under each plan variant (counts must agree; the
-// fastest variant is kept), then the whole set under a few DFS grid sizes and
-// with work stealing on and off.  Trials run on the batch's prepared delta;
+// fastest variant is kept), then (first time, and whenever the plan count
+// has doubled since) the whole set under a few DFS grid sizes and with work
+// stealing on and off.  Trials run on the batch's prepared delta;
 // the DFS does not modify the index, so every trial sees the same input.
 cgb_status mq_autotune(cgb_mq* m, uint64_t n2) {
     cgb_handle* h = m->h;
@@ -581,7 +583,10 @@ cgb_status mq_autotune(cgb_mq* m, uint64_t n2) {
         m->plans_dirty = true;
     }
     MQ_TRY(mq_upload_plans(m));
-    if (m->tuned_global && !any_new) return CGB_OK;
+    // the grid is timed again only once the plan count has doubled since
+    // its last tuning (a registration alone does not pay for four launches
+    // of the whole set)
+    if (m->tuned_global && (!any_new || m->G < 2 * m->tuned_plans)) return CGB_OK;
     // grid size and stealing for the whole set
     struct Cfg { int bps; bool steal; };
     std::vector<Cfg> cfgs;
@@ -608,6 +613,7 @@ cgb_status mq_autotune(cgb_mq* m, uint64_t n2) {
     m->bps = best_c.bps;
     m->steal = best_c.steal;
     m->tuned_global = true;
+    m->tuned_plans = m->G;
     MCK(cudaMemsetAsync(h->d_scal + 2, 0, sizeof(unsigned long long), h->stream));
     MCK(cudaMemsetAsync(h->d_stats, 0, 8 * sizeof(unsigned long long), h->stream));
     return CGB_OK;

@@ -62,7 +62,7 @@ def bench(args, local: int, log) -> dict:
     m, ids = engine()
     dpairs = [torch.from_numpy(b.astype(np.int32).reshape(-1)).to(dev) for b in batches]
     torch.cuda.synchronize()
-    counts, ms, lat, launches, t_phase = {}, [], [], 0, np.zeros(3)
+    counts, ms, lat, launches, t_phase, merge_bytes = {}, [], [], 0, np.zeros(3), 0
     for b in range(len(batches)):
         l0 = m.kernel_launches()
         pos, _ = m.apply_batch_device(dpairs[b].data_ptr(), len(batches[b]))
@@ -72,6 +72,7 @@ def bench(args, local: int, log) -> dict:
             ms.append(float(t[3]))
             t_phase += np.array([float(x) for x in t[:3]])
             launches += m.kernel_launches() - l0
+            merge_bytes += m.stats()["update_bytes"]
         log(f"c4 batch {b}: {float(t[3]):.1f} ms (merge {float(t[0]):.2f}, delta {float(t[1]):.2f}, match "
             f"{float(t[2]):.1f})")
     variants = [m.query_info(i) for i in ids]
@@ -156,6 +157,7 @@ def bench(args, local: int, log) -> dict:
         "latency_ms": {"p50": float(np.percentile(ms, 50)), "p99": float(np.percentile(ms, 99)), "max": max(ms)},
         "phase_ms_per_batch": {"index_merge": t_phase[0] / len(ms), "delta": t_phase[1] / len(ms),
                                "matching": t_phase[2] / len(ms)},
+        "index_merge_achieved_gbs": (merge_bytes / 1e9) / (t_phase[0] / 1e3) if t_phase[0] > 0 else None,
         "matches_per_s": sum(sum(counts[b]) for b in timed) / (dev_ms / 1e3),
         "e2e": {"value": edges / (sum(e2e_ms) / 1e3), "unit": "edge updates/s",
                 "h2d_bytes_per_step": int(8 * np.mean([len(batches[b]) for b in timed])),
@@ -172,3 +174,32 @@ def bench(args, local: int, log) -> dict:
         },
         "counts_equal_plain": not mismatches, "count_mismatches": mismatches[:10],
     }
+
+
+def profile_run(batches: int = 2, queries: int = 64) -> None:
+    """The multi-query engine alone on the R-MAT 1M/10M stream with the stored
+    query set (first `queries`), `batches` batches: the command profiles use
+    (python -m cgbdsm_b200.multiq [batches] [queries])."""
+    from . import queryset
+    from .engine import MultiQuery
+    from .workloads import SPECS, GraphData
+
+    g = GraphData(SPECS["c2"])
+    qs = queryset.load("c2")[:queries]
+    m = MultiQuery(dfs_budget_ms=120000)
+    m.load_graph(g.labels, g.initial)
+    ids = [m.register(q["qv"], [tuple(e) for e in q["edges"]], q["labels"]) for q in qs]
+    for b, batch in enumerate(g.batches()[:batches]):
+        pos, _ = m.apply_batch(ins=batch)
+        t = m.timings()
+        st = m.stats()
+        print(f"batch {b}: {float(t[3]):.1f} ms (merge {float(t[0]):.2f} ms, {st['update_bytes']} B; delta "
+              f"{float(t[1]):.2f} ms; match {float(t[2]):.1f} ms), total count {int(sum(int(pos[i]) for i in ids))}",
+              flush=True)
+    m.close()
+
+
+if __name__ == "__main__":
+    import sys
+
+    profile_run(*(int(x) for x in sys.argv[1:3]))

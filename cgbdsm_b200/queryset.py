@@ -13,7 +13,14 @@ sizes are recorded.  The rule needs a GPU, so the chosen set is computed once
 and stored (cgbdsm_b200/data/queries_<name>.json):
 
     python -m cgbdsm_b200.queryset c2 64        # R-MAT 1M/10M graph, 64 queries
-    python -m cgbdsm_b200.queryset c3_tree 64   # R-MAT 4M/34M graph (serving mix)
+    python -m cgbdsm_b200.queryset c3_tree 16   # R-MAT 4M/34M graph (serving mix)
+
+Two more reports on a workload's own pattern family (shape and size of its
+spec, query seeds varied), through the plain single-query pipeline (CaLiG
+producer + engine), first batch:
+
+    python -m cgbdsm_b200.queryset sweep c2 24 43      # ms or budget hit per seed
+    python -m cgbdsm_b200.queryset find c2 42 400 3    # first 3 seeds with <= 10^11 matches
 """
 from __future__ import annotations
 
@@ -105,7 +112,67 @@ def select(workload: str, n: int, first_seed: int = 1000) -> dict:
             "the first batch alone: next seed", "queries": chosen, "skipped": skipped}
 
 
+def plain_first_batch(workload: str, g, seed: int, budget_ms: int, workdir: str) -> dict:
+    """The spec's pattern family with query seed `seed` through the plain
+    pipeline: edges, first-batch count and matching time, or the budget hit.
+    g: the workload's GraphData (the same sampler materialize() uses)."""
+    from .engine import CgbError, Engine, Producer
+    from .workloads import SPECS, materialize
+
+    spec = SPECS[workload]
+    p = materialize(spec, workdir)
+    q = g.query(spec.qshape, spec.qsize, seed, spec.max_qedges)
+    if q is None:
+        return {"seed": seed, "no_pattern": True}
+    ql, qe = q
+    qpath = os.path.join(os.path.dirname(p["query"]), f"query_s{seed}.graph")
+    with open(qpath, "w") as f:
+        for i, lb in enumerate(ql):
+            f.write(f"v {i} {lb}\n")
+        for a, b in qe:
+            f.write(f"e {a} {b} 0\n")
+    prod = Producer(qpath, p["data"], p["update"], spec.cli_batch_size)
+    init, dv = prod.initial()
+    r = prod.next()
+    prod.close()
+    e = Engine(dfs_budget_ms=budget_ms)
+    e.load_query(len(ql), qe, ql)
+    e.build_index(init, dv)
+    out = {"seed": seed, "qv": len(ql), "qe": len(qe), "query_file": qpath}
+    try:
+        out["count"] = e.apply_batch(r["dv"], r["ins"], r["del"], r["delta"], r["edge_ok"])
+        out["match_ms"] = round(float(e.timings()[2]), 2)
+    except CgbError as err:
+        out["budget_hit"] = f"> {budget_ms} ms ({err.status})"
+    e.close()
+    return out
+
+
+def _report(argv) -> None:
+    from .workloads import SPECS, GraphData
+
+    workdir = os.environ.get("CGB_BENCH_DIR", "/tmp/cgb_queryset")
+    cmd, workload, lo, hi = argv[0], argv[1], int(argv[2]), int(argv[3])
+    g = GraphData(SPECS[workload])
+    if cmd == "sweep":
+        for seed in range(lo, hi + 1):
+            print(json.dumps(plain_first_batch(workload, g, seed, 3000, workdir)), flush=True)
+        return
+    want = int(argv[4]) if len(argv) > 4 else 1
+    found = 0
+    for seed in range(lo, hi + 1):
+        r = plain_first_batch(workload, g, seed, BUDGET_MS, workdir)
+        ok = "count" in r and r["count"] <= MAX_MATCHES
+        print(json.dumps({**r, "kept": ok}), flush=True)
+        found += ok
+        if found >= want:
+            break
+
+
 if __name__ == "__main__":
+    if sys.argv[1] in ("sweep", "find"):
+        _report(sys.argv[1:])
+        sys.exit(0)
     name, n = sys.argv[1], int(sys.argv[2])
     out = select(name, n)
     os.makedirs(DATA, exist_ok=True)
