@@ -448,6 +448,7 @@ def index_layouts(W, local: int) -> dict:
         gpma_ms.append(gp.stats()["device_us"] / 1e3)
         edits.append(int(len(ins) + len(b["del"])))
         pending = b["delta"]
+    gp.batch_update(pending, np.zeros(0, np.uint64))  # the last batch's delta merge-back (read_index applies it too)
     torch.cuda.synchronize()
     same = bool(np.array_equal(np.sort(e.read_index()), np.sort(np.concatenate(
         [(np.uint64(d) << np.uint64(59)) | gp.extract(d) for d in range(2 * len(w["qe"]))]))))

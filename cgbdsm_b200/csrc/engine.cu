@@ -1156,11 +1156,8 @@ struct SeedGroup {
     // sum over the lanes with `on` of the multiplicity of their own c: only
     // the values of X inside the chunk's range [cmin, cmax] are looked at
     __device__ __forceinline__ uint32_t mult_sum(uint32_t c, bool on, uint32_t lane) const {
-        uint32_t cmin = on ? c : 0xffffffffu, cmax = on ? c : 0u;
-        for (int o = 16; o > 0; o >>= 1) {
-            cmin = min(cmin, __shfl_xor_sync(kFull, cmin, o));
-            cmax = max(cmax, __shfl_xor_sync(kFull, cmax, o));
-        }
+        const uint32_t cmin = __reduce_min_sync(kFull, on ? c : 0xffffffffu);
+        const uint32_t cmax = __reduce_max_sync(kFull, on ? c : 0u);
         if (cmin > cmax) return 0;
         uint32_t r = 0;
         if (n <= 32) {
@@ -1411,12 +1408,11 @@ __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
                 len = r.y + r.w;
                 n_bytes += 16;
             }
-            uint32_t best = len, bl = lane;
-            for (int o = 16; o > 0; o >>= 1) {
-                uint32_t ol = __shfl_xor_sync(kFull, best, o);
-                uint32_t oi = __shfl_xor_sync(kFull, bl, o);
-                if (ol < best || (ol == best && oi < bl)) { best = ol; bl = oi; }
-            }
+            // shortest list, lowest lane on ties: one redux over (length << 5 | lane)
+            // (lengths are below 2^27; a longer one is only a worse generator)
+            const uint32_t key = len == 0xffffffffu ? 0xffffffffu : (min(len, (1u << 27) - 1u) << 5) | lane;
+            const uint32_t kmin = __reduce_min_sync(kFull, key);
+            const uint32_t best = kmin >> 5, bl = kmin & 31u;
             if (lane == j) { st_ncand = 0; st_pos = 0; st_next = 0; st_len = nb ? best : 0; st_gen = bl; }
             __syncwarp();
         };

@@ -634,7 +634,8 @@ class Server:
         neg = np.zeros(MQ_MAX_QUERIES, dtype=np.uint64)
         self._check(self.lib.cgb_server_wait(self.h, ticket, timeout_ms, ctypes.byref(res), pos.ctypes.data,
                                              neg.ctypes.data, MQ_MAX_QUERIES))
-        return {"ticket": res.ticket, "kind": res.kind, "status": res.status, "query_id": res.query_id,
+        err = self.lib.cgb_server_last_error(self.h).decode() if res.status != 0 else ""
+        return {"ticket": res.ticket, "kind": res.kind, "status": res.status, "error": err, "query_id": res.query_id,
                 "live_queries": res.live_queries, "t_submit_ms": res.t_submit_ms, "t_staged_ms": res.t_staged_ms,
                 "t_start_ms": res.t_start_ms, "t_done_ms": res.t_done_ms, "device_ms": res.device_ms,
                 "pos": pos, "neg": neg}

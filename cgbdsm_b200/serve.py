@@ -10,11 +10,10 @@ thread and collects the results.  Reported: edge updates/s and matches/s
 over the run (first arrival to last completion), per-batch latency p50/p99
 (arrival to counts available), queueing delay, device busy fraction.
 
-Offered load: the mean inter-arrival time is set from a short calibration
-(the device time per edge of the first batches, after one warm-up batch in
-which the autotuner runs) so that the device is busy about 80% of the time
-at the initial query count; registrations during the run raise the work per
-batch.
+Offered load: a closed-loop pass on a fresh server (every batch submitted at
+once, the same registrations between the same batches) measures the
+capacity; the Poisson pass then offers 80% of it.  Batch 0 is a warm-up in
+both (the autotuner runs there for the initial queries).
 """
 from __future__ import annotations
 
@@ -91,29 +90,47 @@ def bench(args, local: int, log) -> dict:
     batches = cut_batches(g.stream, SEED_BATCHES)
     log(f"c5: {len(batches)} batches, {sum(len(b) for b in batches)} edges, {n_initial}+{n_arriving} queries")
 
-    server = Server(g.labels, g.initial, device=local, staging_bytes=256 << 20, dfs_budget_ms=args.budget_ms)
-    # the initial queries, then a calibration of the service time on the first batches' sizes
-    for q in initial:
-        r = server.wait(server.submit_register(q["qv"], [tuple(e) for e in q["edges"]], q["labels"]))
-        assert r["status"] == 0
-    # batch 0 runs the autotuner for the initial queries (warm-up); batches
-    # 1-3 calibrate the service time per edge (device time)
-    n_cal = 4
-    cal = run_schedule(server, [(0.0, "batch", b) for b in batches[:n_cal]])[1:]
-    svc_ms_per_edge = sum(r["device_ms"] for r in cal) / sum(len(b) for b in batches[1:n_cal])
-    mean_size = float(np.mean([len(b) for b in batches]))
-    mean_gap_s = svc_ms_per_edge * mean_size / 1e3 / 0.8  # about 80% busy
+    def start():
+        srv = Server(g.labels, g.initial, device=local, staging_bytes=256 << 20, dfs_budget_ms=args.budget_ms)
+        for q in initial:
+            r = srv.wait(srv.submit_register(q["qv"], [tuple(e) for e in q["edges"]], q["labels"]))
+            assert r["status"] == 0, r["error"]
+        # batch 0 runs the autotuner for the initial queries (warm-up)
+        r = run_schedule(srv, [(0.0, "batch", batches[0])])[0]
+        assert r["status"] == 0, r["error"]
+        return srv
+
+    # capacity: a fresh server takes the whole stream back to back (closed
+    # loop), with the same registrations between the same batches
+    n_warm = 1
+    timed = batches[n_warm:]
+    regs_at = np.sort(np.random.default_rng(SEED_QUERIES + 1000).integers(0, len(timed), n_arriving))
+    closed = []
+    for i, b in enumerate(timed):
+        for k in np.nonzero(regs_at == i)[0]:
+            q = arriving[k]
+            closed.append((0.0, "register", (q["labels"], [tuple(e) for e in q["edges"]])))
+        closed.append((0.0, "batch", b))
+    server = start()
+    t0 = time.perf_counter()
+    cap_res = run_schedule(server, closed)
+    cap_s = time.perf_counter() - t0
+    server.close()
+    cap_edges = sum(len(b) for b in timed)
+    capacity = cap_edges / cap_s
+    # the Poisson pass offers 80% of that capacity (same batches and registrations)
+    mean_size = float(np.mean([len(b) for b in timed]))
+    mean_gap_s = mean_size / (0.8 * capacity)
     arng = np.random.default_rng(SEED_BATCHES + 1000)
     t, events = 0.0, []
-    for b in batches[n_cal:]:
+    for i, b in enumerate(timed):
         t += float(arng.exponential(mean_gap_s))
+        for k in np.nonzero(regs_at == i)[0]:
+            q = arriving[k]
+            events.append((t, "register", (q["labels"], [tuple(e) for e in q["edges"]])))
         events.append((t, "batch", b))
-    horizon = t
-    qt = np.sort(np.random.default_rng(SEED_QUERIES + 1000).uniform(0, horizon, n_arriving))
-    for tq, q in zip(qt, arriving):
-        events.append((float(tq), "register", (q["labels"], [tuple(e) for e in q["edges"]])))
-    events.sort(key=lambda e: e[0])
-    log(f"c5: mean inter-arrival {mean_gap_s * 1e3:.1f} ms (service {svc_ms_per_edge * 1e3:.3f} us/edge)")
+    log(f"c5: capacity {capacity:.0f} edge updates/s; mean inter-arrival {mean_gap_s * 1e3:.1f} ms")
+    server = start()
     res = run_schedule(server, events)
     st = server.stats()
     server.close()
@@ -124,6 +141,10 @@ def bench(args, local: int, log) -> dict:
     span_s = (max(r["t_done_ms"] for r in br) - min(r["t_submit_ms"] for r in res)) / 1e3
     edges = sum(len(e[2]) for e in events if e[1] == "batch")
     matches = sum(int(r["pos"].sum(dtype=np.uint64)) for r in ok)
+    # every query's counts are the same in the capacity pass and the Poisson
+    # pass (same batches, registrations between the same batches)
+    cap_b = [r for r in cap_res if r["what"] == "batch"]
+    same = len(cap_b) == len(br) and all(np.array_equal(a["pos"], b["pos"]) for a, b in zip(cap_b, br))
     return {
         "metric": "served edge updates/sec and matches/sec under Poisson arrivals; p50/p99 batch latency",
         "value": edges / span_s, "unit": "edge updates/s",
@@ -131,12 +152,14 @@ def bench(args, local: int, log) -> dict:
                                "(seed 51), sizes log-uniform 1,000-1,000,000 cut from the held-out stream; "
                                f"{n_initial} queries registered at start, {n_arriving} arriving (seed 52)",
                    "batches": len(br), "edges": edges, "mean_interarrival_ms": mean_gap_s * 1e3,
-                   "calibration_batches": n_cal},
+                   "offered_load": "80% of the closed-loop capacity", "warmup_batches": n_warm},
+        "capacity_closed_loop": capacity,
         "matches_per_s": matches / span_s,
         "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
                        "max": float(max(lat))},
         "queue_ms": {"p50": float(np.percentile(queue, 50)), "p99": float(np.percentile(queue, 99))},
         "device_busy_frac": sum(r["device_ms"] for r in ok) / 1e3 / span_s,
-        "rejected": len(br) - len(ok),
+        "rejected": [{"status": r["status"], "error": r["error"]} for r in br if r["status"] != 0],
+        "counts_same_as_closed_loop": bool(same),
         "live_queries_at_end": st["live_queries"],
     }
