@@ -163,11 +163,17 @@ def pct(values, p):
 # plain single-query pipeline (CaLiG producer + engine per pattern)
 # ---------------------------------------------------------------------------
 def produce(spec, rank: int):
-    """Stage 1 for every batch: the product's CaLiG producer (keys, vertex counts)."""
-    from cgbdsm_b200 import Producer
+    """Stage 1 for every batch: the product's CaLiG producer (keys, vertex counts).
+    The workload files are written once, by rank 0, into a directory all
+    ranks of the node share; the others wait at a barrier and read them."""
+    from cgbdsm_b200 import Producer, dist
     from cgbdsm_b200.workloads import materialize, read_query
 
-    paths = materialize(spec, os.environ.get("CGB_BENCH_DIR", f"/tmp/cgb_bench_r{rank}"))
+    workdir = os.environ.get("CGB_BENCH_DIR", "/tmp/cgb_bench")
+    if rank == 0:
+        materialize(spec, workdir)
+    dist.barrier()
+    paths = materialize(spec, workdir)
     t0 = time.perf_counter()
     prod = Producer(paths["query"], paths["data"], paths["update"], spec.cli_batch_size)
     init, dv0 = prod.initial()
@@ -489,7 +495,7 @@ def run_ours(args) -> None:
         if bind.have_ref():
             log("cpu baseline: reference CPU path on batch 0 of each pattern")
             line["cpu_baseline"] = reference_line(names, args.cpu_budget_s,
-                                                  os.environ.get("CGB_BENCH_DIR", "/tmp/cgb_bench_r0"))
+                                                  os.environ.get("CGB_BENCH_DIR", "/tmp/cgb_bench"))
         else:
             line["cpu_baseline"] = {"unavailable": "oracle/_ref/libcgbref.so was not built (no reference tree)"}
     extras = {}
@@ -526,7 +532,7 @@ def run_reference(args) -> None:
     if not bind.have_ref():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libcgbref.so was not built"}))
         return
-    workdir = os.environ.get("CGB_BENCH_DIR", "/tmp/cgb_bench_r0")
+    workdir = os.environ.get("CGB_BENCH_DIR", "/tmp/cgb_bench")
     vals, cb = [], None
     per_step_budget = max(2.0, min(args.cpu_budget_s, 150.0 / max(1, args.steps + args.warmup)))
     for i in range(args.warmup + args.steps):

@@ -95,7 +95,7 @@ def bench(args, local: int, log) -> dict:
 
     # ---- plain pipeline, one query at a time
     log("c4: plain pipeline (CaLiG producer + single-query engine per query)")
-    p = materialize(spec, os.environ.get("CGB_BENCH_DIR", "/tmp/cgb_bench_r0"))
+    p = materialize(spec, os.environ.get("CGB_BENCH_DIR", "/tmp/cgb_bench"))
     qdir = os.path.join(os.path.dirname(p["query"]), "c4_queries")
     os.makedirs(qdir, exist_ok=True)
     plain_gpu = {b: 0.0 for b in PLAIN_BATCHES}

@@ -8,7 +8,7 @@ from cgbdsm_b200 import Producer
 from cgbdsm_b200.workloads import SPECS, materialize
 from oracle import bind
 
-CASES = ["t_tiny", "t_er5", "t_er6", "t_er_sparse", "t_er_tree", "t_rmat"]
+CASES = ["t_tiny", "t_er5", "t_er6", "t_er_sparse", "t_er_tree", "t_rmat", "c1_q25"]
 
 
 def to_original(keys, new2old):
