@@ -42,6 +42,7 @@
 #include <vector>
 
 #include "cgbdsm.h"
+#include "staging_ring.h"
 
 namespace {
 
@@ -80,7 +81,7 @@ struct cgb_server {
     std::string err;
     std::chrono::steady_clock::time_point t0;
     // staging ring (bytes): pinned host mirror + device
-    uint64_t ring_cap = 0, ring_head = 0, ring_used = 0;
+    cgb::StagingRing ring;
     unsigned char* h_ring = nullptr;
     unsigned char* d_ring = nullptr;
     cudaStream_t copy_stream = nullptr;
@@ -107,32 +108,6 @@ namespace {
 
 uint64_t round16(uint64_t x) { return (x + 15) & ~15ull; }
 
-// Ring allocation of len bytes (contiguous), FIFO release.  Caller holds mu.
-bool ring_alloc(cgb_server* s, uint64_t len, uint64_t* off) {
-    if (len > s->ring_cap) return false;
-    if (s->ring_used + len > s->ring_cap) return false;
-    uint64_t tail = (s->ring_head + s->ring_used) % s->ring_cap;  // first free byte
-    if (tail + len > s->ring_cap) {  // wrap: skip the end of the ring
-        const uint64_t skip = s->ring_cap - tail;
-        if (s->ring_used + skip + len > s->ring_cap) return false;
-        s->ring_used += skip;
-        tail = 0;
-    }
-    *off = tail;
-    s->ring_used += len;
-    return true;
-}
-
-void ring_release(cgb_server* s, uint64_t off, uint64_t len) {
-    if (len == 0) return;
-    // FIFO: the released block is the oldest; release through its end
-    const uint64_t end = off + len;
-    const uint64_t freed = (end >= s->ring_head) ? end - s->ring_head : s->ring_cap - s->ring_head + end;
-    s->ring_used -= std::min(freed, s->ring_used);
-    s->ring_head = end % s->ring_cap;
-    if (s->ring_used == 0) s->ring_head = 0;
-}
-
 void stager_loop(cgb_server* s) {
     cudaSetDevice(s->device);
     std::unique_lock<std::mutex> lk(s->mu);
@@ -144,8 +119,8 @@ void stager_loop(cgb_server* s) {
         if (!r) { s->cv_stage.wait(lk); continue; }
         const uint64_t bytes = round16((r->n_ins + r->n_del) * 8);
         uint64_t off = 0;
-        if (bytes && !ring_alloc(s, bytes, &off)) {
-            if (bytes > s->ring_cap) {  // can never be staged: reject in order
+        if (bytes && !s->ring.alloc(bytes, &off)) {
+            if (bytes > s->ring.cap) {  // can never be staged: reject in order
                 r->staged = true;
                 r->status = CGB_ERR_LIMIT;
                 r->err = "batch larger than the staging budget";
@@ -247,7 +222,7 @@ void scheduler_loop(cgb_server* s) {
         if (r->copied) cudaEventDestroy(r->copied);
         r->copied = nullptr;
         lk.lock();
-        ring_release(s, r->ring_off, r->ring_len);
+        s->ring.release(r->ring_off, r->ring_len);
         r->status = st;
         r->err = err;
         if (st == CGB_OK) {
@@ -312,12 +287,12 @@ cgb_status cgb_server_create(const cgb_server_config* cfg, uint32_t n, const uin
     // the budget covers what the server may add on top of the loaded index
     s->base_used = (uint64_t)(total_b - free_b);
     s->budget = s->cfg.hbm_budget_bytes ? s->cfg.hbm_budget_bytes : (uint64_t)(free_b * 0.9);
-    s->ring_cap = round16(std::max<uint64_t>(s->cfg.staging_bytes ? s->cfg.staging_bytes : (64ull << 20), 1 << 20));
-    if (s->ring_cap > s->budget) {
+    s->ring.cap = round16(std::max<uint64_t>(s->cfg.staging_bytes ? s->cfg.staging_bytes : (64ull << 20), 1 << 20));
+    if (s->ring.cap > s->budget) {
         s->err = "staging ring larger than the HBM budget";
         return CGB_ERR_LIMIT;
     }
-    if (cudaMallocHost(&s->h_ring, s->ring_cap) != cudaSuccess || cudaMalloc(&s->d_ring, s->ring_cap) != cudaSuccess ||
+    if (cudaMallocHost(&s->h_ring, s->ring.cap) != cudaSuccess || cudaMalloc(&s->d_ring, s->ring.cap) != cudaSuccess ||
         cudaStreamCreateWithFlags(&s->copy_stream, cudaStreamNonBlocking) != cudaSuccess) {
         s->err = "staging allocation failed";
         return CGB_ERR_OOM;
@@ -424,7 +399,7 @@ cgb_status cgb_server_stats(const cgb_server* s, uint64_t* out8) {
     out8[2] = s->rejected;
     out8[3] = s->live;
     out8[4] = s->queue.size();
-    out8[5] = s->ring_cap;
+    out8[5] = s->ring.cap;
     out8[6] = s->budget;
     out8[7] = (uint64_t)(s->busy_ms * 1000.0);
     return CGB_OK;

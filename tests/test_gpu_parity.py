@@ -421,3 +421,53 @@ def test_seed_shards_match_counted_tail_restatement(name, workdir):
             assert c == want["count"], f"shard {sh['shard']} batch {want['batch']}: {c} != {want['count']}"
             assert [int(x) for x in eng.edge_counts()] == want["edge_counts"]
         eng.close()
+
+
+def test_c2_patterns_match_reference_at_full_size(workdir, tmp_path):
+    """Patterns on the full R-MAT 1M/10M stream (batches of 100,000) whose
+    counts the reference's enumerating CPU path can reach: its counts
+    (tests/golden/c2_patterns.json, made by make_c2_golden.py from
+    oracle/_ref) equal the plain pipeline's (product producer + engine) and
+    the multi-query engine's, batch by batch."""
+    import json
+    import os
+
+    from cgbdsm_b200 import MultiQuery, Producer
+    from cgbdsm_b200.workloads import GraphData
+
+    g_path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "c2_patterns.json")
+    gold = json.load(open(g_path))
+    spec = SPECS["c2"]
+    assert gold["spec"] == repr(spec)
+    p = materialize(spec, workdir)
+    g = GraphData(spec)
+    m = MultiQuery(dfs_budget_ms=120000)
+    m.load_graph(g.labels, g.initial)
+    ids = [m.register(len(q["labels"]), [tuple(e) for e in q["edges"]], q["labels"]) for q in gold["patterns"]]
+    nb = max(len(q["reference_counts"]) for q in gold["patterns"])
+    mq = []
+    for b, batch in enumerate(g.batches()[:nb]):
+        pos, _ = m.apply_batch(ins=batch)
+        mq.append([int(pos[i]) for i in ids])
+    m.close()
+    for k, q in enumerate(gold["patterns"]):
+        want = q["reference_counts"]
+        assert [mq[b][k] for b in range(len(want))] == want, f"pattern {q['index']}: multi-query"
+        qp = str(tmp_path / f"q{k}.graph")
+        with open(qp, "w") as f:
+            for i, lb in enumerate(q["labels"]):
+                f.write(f"v {i} {lb}\n")
+            for a, b in q["edges"]:
+                f.write(f"e {a} {b} 0\n")
+        prod = Producer(qp, p["data"], p["update"], spec.cli_batch_size)
+        init, dv = prod.initial()
+        eng = Engine(dfs_budget_ms=120000)
+        eng.load_query(len(q["labels"]), [tuple(e) for e in q["edges"]], q["labels"])
+        eng.build_index(init, dv)
+        got = []
+        for _ in want:
+            r = prod.next()
+            got.append(eng.apply_batch(r["dv"], r["ins"], r["del"], r["delta"], r["edge_ok"]))
+        eng.close()
+        prod.close()
+        assert got == want, f"pattern {q['index']}: plain pipeline"

@@ -37,3 +37,14 @@ def test_sorted_set_runs_match_set_algorithms(tmp_path):
     out = subprocess.run([exe], capture_output=True, text=True, timeout=300)
     assert out.returncode == 0, out.stdout + out.stderr
     assert "bad=0" in out.stdout
+
+
+@pytest.mark.skipif(shutil.which("g++") is None, reason="g++ not available")
+def test_serving_staging_ring(tmp_path):
+    """The serving loop's staging ring (FIFO allocate / release of edge-pair
+    blocks, wrapping at the end): live blocks inside the ring and disjoint,
+    all space back when every block is released."""
+    exe = _build(tmp_path, "staging_ring")
+    out = subprocess.run([exe], capture_output=True, text=True, timeout=300)
+    assert out.returncode == 0, out.stdout + out.stderr
+    assert "bad=0" in out.stdout and "wraps=0" not in out.stdout
