@@ -224,6 +224,9 @@ def run_pipelines(names: list[str], args, rank: int, world: int, local: int, foo
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.int32, device=dev)
     torch.cuda.synchronize()
     state = {"eng": [new_engine(w) for w in W], "pos": 0}
+    free_b, total_b = torch.cuda.mem_get_info(local)
+    device_gb = (total_b - free_b) / 1e9
+    log(f"device memory in use: {device_gb:.2f} GB of {total_b / 1e9:.0f} GB")
 
     def restart():
         for e in state["eng"]:
@@ -308,6 +311,7 @@ def run_pipelines(names: list[str], args, rank: int, world: int, local: int, foo
                       "stage1_init_s": round(w["stage1_init_s"], 2),
                       "stage1_ms_per_batch": round(float(np.mean(w["stage1_ms"])), 2)} for w in W],
         "setup_s": round(setup_s, 1),
+        "device_memory_gb": round(device_gb, 2),
         "clocks": clk.summary(),
     }
     # the reference's Bottleneck = max(S1, S2) view (main_calig.cpp:435-437):

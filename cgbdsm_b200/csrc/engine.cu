@@ -52,11 +52,10 @@ constexpr uint32_t kTaskCap = 1u << 20;  // stolen-range ring capacity (64 MiB),
 constexpr uint32_t kTaskSlack = 1u << 13; // tickets kept between the ring's tail and head
 constexpr uint64_t kMaxBatchKeys = 1ull << 36;  // per key array of one batch: 512 GiB, beyond any HBM
 
-__constant__ EdgePlan c_plan[kMaxQE];
-// plans are copied to shared memory as 32-bit words (k_dfs_count<true>)
+// Plans belong to a handle (several handles may share a process and a
+// device): they live in the handle's device memory, and the DFS copies them
+// to shared memory as 32-bit words.
 static_assert(sizeof(EdgePlan) % 4 == 0, "EdgePlan must be a whole number of words");
-__constant__ cgb::VbPlan c_vb[kMaxQE];
-__constant__ uint8_t c_dir_edge[kMaxDir];
 
 // ---------------------------------------------------------------------------
 // key packing
@@ -518,8 +517,8 @@ __global__ void k_delta_recs(uint4* rec, uint32_t dvcap, const uint32_t* run_du,
 // Seed ranges: delta entries of direction seed_dir(ei) form one contiguous
 // range of the sorted packed delta array.
 __global__ void k_seed_ranges(const uint64_t* __restrict__ dkeys, uint64_t n, uint32_t B, uint32_t qe,
-                              const uint8_t* qe_dirs /*[qe][2]*/, const uint8_t* edge_ok, int have_ok,
-                              uint32_t* seed_lo, uint32_t* seed_pre) {
+                              const EdgePlan* __restrict__ plans, const uint8_t* qe_dirs /*[qe][2]*/,
+                              const uint8_t* edge_ok, int have_ok, uint32_t* seed_lo, uint32_t* seed_pre) {
     __shared__ uint32_t cnt[kMaxQE];
     const uint32_t t = threadIdx.x;
     auto lower = [&](uint64_t key) {
@@ -531,7 +530,7 @@ __global__ void k_seed_ranges(const uint64_t* __restrict__ dkeys, uint64_t n, ui
         return (uint32_t)lo;
     };
     if (t < qe) {
-        uint32_t s = c_plan[t].seed_dir;
+        uint32_t s = plans[t].seed_dir;
         uint32_t lo = lower((uint64_t)s << (2 * B));
         uint32_t hi = lower((uint64_t)(s + 1) << (2 * B));
         uint32_t d0 = qe_dirs[2 * t], d1 = qe_dirs[2 * t + 1];
@@ -711,9 +710,11 @@ struct DfsArgs {
     const uint32_t* rb_slot;     // run bit sets: slot of (dir, vertex) [nd][dvcap] or nullptr (none)
     const uint32_t* rb_bits;     // [slot][rb_words]
     uint32_t rb_words;
-    const EdgePlan* plans;       // k_dfs_count<true>: every registered query's plans
+    const EdgePlan* plans;       // [qe] (k_dfs_count<true>: every registered query's plans)
     const unsigned int* epoch_ptr;  // non-null: the launch tag is read here (k_epoch_bump)
     uint32_t* touched;           // footprint runs: bit per record resolved (nullptr: off)
+    unsigned long long* lsum_tab;  // level-sum table [lsum_mask + 1][2], zeroed before the launch (nullptr: none)
+    uint32_t lsum_mask;
 };
 
 // Footprint of a matching launch: the bytes of every distinct record it
@@ -783,17 +784,22 @@ struct RunBits {
     __device__ __forceinline__ void note(uint32_t k, size_t at) const {
         if (slot) bslot[k] = __ldg(slot + at);
     }
-    // x in the resolved list bn[k] = r: one bit test for a long old run
-    __device__ __forceinline__ bool has(uint32_t k, const uint4& r, const uint32_t* __restrict__ pool,
-                                       const uint32_t* __restrict__ dval, uint32_t x) const {
-        if (slot) {
-            const uint32_t sl = bslot[k];
-            if (sl != kNoSlot) {
-                if ((__ldg(bits + (size_t)sl * words + (x >> 5)) >> (x & 31)) & 1u) return true;
-                return r.w && sorted_has_bl(dval + r.z, r.w, x);
-            }
+    // a lane's own record (not kept in bslot): nothing to note here
+    __device__ __forceinline__ void touch(size_t) const {}
+    __device__ __forceinline__ uint32_t slot_at(size_t at) const { return slot ? __ldg(slot + at) : kNoSlot; }
+    // x in the list r whose old run has the bit set sl: one bit test for a long old run
+    __device__ __forceinline__ bool has_slot(uint32_t sl, const uint4& r, const uint32_t* __restrict__ pool,
+                                            const uint32_t* __restrict__ dval, uint32_t x) const {
+        if (sl != kNoSlot) {
+            if ((__ldg(bits + (size_t)sl * words + (x >> 5)) >> (x & 31)) & 1u) return true;
+            return r.w && sorted_has_bl(dval + r.z, r.w, x);
         }
         return list_contains(pool, dval, r, x);
+    }
+    // x in the resolved list bn[k] = r
+    __device__ __forceinline__ bool has(uint32_t k, const uint4& r, const uint32_t* __restrict__ pool,
+                                       const uint32_t* __restrict__ dval, uint32_t x) const {
+        return has_slot(slot ? bslot[k] : kNoSlot, r, pool, dval, x);
     }
 };
 
@@ -804,8 +810,9 @@ struct RunBitsCount : RunBits {
     uint32_t* touched;
     __device__ __forceinline__ void note(uint32_t k, size_t at) const {
         RunBits::note(k, at);
-        atomicOr(touched + (at >> 5), 1u << (at & 31));
+        touch(at);
     }
+    __device__ __forceinline__ void touch(size_t at) const { atomicOr(touched + (at >> 5), 1u << (at & 31)); }
 };
 
 
@@ -1032,10 +1039,14 @@ __device__ unsigned long long tail_eval(const EdgePlan& P, const uint32_t* m, ui
 // Tail count for the candidate c of the last core position, evaluated by
 // one lane (plans with tail_lane): every cached subset count is prefix-only
 // and c is removed from it when c lies in all of the subset's lists (only
-// for groups sharing the last core vertex's label).  Lanes diverge only in
-// the searches.
+// for groups sharing the last core vertex's label).  A group whose one list
+// hangs off the last core position (tail_lane 2, cached as kDynamic) counts
+// c's own list: its length minus the excluded prefix vertices it holds (c
+// is not in its own list: no self-loops on this path).  Lanes diverge only
+// in the loads and searches.
 template <class RB>
 __device__ unsigned long long tail_eval_lane(const EdgePlan& P, const uint4* bn, const unsigned long long* cache,
+                                             const uint4* __restrict__ rec, uint32_t dvcap, const uint32_t* m,
                                              const uint32_t* __restrict__ pool, const uint32_t* __restrict__ dval,
                                              uint32_t c, unsigned long long& bytes, const RB& rb) {
     const uint32_t nc = P.n_core, n = P.n, j = nc - 1;
@@ -1049,7 +1060,23 @@ __device__ unsigned long long tail_eval_lane(const EdgePlan& P, const uint4* bn,
         unsigned long long sc[8];
         for (uint32_t mask = 1; mask < (1u << k); ++mask) {
             unsigned long long cv = cache[t * 8 + mask];
-            if (same_label) {
+            if (cv == kDynamic) {
+                const uint32_t q = P.bn_off[t];
+                const size_t at = (size_t)P.bn_dir[q] * dvcap + c;
+                uint4 r = rec[at];
+                if (!P.bn_dvis[q]) r.w = 0;
+                rb.touch(at);
+                bytes += 16;
+                cv = (unsigned long long)r.y + r.w;
+                const uint32_t ex = P.excl[t] & ((1u << j) - 1u);
+                if (ex) {
+                    const uint32_t sl = rb.slot_at(at);
+                    for (uint32_t b = ex; b; b &= b - 1) {
+                        bytes += 32u * (33u - __clz(r.y | 1u));
+                        cv -= rb.has_slot(sl, r, pool, dval, m[__ffs(b) - 1]) ? 1ull : 0ull;
+                    }
+                }
+            } else if (same_label) {
                 bool in = true;
                 for (uint32_t i = 0; i < k && in; ++i)
                     if (mask & (1u << i))
@@ -1078,6 +1105,80 @@ __device__ unsigned long long tail_const_value(const EdgePlan& P, const unsigned
         uint32_t e = t;
         while (e < P.n && P.tail_gid[e] == P.tail_gid[t]) ++e;
         prod *= group_count(cache + t * 8, e - t);
+        t = e;
+    }
+    return prod;
+}
+
+// Level sums (plans with level_sum): the product of the lengths of c's own
+// lists towards the tail vertices in sum_tails (1 when there are none).
+template <class RB>
+__device__ __forceinline__ unsigned long long sum_lens(const EdgePlan& P, const uint4* __restrict__ rec,
+                                                       uint32_t dvcap, uint32_t c, const RB& rb) {
+    unsigned long long v = 1;
+    for (uint32_t b = P.sum_tails; b; b &= b - 1) {
+        const uint32_t q = P.bn_off[__ffs(b) - 1];
+        const size_t at = (size_t)P.bn_dir[q] * dvcap + c;
+        uint4 r = rec[at];
+        if (!P.bn_dvis[q]) r.w = 0;
+        rb.touch(at);
+        v *= (unsigned long long)r.y + r.w;
+    }
+    return v;
+}
+
+// Level-sum table: slots of {key, value}; key 0 = empty, K << 1 = claimed
+// by a warp computing the value, K << 1 | 1 = value published, with
+// K = (plan << 27 | vertex) + 1.  Zeroed before every launch, so values never
+// outlive the index state they were computed on.  A lookup probes
+// kLsumProbes slots; a warp that finds its key busy or every probe taken by
+// other keys computes the value itself (nobody waits).
+constexpr uint32_t kLsumProbes = 4;
+constexpr uint32_t kLsumNone = 0xffffffffu;
+
+__device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long* p) {
+    unsigned long long v;
+    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release_u64(unsigned long long* p, unsigned long long v) {
+    asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+// One thread: the published value of K (hit = true), or the slot this
+// thread claimed for K (to publish into), or kLsumNone.
+__device__ __forceinline__ uint32_t lsum_find(unsigned long long* tab, uint32_t mask, unsigned long long K, bool& hit,
+                                              unsigned long long& val) {
+    uint32_t s = (uint32_t)((K * 0x9e3779b97f4a7c15ull) >> 32) & mask;
+    for (uint32_t probe = 0; probe < kLsumProbes; ++probe, s = (s + 1) & mask) {
+        unsigned long long* slot = tab + 2 * (size_t)s;
+        unsigned long long k = ld_acquire_u64(slot);
+        if (k == 0) {
+            const unsigned long long prev = atomicCAS(slot, 0ull, K << 1);
+            if (prev == 0) return s;
+            k = prev;
+            if (k & 1ull) k = ld_acquire_u64(slot);  // published meanwhile: read with acquire
+        }
+        if ((k >> 1) == K) {
+            if (k & 1ull) {
+                hit = true;
+                val = *(volatile const unsigned long long*)(slot + 1);
+            }
+            return kLsumNone;  // published, or being computed by another warp
+        }
+    }
+    return kLsumNone;
+}
+
+// Product of the cached prefix-only group counts (groups whose lists hang
+// off the last core position are cached as kDynamic and left out).
+__device__ unsigned long long tail_static_product(const EdgePlan& P, const unsigned long long* cache) {
+    unsigned long long prod = 1;
+    uint32_t t = P.n_core;
+    while (t < P.n && prod) {
+        uint32_t e = t;
+        while (e < P.n && P.tail_gid[e] == P.tail_gid[t]) ++e;
+        if (cache[t * 8 + 1] != kDynamic) prod *= group_count(cache + t * 8, e - t);
         t = e;
     }
     return prod;
@@ -1208,11 +1309,12 @@ __host__ __device__ __forceinline__ uint32_t seed_shard(uint32_t ei, uint32_t x,
 constexpr uint32_t kCandBits = 27;
 constexpr uint32_t kCandMask = (1u << kCandBits) - 1u;
 
-// kMulti = false: one query, plans in constant memory (c_plan), seed table
-// in shared memory.  kMulti = true: the plans of every registered query in
-// global memory (a.plans, one per (query, edge); a.qe of them), seed table
-// searched in global memory, each warp's current plan copied to shared
-// memory when its unit changes plan.
+// kMulti = false: one query, its plans (a.plans, one per edge, at most
+// kMaxQEKeyed) and seed table copied to shared memory by every block.
+// kMulti = true: the plans of every registered query in global memory
+// (a.plans, one per (query, edge); a.qe of them), seed table searched in
+// global memory, each warp's current plan copied to shared memory when its
+// unit changes plan.
 template <bool kMulti, bool kFoot = false>
 __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
     __shared__ uint32_t s_cand[kDfsWarps][kMaxQV][32];
@@ -1222,7 +1324,7 @@ __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
     __shared__ unsigned long long s_tc[kDfsWarps][kMaxQV * 8];
     __shared__ uint32_t s_pre[kMulti ? 1 : kMaxQE + 1];
     __shared__ uint32_t s_lo[kMulti ? 1 : kMaxQE];
-    __shared__ __align__(16) EdgePlan s_plan[kMulti ? kDfsWarps : 1];
+    __shared__ __align__(16) EdgePlan s_plan[kMulti ? kDfsWarps : cgb::kMaxQEKeyed];
 
     const uint32_t lane = threadIdx.x & 31;
     const uint32_t w = threadIdx.x >> 5;
@@ -1233,11 +1335,15 @@ __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
     if (!kMulti) {
         if (threadIdx.x <= a.qe) s_pre[threadIdx.x] = a.seed_pre[threadIdx.x];
         if (threadIdx.x < a.qe) s_lo[threadIdx.x] = a.seed_lo[threadIdx.x];
+        const uint32_t* src = reinterpret_cast<const uint32_t*>(a.plans);
+        uint32_t* dst = reinterpret_cast<uint32_t*>(s_plan);
+        for (uint32_t t = threadIdx.x; t < a.qe * (uint32_t)(sizeof(EdgePlan) / 4); t += blockDim.x)
+            dst[t] = __ldg(src + t);
     }
     __syncthreads();
     auto pre_at = [&](uint32_t e) -> uint32_t { return kMulti ? __ldg(a.seed_pre + e) : s_pre[e]; };
     auto lo_at = [&](uint32_t e) -> uint32_t { return kMulti ? __ldg(a.seed_lo + e) : s_lo[e]; };
-    auto grouped_at = [&](uint32_t e) -> bool { return kMulti ? a.plans[e].grouped != 0 : c_plan[e].grouped != 0; };
+    auto grouped_at = [&](uint32_t e) -> bool { return kMulti ? a.plans[e].grouped != 0 : s_plan[e].grouped != 0; };
     int plan_in_smem = -1;  // kMulti: plan held in s_plan[w]
     // every engine walks all seeds; a sharded one skips the groups of other shards
     const uint32_t total = pre_at(a.qe);
@@ -1265,6 +1371,8 @@ __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
     bool out_of_time = false;
     uint32_t ticket = kNoTicket;  // lane 0: ticket of the task ring this warp waits on
     uint32_t dirty = 0;  // shallowest position changed since the tail cache was filled (kClean: none)
+    unsigned long long lsum = 0;  // level sum over G of the current m[p] (plans with level_sum)
+    uint32_t ls_dirty = 0;        // shallowest position changed since lsum was computed (kClean: none)
     unsigned long long tail_const = 0;  // tail count of the current prefix (plans with tail_const)
     uint32_t idle_spins = 0;
 
@@ -1370,7 +1478,7 @@ __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
             __syncwarp();
             plan_in_smem = ei;
         }
-        const EdgePlan& P = kMulti ? s_plan[w] : c_plan[ei];
+        const EdgePlan& P = kMulti ? s_plan[w] : s_plan[ei];
         const bool tail_cache = a.tail_cache && !(P.flags & cgb::kPlanNoTailCache);
         const uint32_t nc = P.n_core;
         const bool has_tail = nc < P.n;
@@ -1418,6 +1526,8 @@ __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
         };
 
         dirty = 0;  // new unit: every cached tail count is stale
+        ls_dirty = 0;
+        const bool level_sum = P.level_sum && !a.vb && !self_loops && (tail_cache || !has_tail);
         setup(jbase);
         if (kind == 2 && lane == jbase) { st_gen = tgen; st_next = tlo; st_len = thi; }
         if (P.grouped) {
@@ -1442,6 +1552,7 @@ __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
                 if (lane == 0) m[j] = s_cand[w][j][pos] & kCandMask;
                 __syncwarp();
                 dirty = min(dirty, j);
+                ls_dirty = min(ls_dirty, j);
                 if (P.grouped) {
                     uint32_t h = __shfl_sync(kFull, st_hs, j);
                     if ((P.hit_mask >> j) & 1u) h += X.mult(m[j], lane);
@@ -1453,6 +1564,64 @@ __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
             }
             const uint32_t gnext = __shfl_sync(kFull, st_next, j);
             uint32_t glen = __shfl_sync(kFull, st_len, j);
+            if (level_sum && j == nc - 1 && gnext == 0 && glen > 0) {
+                // the whole last level at once (not a stolen part of it): the
+                // level sum over G, less the matched prefix vertices in G
+                const uint32_t o0 = P.bn_off[j];
+                const uint4 gr = bn[o0];
+                if (glen == gr.y + gr.w) {
+                    if (ls_dirty <= P.bn_pos[o0]) {
+                        // the sum over G of the owner m[p]: from the table, or
+                        // scanned (and published when this warp claimed its slot)
+                        const unsigned long long K = (((unsigned long long)ei << 27) | m[P.bn_pos[o0]]) + 1ull;
+                        uint32_t claim = kLsumNone;
+                        bool hit = false;
+                        unsigned long long hv = 0;
+                        if (a.lsum_tab && lane == 0) claim = lsum_find(a.lsum_tab, a.lsum_mask, K, hit, hv);
+                        if (__shfl_sync(kFull, hit ? 1u : 0u, 0)) {
+                            lsum = __shfl_sync(kFull, hv, 0);
+                        } else {
+                            unsigned long long sv = 0;
+                            for (uint32_t idx = lane; idx < glen; idx += 32) {
+                                const uint32_t c =
+                                    idx < gr.y ? __ldg(a.pool + gr.x + idx) : __ldg(a.dval + gr.z + (idx - gr.y));
+                                sv += sum_lens(P, a.rec, a.dvcap, c, rb);
+                                n_bytes += 4;
+                            }
+                            lsum = warp_sum(sv);
+                            if (lane == 0 && claim != kLsumNone) {
+                                a.lsum_tab[2 * (size_t)claim + 1] = lsum;
+                                st_release_u64(a.lsum_tab + 2 * (size_t)claim, (K << 1) | 1ull);
+                            }
+                        }
+                        ls_dirty = kClean;
+                    }
+                    unsigned long long corr = 0;
+                    bool hit = false;
+                    if (lane < j && ((P.sum_same >> lane) & 1u)) {
+                        const uint32_t x = m[lane];
+                        if (x != kNoVertex && rb.has(o0, gr, a.pool, a.dval, x)) {
+                            hit = true;
+                            corr = sum_lens(P, a.rec, a.dvcap, x, rb);
+                        }
+                    }
+                    corr = warp_sum(corr);
+                    const uint32_t nhit = __popc(__ballot_sync(kFull, hit));
+                    unsigned long long v = lsum - corr;
+                    if (has_tail) {
+                        if (dirty <= P.tail_dep)
+                            tail_prepare(P, m, bn, s_tc[w], dirty, a.rec, a.dvcap, a.pool, a.dval, self_loops, lane,
+                                         n_bytes, rb);
+                        dirty = kClean;
+                        v *= tail_static_product(P, s_tc[w]);
+                    }
+                    if (P.grouped) v *= (unsigned long long)(X.n - __shfl_sync(kFull, st_hs, j));
+                    if (lane == 0) { cnt += v; n_tail += glen - nhit; }
+                    if (lane == j) st_next = glen;
+                    __syncwarp();
+                    continue;
+                }
+            }
             if (gnext < glen) {
                 const uint32_t g = __shfl_sync(kFull, st_gen, j);
                 // While warps wait for tasks, hand the work not yet started at the
@@ -1573,7 +1742,8 @@ __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
                             }
                             if (lane == 0) { cnt += wsum * tail_const; n_tail += __popc(bal); }
                         }
-                    } else if (has_tail && P.tail_lane && tail_cache && !hit_last) {
+                    } else if (has_tail && P.tail_lane && (P.tail_lane == 1 || !self_loops) && tail_cache &&
+                               !hit_last) {
                         // the tail depends on the candidate only through prefix-only
                         // lists: every lane counts its own candidate's tail
                         const uint32_t bal = __ballot_sync(kFull, ok);
@@ -1582,7 +1752,8 @@ __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
                                 tail_prepare(P, m, bn, s_tc[w], dirty, a.rec, a.dvcap, a.pool, a.dval, self_loops, lane, n_bytes, rb);
                             dirty = kClean;
                             if (ok) {
-                                const unsigned long long tc = tail_eval_lane(P, bn, s_tc[w], a.pool, a.dval, c, n_bytes, rb);
+                                const unsigned long long tc =
+                                    tail_eval_lane(P, bn, s_tc[w], a.rec, a.dvcap, m, a.pool, a.dval, c, n_bytes, rb);
                                 cnt += P.grouped ? tc * (unsigned long long)(X.n - hs) : tc;
                             }
                             if (lane == 0) n_tail += __popc(bal);
@@ -1658,26 +1829,28 @@ __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
 // that some embedding mapping ei to a delta edge can place at u.
 // ---------------------------------------------------------------------------
 // Rebuilt (ei, u) start empty, the others all ones (graph_gpu.cu:818-828).
-__global__ void k_vb_fill(uint32_t* vb, uint32_t qe, uint32_t qv, uint32_t stride) {
+__global__ void k_vb_fill(const cgb::VbPlan* __restrict__ vbp, uint32_t* vb, uint32_t qe, uint32_t qv,
+                          uint32_t stride) {
     const size_t n = (size_t)qe * qv * stride;
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
         const uint32_t ei = (uint32_t)(i / ((size_t)qv * stride));
         const uint32_t u = (uint32_t)((i / stride) % qv);
-        vb[i] = ((c_vb[ei].rebuild >> u) & 1u) ? 0u : 0xffffffffu;
+        vb[i] = ((vbp[ei].rebuild >> u) & 1u) ? 0u : 0xffffffffu;
     }
 }
 
 // Endpoints of ei: vertices with a delta list in ei's own direction
 // (setInitialValidBitsAll1Bit, indexing.cu:2295-2317), set from the sorted
 // packed delta keys (d << 2B | u << B | v): one bit per key, no full sweep.
-__global__ void k_vb_seed(const uint64_t* __restrict__ dkeys, uint64_t n, uint32_t B, uint32_t* vb, uint32_t qv,
+__global__ void k_vb_seed(const cgb::VbPlan* __restrict__ vbp, const uint8_t* __restrict__ dir_edge,
+                          const uint64_t* __restrict__ dkeys, uint64_t n, uint32_t B, uint32_t* vb, uint32_t qv,
                           uint32_t stride) {
     const uint64_t m = (1ull << B) - 1ull;
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
         const uint64_t k = dkeys[i];
         const uint32_t d = (uint32_t)(k >> (2 * B)), u = (uint32_t)((k >> B) & m);
-        const uint32_t ei = c_dir_edge[d];
-        const cgb::VbPlan& P = c_vb[ei];
+        const uint32_t ei = dir_edge[d];
+        const cgb::VbPlan& P = vbp[ei];
         const uint32_t qu = d == P.d01 ? P.vs[0] : P.vs[1];
         atomicOr(vb + ((size_t)ei * qv + qu) * stride + (u >> 5), 1u << (u & 31));
     }
@@ -1688,11 +1861,11 @@ __global__ void k_vb_seed(const uint64_t* __restrict__ dkeys, uint64_t n, uint32
 // neighbour (old run, plus the delta run when visible) holds a vertex whose
 // bit is set (checkAllConstraintsAndSetBitsAll1Bit, indexing.cu:2319-2377).
 // One warp per mask word, one lane per vertex.
-__global__ void k_vb_depth(const uint4* __restrict__ rec, uint32_t dvcap, const uint32_t* __restrict__ pool,
-                           const uint32_t* __restrict__ dval, uint32_t dv, uint32_t* vb, uint32_t qv,
-                           uint32_t stride, uint32_t depth) {
+__global__ void k_vb_depth(const cgb::VbPlan* __restrict__ vbp, const uint4* __restrict__ rec, uint32_t dvcap,
+                           const uint32_t* __restrict__ pool, const uint32_t* __restrict__ dval, uint32_t dv,
+                           uint32_t* vb, uint32_t qv, uint32_t stride, uint32_t depth) {
     const uint32_t ei = blockIdx.y;
-    const cgb::VbPlan& P = c_vb[ei];
+    const cgb::VbPlan& P = vbp[ei];
     const uint32_t u = P.vs[depth];
     if (!((P.rebuild >> u) & 1u)) return;
     uint32_t* out = vb + ((size_t)ei * qv + u) * stride;
@@ -1808,6 +1981,9 @@ struct cgb_handle {
     bool have_query = false;
     cgb::QueryMeta q;
     EdgePlan plans[kMaxQE];
+    EdgePlan* d_plans = nullptr;       // [kMaxQE] device copy of plans
+    cgb::VbPlan* d_vbplans = nullptr;  // [kMaxQE] valid-bit plans
+    uint8_t* d_dir_edge = nullptr;     // [kMaxDir] query edge of each direction
     uint8_t* d_qe_dirs = nullptr;  // [qe][2]
     uint8_t* d_edge_ok = nullptr;  // [kMaxQE]
 
@@ -1861,6 +2037,8 @@ struct cgb_handle {
     uint32_t rb_min_len = kRunBitsMinLen;
     uint8_t* d_rev = nullptr;          // reverse direction of each direction
     uint32_t* d_touched = nullptr; size_t touched_cap = 0;  // footprint runs: record bit set
+    unsigned long long* d_lsum = nullptr;  // level-sum table, sized with the record table
+    uint32_t lsum_slots = 0;
 
     // label-keyed mode (the multi-query engine's data-graph index): the
     // "direction" of a key is the label of its target vertex, the delta keys
@@ -1951,6 +2129,29 @@ cgb_status ensure_dvcap(cgb_handle* h, uint32_t dv) {
     h->rec = nr;
     h->dvcap = nc;
     h->rb_valid = false;  // the slot table and the bit sets follow the record layout
+    // level-sum table: about two slots per vertex, 2^12 to 2^24 slots (16 B each)
+    uint32_t slots = 1u << 12;
+    while (slots < (1u << 24) && slots < 2ull * nc) slots <<= 1;
+    if (slots > h->lsum_slots) {
+        if (h->d_lsum) CK(cudaFree(h->d_lsum));
+        h->d_lsum = nullptr;
+        h->lsum_slots = 0;
+        CK(cudaMalloc(&h->d_lsum, (size_t)slots * 2 * sizeof(unsigned long long)));
+        h->lsum_slots = slots;
+    }
+    return CGB_OK;
+}
+
+// Level-sum table of a DFS launch (none when no plan uses level sums);
+// lsum_clear zeroes it on the stream before each launch.
+void lsum_bind(const cgb_handle* h, bool any, DfsArgs& da) {
+    const bool on = any && h->d_lsum;
+    da.lsum_tab = on ? h->d_lsum : nullptr;
+    da.lsum_mask = on ? h->lsum_slots - 1 : 0;
+}
+cgb_status lsum_clear(cgb_handle* h, const DfsArgs& da) {
+    if (da.lsum_tab)
+        CK(cudaMemsetAsync(da.lsum_tab, 0, ((size_t)da.lsum_mask + 1) * 2 * sizeof(unsigned long long), h->stream));
     return CGB_OK;
 }
 
@@ -2262,6 +2463,9 @@ cgb_status cgb_create(const cgb_config* cfg, cgb_handle** out) {
     CKC(cudaMemset(h->d_tasks, 0, (size_t)kTaskCap * kTaskWords * sizeof(uint32_t)));
     CKC(cudaMalloc(&h->d_qe_dirs, 2 * kMaxQE));
     CKC(cudaMalloc(&h->d_edge_ok, kMaxQE));
+    CKC(cudaMalloc(&h->d_plans, sizeof(EdgePlan) * kMaxQE));
+    CKC(cudaMalloc(&h->d_vbplans, sizeof(cgb::VbPlan) * kMaxQE));
+    CKC(cudaMalloc(&h->d_dir_edge, kMaxDir));
     for (auto& ev : h->ev) CKC(cudaEventCreate(&ev));
 #undef CKC
     *out = h;
@@ -2277,7 +2481,8 @@ void cgb_destroy(cgb_handle* h) {
                     h->d_dkeys, h->d_dkeys_alt, h->d_dval, h->d_ddu, h->d_drun_du, h->d_drun_len, h->d_drun_off,
                     h->d_seed, h->d_counts, h->d_stats, h->d_tasks, h->d_qctr, h->d_temp, h->d_qe_dirs, h->d_edge_ok,
                     h->d_vb, h->d_rb_slot, h->d_rb_sel, h->d_rb_bits, h->d_rb_ctr, h->d_rb_new, h->d_small_runs,
-                    h->d_big_runs, h->d_tiny_runs, h->d_list_ctr, h->d_rev, h->d_touched};
+                    h->d_big_runs, h->d_tiny_runs, h->d_list_ctr, h->d_rev, h->d_touched, h->d_plans,
+                    h->d_vbplans, h->d_dir_edge, h->d_lsum};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (h->h_scal) cudaFreeHost(h->h_scal);
@@ -2347,8 +2552,9 @@ cgb_status cgb_build_index(cgb_handle* h, const uint64_t* keys, uint64_t n, uint
     float avg[kMaxDir] = {0};
     for (uint32_t d = 0; d < h->nd; ++d) avg[d] = nodes[d] ? (float)card[d] / (float)nodes[d] : 0.f;
     cgb::plan_edges(h->q, avg, h->plans, !(h->cfg.flags & CGB_FLAG_ENUMERATE_TAIL),
-                    !(h->cfg.flags & CGB_FLAG_PLAIN_CORE_ORDER), !(h->cfg.flags & CGB_FLAG_NO_SEED_GROUPS));
-    CK(cudaMemcpyToSymbol(c_plan, h->plans, sizeof(EdgePlan) * kMaxQE));
+                    !(h->cfg.flags & CGB_FLAG_PLAIN_CORE_ORDER), !(h->cfg.flags & CGB_FLAG_NO_SEED_GROUPS),
+                    !(h->cfg.flags & CGB_FLAG_WARP_TAIL), !(h->cfg.flags & CGB_FLAG_NO_LEVEL_SUM));
+    CK(cudaMemcpy(h->d_plans, h->plans, sizeof(EdgePlan) * kMaxQE, cudaMemcpyHostToDevice));
     {
         // valid-bit plans from the reference's starting edge
         cgb::select_starting_edge(h->q, card.data(), avg, h->vb_start);
@@ -2357,8 +2563,8 @@ cgb_status cgb_build_index(cgb_handle* h, const uint64_t* keys, uint64_t n, uint
         h->vb_plan_error = cgb::plan_valid_bits(h->q, h->vb_start, vbp);
         if (!h->vb_plan_error.empty() && (h->cfg.flags & (CGB_FLAG_VALID_BITS | CGB_FLAG_MASK_PRUNE)))
             return fail(h, CGB_ERR_ARG, "valid bits: %s", h->vb_plan_error.c_str());
-        CK(cudaMemcpyToSymbol(c_vb, vbp, sizeof(vbp)));
-        CK(cudaMemcpyToSymbol(c_dir_edge, h->q.dir_to_edge, sizeof(h->q.dir_to_edge)));
+        CK(cudaMemcpy(h->d_vbplans, vbp, sizeof(vbp), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(h->d_dir_edge, h->q.dir_to_edge, sizeof(h->q.dir_to_edge), cudaMemcpyHostToDevice));
     }
 
     h->dv = dv_count;
@@ -2435,7 +2641,7 @@ cgb_status cgb_apply_batch_device(cgb_handle* h, uint32_t dv_count, const uint64
                                                                    h->d_drun_off, h->d_num_runs + 1, B, 0);
         LAUNCHED();
         if (edge_ok) CK(cudaMemcpyAsync(h->d_edge_ok, edge_ok, h->q.qe, cudaMemcpyHostToDevice, h->stream));
-        k_seed_ranges<<<1, 32, 0, h->stream>>>(h->d_dkeys, n_delta, B, h->q.qe, h->d_qe_dirs, h->d_edge_ok,
+        k_seed_ranges<<<1, 32, 0, h->stream>>>(h->d_dkeys, n_delta, B, h->q.qe, h->d_plans, h->d_qe_dirs, h->d_edge_ok,
                                                edge_ok ? 1 : 0, h->d_seed, h->d_seed + kMaxQE);
         LAUNCHED();
         CK(cudaGetLastError());
@@ -2449,14 +2655,15 @@ cgb_status cgb_apply_batch_device(cgb_handle* h, uint32_t dv_count, const uint64
             CK(cudaEventRecord(h->ev[6], h->stream));
             const size_t words = (size_t)qe * qv * stride;
             k_vb_fill<<<(unsigned)std::min<size_t>((words + 255) / 256, (size_t)h->num_sms * 16), 256, 0,
-                        h->stream>>>(h->d_vb, qe, qv, stride);
+                        h->stream>>>(h->d_vbplans, h->d_vb, qe, qv, stride);
             LAUNCHED();
-            k_vb_seed<<<grid_for(h, n_delta), 256, 0, h->stream>>>(h->d_dkeys, n_delta, B, h->d_vb, qv, stride);
+            k_vb_seed<<<grid_for(h, n_delta), 256, 0, h->stream>>>(h->d_vbplans, h->d_dir_edge, h->d_dkeys, n_delta,
+                                                                   B, h->d_vb, qv, stride);
             LAUNCHED();
             const dim3 g((unsigned)std::min<uint32_t>((stride + 7) / 8, (uint32_t)h->num_sms * 8), qe);
             for (uint32_t d = 2; d < qv; ++d) {
-                k_vb_depth<<<g, 256, 0, h->stream>>>(h->rec, h->dvcap, h->pool, h->d_dval, dv_count, h->d_vb, qv,
-                                                     stride, d);
+                k_vb_depth<<<g, 256, 0, h->stream>>>(h->d_vbplans, h->rec, h->dvcap, h->pool, h->d_dval, dv_count,
+                                                     h->d_vb, qv, stride, d);
                 LAUNCHED();
             }
             CK(cudaGetLastError());
@@ -2505,7 +2712,7 @@ cgb_status cgb_apply_batch_device(cgb_handle* h, uint32_t dv_count, const uint64
         da.rb_slot = rb_on ? h->d_rb_slot : nullptr;
         da.rb_bits = h->d_rb_bits;
         da.rb_words = h->rb_words;
-        da.plans = nullptr;
+        da.plans = h->d_plans;
         da.epoch_ptr = nullptr;
         da.touched = nullptr;
         const bool footprint = (h->cfg.flags & CGB_FLAG_FOOTPRINT) != 0;
@@ -2525,6 +2732,10 @@ cgb_status cgb_apply_batch_device(cgb_handle* h, uint32_t dv_count, const uint64
         }
         int bps = h->dfs_occupancy;
         if (h->cfg.dfs_blocks_per_sm) bps = std::min(bps, (int)h->cfg.dfs_blocks_per_sm);
+        bool any_sum = false;
+        for (uint32_t e = 0; e < h->q.qe; ++e) any_sum |= h->plans[e].level_sum != 0;
+        lsum_bind(h, any_sum, da);
+        if ((s = lsum_clear(h, da)) != CGB_OK) return s;
         if (footprint) k_dfs_count<false, true><<<h->num_sms * bps, kDfsWarps * 32, 0, h->stream>>>(da);
         else k_dfs_count<false><<<h->num_sms * bps, kDfsWarps * 32, 0, h->stream>>>(da);
         LAUNCHED();

@@ -432,6 +432,7 @@ DfsArgs mq_dfs_args(cgb_mq* m, const EdgePlan* plans, uint32_t G, uint64_t budge
     da.plans = plans;
     da.touched = nullptr;
     da.budget_ns = budget_ms * 1000000ull;
+    lsum_bind(h, true, da);
     return da;
 }
 
@@ -452,6 +453,7 @@ cgb_status mq_match_enqueue(cgb_mq* m, const EdgePlan* plans, const uint16_t* pa
     k_epoch_bump<<<1, 1, 0, h->stream>>>(h->d_epoch);
     LAUNCHED();
     DfsArgs da = mq_dfs_args(m, plans, G, budget_ms, steal);
+    if (lsum_clear(h, da) != CGB_OK) return mq_fail(m, CGB_ERR_CUDA, "%s", h->err.c_str());
     k_dfs_count<true><<<h->num_sms * bps, kDfsWarps * 32, 0, h->stream>>>(da);
     LAUNCHED();
     // fixed grid (grid-stride over the runs counted on the device): the step's

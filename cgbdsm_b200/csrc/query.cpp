@@ -117,7 +117,7 @@ std::string build_query_meta(uint32_t qv, uint32_t qe, const uint32_t* edges, co
 // same-label vertices can collide); groups are limited to 3 members, extra
 // members go back to the core.
 void plan_edges(const QueryMeta& q, const float* avg_deg, EdgePlan* plans, bool analytic_tail, bool pick_last,
-                bool group_pendant) {
+                bool group_pendant, bool lane_tail, bool level_sum) {
     for (uint32_t ei = 0; ei < q.qe; ++ei) {
         EdgePlan& p = plans[ei];
         std::memset(&p, 0, sizeof(p));
@@ -299,15 +299,48 @@ void plan_edges(const QueryMeta& q, const float* avg_deg, EdgePlan* plans, bool 
             for (uint32_t c = 0; c + 1 < n_core; ++c)
                 if ((p.excl[t] >> c) & 1u) p.tail_dep = std::max<uint8_t>(p.tail_dep, (uint8_t)c);
         }
-        if (n_core >= 2 && n_core < q.qv && !p.tail_const) {
-            bool off_last = false;
-            for (uint32_t b2 = p.bn_off[n_core]; b2 < p.bn_off[q.qv]; ++b2) off_last |= p.bn_pos[b2] + 1u == n_core;
-            p.tail_lane = off_last ? 0 : 1;
+        if (lane_tail && n_core >= 2 && n_core < q.qv && !p.tail_const) {
+            // tail vertices hanging off the last core vertex: lane-countable
+            // when each has one list and a label group of its own
+            bool off_last = false, single = true;
+            for (uint32_t t = n_core; t < q.qv; ++t) {
+                bool t_off = false;
+                for (uint32_t b2 = p.bn_off[t]; b2 < p.bn_off[t + 1]; ++b2) t_off |= p.bn_pos[b2] + 1u == n_core;
+                if (!t_off) continue;
+                off_last = true;
+                const bool alone = (t == n_core || p.tail_gid[t - 1] != p.tail_gid[t]) &&
+                                   (t + 1 == q.qv || p.tail_gid[t + 1] != p.tail_gid[t]);
+                single &= alone && p.bn_off[t + 1] - p.bn_off[t] == 1;
+            }
+            p.tail_lane = !off_last ? 1 : (single ? 2 : 0);
         }
         if (pendant) {
             p.grouped = 1;
             for (uint32_t j = 2; j < n_core; ++j)
                 if (lab(p.vs[j]) == lab(b)) p.hit_mask |= (uint16_t)(1u << j);
+        }
+        if (level_sum && analytic_tail && n_core >= 3 && (n_core == q.qv || p.tail_lane || p.tail_const)) {
+            const uint32_t j = n_core - 1;
+            if (p.bn_off[j + 1] - p.bn_off[j] == 1 && !(p.grouped && ((p.hit_mask >> j) & 1u))) {
+                bool ok = true;
+                uint16_t tails = 0;
+                for (uint32_t t = n_core; t < q.qv; ++t) {
+                    bool off = false;
+                    for (uint32_t b2 = p.bn_off[t]; b2 < p.bn_off[t + 1]; ++b2) off |= p.bn_pos[b2] == j;
+                    if (off) {
+                        tails |= (uint16_t)(1u << t);
+                        ok &= (p.excl[t] & ((1u << j) - 1u)) == 0;
+                    } else {
+                        ok &= ((p.excl[t] >> j) & 1u) == 0;
+                    }
+                }
+                if (ok) {
+                    p.level_sum = 1;
+                    p.sum_tails = tails;
+                    for (uint32_t t = 0; t < j; ++t)
+                        if (!known || lab(p.vs[t]) == lab(p.vs[j])) p.sum_same |= (uint16_t)(1u << t);
+                }
+            }
         }
     }
 }

@@ -69,14 +69,30 @@ struct EdgePlan {
     // unknown); only those are excluded from t's counts.
     uint16_t excl[kMaxQV];
     uint16_t hit_mask;
-    // tail_lane: no tail list hangs off the last core vertex, so a candidate
-    // there changes the tail count only by lying in prefix-only lists (same
-    // label); each lane then evaluates its own candidate's tail count.
+    // level_sum: the last core position j has one backward list G (owned by
+    // position p < j), and every tail count is a prefix-only value times the
+    // lengths of the candidate's own lists towards the tail vertices in
+    // sum_tails (single-list groups of their own, no excluded prefix vertex
+    // in their label).  The last level then contributes
+    //   (sum over c in G of those lengths - the same over the matched prefix
+    //    vertices at positions sum_same that lie in G) x the prefix-only value,
+    // and the sum over G depends on the vertex m[p] only: it is computed once
+    // per (plan, vertex) and launch and shared through a table.
+    uint16_t sum_tails;
+    uint16_t sum_same;  // positions < j whose vertex can lie in G (same label)
+    // tail_lane: each lane evaluates its own candidate's tail count at the
+    // last core position.  1: no tail list hangs off the last core vertex,
+    // so a candidate changes the tail count only by lying in prefix-only
+    // lists (same label).  2: as 1, except for tail vertices whose only list
+    // hangs off the last core vertex and whose label group they form alone:
+    // such a count is the length of the candidate's list minus the excluded
+    // prefix vertices in it.  0: the warp counts one embedding at a time.
     uint8_t tail_lane;
     // tail_dep: the deepest core position below n_core - 1 that a tail count
     // reads (a list's owner or an excluded vertex); a prefix change at a
     // deeper position leaves every prefix-only tail count as it was.
     uint8_t tail_dep;
+    uint8_t level_sum;
     // kPlan* bits: per-plan schedule choices (the multi-query autotuner's)
     uint8_t flags;
 };
@@ -116,8 +132,9 @@ std::string parse_query_file(const std::string& path, std::vector<uint32_t>& lab
 // analytic_tail = false keeps every vertex in the enumerated core.
 // pick_last = true puts the core vertex with the fewest tail neighbours last.
 // group_pendant = true groups the seeds of edges with a pendant endpoint
-// (EdgePlan::grouped; needs labels).
+// (EdgePlan::grouped; needs labels).  lane_tail = false leaves tail_lane 0;
+// level_sum = false leaves level_sum 0.
 void plan_edges(const QueryMeta& q, const float* avg_deg, EdgePlan* plans, bool analytic_tail = true,
-                bool pick_last = true, bool group_pendant = true);
+                bool pick_last = true, bool group_pendant = true, bool lane_tail = true, bool level_sum = true);
 
 }  // namespace cgb

@@ -68,6 +68,8 @@ FLAG_MASK_PRUNE = 0x80
 FLAG_NO_SEED_GROUPS = 0x100
 FLAG_NO_RUN_BITS = 0x200
 FLAG_FOOTPRINT = 0x400
+FLAG_WARP_TAIL = 0x800
+FLAG_NO_LEVEL_SUM = 0x1000
 
 
 class MqConfig(ctypes.Structure):

@@ -11,7 +11,8 @@ import pytest
 
 from cgbdsm_b200 import CgbError, Engine
 from cgbdsm_b200.engine import (FLAG_ENUMERATE_TAIL, FLAG_FORCE_SPLIT, FLAG_MASK_PRUNE, FLAG_NO_RUN_BITS,
-                                FLAG_NO_SEED_GROUPS, FLAG_NO_TAIL_CACHE, FLAG_PLAIN_CORE_ORDER, FLAG_VALID_BITS)
+                                FLAG_NO_SEED_GROUPS, FLAG_NO_TAIL_CACHE, FLAG_PLAIN_CORE_ORDER, FLAG_VALID_BITS,
+                                FLAG_NO_LEVEL_SUM, FLAG_WARP_TAIL)
 from cgbdsm_b200.workloads import SPECS, materialize, read_query
 from oracle import bind
 
@@ -25,9 +26,11 @@ def _key(d, u, v):
 
 
 @pytest.mark.parametrize("flags", [0, FLAG_ENUMERATE_TAIL, FLAG_FORCE_SPLIT | FLAG_ENUMERATE_TAIL, FLAG_FORCE_SPLIT,
-                                   FLAG_NO_TAIL_CACHE, FLAG_NO_SEED_GROUPS, FLAG_NO_RUN_BITS, FLAG_PLAIN_CORE_ORDER],
+                                   FLAG_NO_TAIL_CACHE, FLAG_NO_SEED_GROUPS, FLAG_NO_RUN_BITS, FLAG_PLAIN_CORE_ORDER,
+                                   FLAG_WARP_TAIL, FLAG_NO_LEVEL_SUM | FLAG_FORCE_SPLIT],
                          ids=["counted_tail", "enumerated_tail", "stolen_enumerated", "stolen_counted",
-                              "counted_no_prefix_cache", "seed_per_dfs", "searched_runs", "greedy_core_order"])
+                              "counted_no_prefix_cache", "seed_per_dfs", "searched_runs", "greedy_core_order",
+                              "warp_tail", "no_level_sum_stolen"])
 @pytest.mark.parametrize("name", PIPELINE_CASES)
 def test_engine_matches_reference_cpu_path(name, flags, workdir):
     if not bind.have_ref():
@@ -471,3 +474,40 @@ def test_c2_patterns_match_reference_at_full_size(workdir, tmp_path):
         eng.close()
         prod.close()
         assert got == want, f"pattern {q['index']}: plain pipeline"
+
+
+@pytest.mark.gpu
+def test_two_live_engines_keep_their_own_plans(workdir):
+    """Two handles in one process (different patterns, both indexes built
+    before either matches, batches interleaved): each engine's counts equal
+    the reference's for its own pattern.  Plans and valid-bit plans are per
+    handle, so building the second engine leaves the first one's intact.
+    (The reference's CPU library keeps global state, so its two runs are
+    recorded one after the other first.)"""
+    if not bind.have_ref():
+        pytest.skip("oracle/_ref/libcgbref.so not built")
+    names = ["t_er_tree", "t_er_sparse"]
+    runs, engs = [], []
+    for name in names:
+        spec = SPECS[name]
+        p = materialize(spec, workdir)
+        ref = bind.RefPipeline(p["query"], p["data"], p["update"], spec.cli_batch_size)
+        run = {"init": ref.init_keys(), "dv": ref.dv_count, "batches": []}
+        while ref.step() >= 0:
+            run["batches"].append(ref.last())
+        ref.close()
+        runs.append(run)
+        qlabels, qedges = read_query(p["query"])
+        e = Engine(flags=FLAG_MASK_PRUNE)  # the valid-bit plans steer the pruning
+        e.load_query(len(qlabels), qedges, qlabels)
+        engs.append(e)
+    for run, e in zip(runs, engs):
+        e.build_index(run["init"], run["dv"])
+    for b in range(max(len(r["batches"]) for r in runs)):
+        for k, (run, e) in enumerate(zip(runs, engs)):
+            if b < len(run["batches"]):
+                r = run["batches"][b]
+                c = e.apply_batch(r["dv"], r["ins"], r["del"], r["delta"], r["edge_ok"])
+                assert c == r["count"], f"{names[k]} batch {b}: engine {c} != reference {r['count']}"
+    for e in engs:
+        e.close()
