@@ -715,6 +715,7 @@ struct DfsArgs {
     uint32_t* touched;           // footprint runs: bit per record resolved (nullptr: off)
     unsigned long long* lsum_tab;  // level-sum table [lsum_mask + 1][2], zeroed before the launch (nullptr: none)
     uint32_t lsum_mask;
+    const unsigned long long* wsum;  // dense level sums [array][dvcap] (nullptr: none)
 };
 
 // Footprint of a matching launch: the bytes of every distinct record it
@@ -938,13 +939,14 @@ constexpr uint32_t kClean = 0xffu;  // tail cache up to date
 // position whose vertex changed since the last call): an entry's count
 // depends on the positions of its lists' backward neighbours and of the
 // excluded core vertices, so e.g. a subset hanging off positions 0 and 1
-// is counted once per (m[0], m[1]), not once per prefix.
+// is counted once per (m[0], m[1]), not once per prefix.  Positions >= j
+// are not matched yet: subsets with a list there are left kDynamic.
 template <class RB>
 __device__ void tail_prepare(const EdgePlan& P, const uint32_t* m, uint4* bn, unsigned long long* cache,
-                             uint32_t dirty, const uint4* rec, uint32_t dvcap, const uint32_t* __restrict__ pool,
-                             const uint32_t* __restrict__ dval, bool self_loops, uint32_t lane,
-                             unsigned long long& bytes, const RB& rb) {
-    const uint32_t nc = P.n_core, n = P.n, j = nc - 1;
+                             uint32_t dirty, uint32_t j, const uint4* rec, uint32_t dvcap,
+                             const uint32_t* __restrict__ pool, const uint32_t* __restrict__ dval, bool self_loops,
+                             uint32_t lane, unsigned long long& bytes, const RB& rb) {
+    const uint32_t nc = P.n_core, n = P.n;
     for (uint32_t k = P.bn_off[nc] + lane; k < P.bn_off[n]; k += 32) {
         if (P.bn_pos[k] >= j || P.bn_pos[k] < dirty) continue;  // records of unchanged owners are current
         const size_t at = (size_t)P.bn_dir[k] * dvcap + m[P.bn_pos[k]];
@@ -968,7 +970,7 @@ __device__ void tail_prepare(const EdgePlan& P, const uint32_t* m, uint4* bn, un
                 if (mask & (1u << i))
                     for (uint32_t q = P.bn_off[t + i]; q < P.bn_off[t + i + 1]; ++q) {
                         ids[nl++] = (uint8_t)q;
-                        dynamic |= P.bn_pos[q] == j;
+                        dynamic |= P.bn_pos[q] >= j;
                         dep = max(dep, (uint32_t)P.bn_pos[q]);
                     }
             const uint32_t ex = P.excl[t] & ((1u << j) - 1u) & ~(self_loops ? 0u : owner_mask(P, ids, nl));
@@ -1110,7 +1112,7 @@ __device__ unsigned long long tail_const_value(const EdgePlan& P, const unsigned
     return prod;
 }
 
-// Level sums (plans with level_sum): the product of the lengths of c's own
+// Level sums (plans with sum_from): the product of the lengths of c's own
 // lists towards the tail vertices in sum_tails (1 when there are none).
 template <class RB>
 __device__ __forceinline__ unsigned long long sum_lens(const EdgePlan& P, const uint4* __restrict__ rec,
@@ -1371,7 +1373,7 @@ __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
     bool out_of_time = false;
     uint32_t ticket = kNoTicket;  // lane 0: ticket of the task ring this warp waits on
     uint32_t dirty = 0;  // shallowest position changed since the tail cache was filled (kClean: none)
-    unsigned long long lsum = 0;  // level sum over G of the current m[p] (plans with level_sum)
+    unsigned long long lsum = 0;  // one-position level sum over G of the current m[p]
     uint32_t ls_dirty = 0;        // shallowest position changed since lsum was computed (kClean: none)
     unsigned long long tail_const = 0;  // tail count of the current prefix (plans with tail_const)
     uint32_t idle_spins = 0;
@@ -1527,7 +1529,7 @@ __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
 
         dirty = 0;  // new unit: every cached tail count is stale
         ls_dirty = 0;
-        const bool level_sum = P.level_sum && !a.vb && !self_loops && (tail_cache || !has_tail);
+        const bool level_sum = P.sum_from && !a.vb && !self_loops && (tail_cache || !has_tail);
         setup(jbase);
         if (kind == 2 && lane == jbase) { st_gen = tgen; st_next = tlo; st_len = thi; }
         if (P.grouped) {
@@ -1564,7 +1566,33 @@ __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
             }
             const uint32_t gnext = __shfl_sync(kFull, st_next, j);
             uint32_t glen = __shfl_sync(kFull, st_len, j);
-            if (level_sum && j == nc - 1 && gnext == 0 && glen > 0) {
+            if (level_sum && P.sum_dense && a.wsum && j == P.sum_from && gnext == 0 && glen > 0 &&
+                glen == bn[P.bn_off[j]].y + bn[P.bn_off[j]].w) {
+                // positions [j, n_core) counted at once: the product of the
+                // precomputed sums of the positions owned by prefix positions
+                unsigned long long v = 1;
+                if (lane >= j && lane < nc) {
+                    const uint32_t p = P.bn_pos[P.bn_off[lane]];
+                    if (p < j) {
+                        v = __ldg(a.wsum + (size_t)(P.wslot + lane - j) * a.dvcap + m[p]);
+                        n_bytes += 8;
+                    }
+                }
+                for (int o = 16; o > 0; o >>= 1) v *= __shfl_xor_sync(kFull, v, o);
+                if (has_tail) {
+                    if (dirty <= P.tail_dep)
+                        tail_prepare(P, m, bn, s_tc[w], dirty, j, a.rec, a.dvcap, a.pool, a.dval, self_loops, lane,
+                                     n_bytes, rb);
+                    dirty = kClean;
+                    v *= tail_static_product(P, s_tc[w]);
+                }
+                if (P.grouped) v *= (unsigned long long)(X.n - __shfl_sync(kFull, st_hs, j));
+                if (lane == 0) { cnt += v; ++n_tail; }
+                if (lane == j) st_next = glen;
+                __syncwarp();
+                continue;
+            }
+            if (level_sum && !P.sum_dense && j == nc - 1 && gnext == 0 && glen > 0) {
                 // the whole last level at once (not a stolen part of it): the
                 // level sum over G, less the matched prefix vertices in G
                 const uint32_t o0 = P.bn_off[j];
@@ -1610,7 +1638,8 @@ __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
                     unsigned long long v = lsum - corr;
                     if (has_tail) {
                         if (dirty <= P.tail_dep)
-                            tail_prepare(P, m, bn, s_tc[w], dirty, a.rec, a.dvcap, a.pool, a.dval, self_loops, lane,
+                            tail_prepare(P, m, bn, s_tc[w], dirty, nc - 1, a.rec, a.dvcap, a.pool, a.dval,
+                                         self_loops, lane,
                                          n_bytes, rb);
                         dirty = kClean;
                         v *= tail_static_product(P, s_tc[w]);
@@ -1731,7 +1760,8 @@ __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
                         const uint32_t bal = __ballot_sync(kFull, ok);
                         if (bal) {
                             if (dirty <= P.tail_dep) {
-                                tail_prepare(P, m, bn, s_tc[w], dirty, a.rec, a.dvcap, a.pool, a.dval, self_loops, lane, n_bytes, rb);
+                                tail_prepare(P, m, bn, s_tc[w], dirty, nc - 1, a.rec, a.dvcap, a.pool, a.dval,
+                                             self_loops, lane, n_bytes, rb);
                                 tail_const = tail_const_value(P, s_tc[w]);
                             }
                             dirty = kClean;
@@ -1749,7 +1779,8 @@ __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
                         const uint32_t bal = __ballot_sync(kFull, ok);
                         if (bal) {
                             if (dirty <= P.tail_dep)
-                                tail_prepare(P, m, bn, s_tc[w], dirty, a.rec, a.dvcap, a.pool, a.dval, self_loops, lane, n_bytes, rb);
+                                tail_prepare(P, m, bn, s_tc[w], dirty, nc - 1, a.rec, a.dvcap, a.pool, a.dval,
+                                             self_loops, lane, n_bytes, rb);
                             dirty = kClean;
                             if (ok) {
                                 const unsigned long long tc =
@@ -1767,7 +1798,8 @@ __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
                             const uint32_t cl = __shfl_sync(kFull, c, l);
                             if (dirty <= P.tail_dep && tail_cache) {
                                 // first embedding since the prefix changed: recount the stale prefix-only subsets
-                                tail_prepare(P, m, bn, s_tc[w], dirty, a.rec, a.dvcap, a.pool, a.dval, self_loops, lane, n_bytes, rb);
+                                tail_prepare(P, m, bn, s_tc[w], dirty, nc - 1, a.rec, a.dvcap, a.pool, a.dval,
+                                             self_loops, lane, n_bytes, rb);
                             }
                             dirty = kClean;
                             if (lane == 0) m[j] = cl;
@@ -1819,6 +1851,70 @@ __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
         atomicAdd(a.stats + 3, tails);
         atomicAdd(a.stats + 4, bytes);
         atomicAdd(a.stats + 7, n_tasks);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// dense level sums: W_k(x) for every vertex x of one level-sum position k of
+// a plan (EdgePlan::sum_dense), computed children first before the DFS
+// ---------------------------------------------------------------------------
+struct WsumJob {
+    uint32_t dir, dvis;  // G_k(x): the list of direction dir at x (delta part if dvis)
+    uint32_t nt;         // pendant tails of k: lists of direction tdir at c (delta part if tvis)
+    uint32_t tdir[cgb::kMaxSumTails], tvis[cgb::kMaxSumTails];
+    uint32_t nch;        // positions owned by k: their sums at c
+    const unsigned long long* child[cgb::kMaxSumChildren];
+    unsigned long long* out;
+};
+constexpr uint32_t kWsumLane = 16;  // owners with lists up to this long are summed by one lane
+
+// W(x) = sum over c in G(x) of (product of c's pendant list lengths) x
+// (product of the children's W(c)), for every x < dv.  Lane per owner for
+// short lists (records read coalesced, 32 consecutive owners per warp),
+// the whole warp for each longer one.
+__global__ void k_wsum(const uint4* __restrict__ rec, uint32_t dvcap, const uint32_t* __restrict__ pool,
+                       const uint32_t* __restrict__ dval, uint32_t dv, WsumJob J) {
+    const uint32_t lane = threadIdx.x & 31;
+    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    auto term = [&](uint32_t c) -> unsigned long long {
+        unsigned long long v = 1;
+#pragma unroll
+        for (uint32_t i = 0; i < cgb::kMaxSumTails; ++i)
+            if (i < J.nt) {
+                const uint4 t = rec[(size_t)J.tdir[i] * dvcap + c];
+                v *= (unsigned long long)t.y + (J.tvis[i] ? t.w : 0u);
+            }
+#pragma unroll
+        for (uint32_t i = 0; i < cgb::kMaxSumChildren; ++i)
+            if (i < J.nch) v *= __ldg(J.child[i] + c);
+        return v;
+    };
+    for (uint64_t base = (((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5) << 5; base < dv;
+         base += nwarps * 32) {
+        const uint64_t x = base + lane;
+        uint4 r = make_uint4(0, 0, 0, 0);
+        if (x < dv) {
+            r = rec[(size_t)J.dir * dvcap + x];
+            if (!J.dvis) r.w = 0;
+        }
+        const uint32_t len = r.y + r.w;
+        unsigned long long acc = 0;
+        if (len <= kWsumLane)
+            for (uint32_t i = 0; i < len; ++i)
+                acc += term(i < r.y ? __ldg(pool + r.x + i) : __ldg(dval + r.z + (i - r.y)));
+        uint32_t big = __ballot_sync(kFull, len > kWsumLane);
+        while (big) {
+            const uint32_t i = __ffs(big) - 1;
+            big &= big - 1;
+            const uint32_t rx = __shfl_sync(kFull, r.x, i), ry = __shfl_sync(kFull, r.y, i);
+            const uint32_t rz = __shfl_sync(kFull, r.z, i), rw = __shfl_sync(kFull, r.w, i);
+            unsigned long long sv = 0;
+            for (uint32_t t = lane; t < ry + rw; t += 32)
+                sv += term(t < ry ? __ldg(pool + rx + t) : __ldg(dval + rz + (t - ry)));
+            for (int o = 16; o > 0; o >>= 1) sv += __shfl_xor_sync(kFull, sv, o);
+            if (lane == i) acc = sv;
+        }
+        if (x < dv) J.out[x] = acc;
     }
 }
 
@@ -2039,6 +2135,8 @@ struct cgb_handle {
     uint32_t* d_touched = nullptr; size_t touched_cap = 0;  // footprint runs: record bit set
     unsigned long long* d_lsum = nullptr;  // level-sum table, sized with the record table
     uint32_t lsum_slots = 0;
+    unsigned long long* d_wsum = nullptr; size_t wsum_cap = 0;  // dense level sums [n_wsum][dvcap]
+    uint32_t n_wsum = 0;
 
     // label-keyed mode (the multi-query engine's data-graph index): the
     // "direction" of a key is the label of its target vertex, the delta keys
@@ -2139,6 +2237,38 @@ cgb_status ensure_dvcap(cgb_handle* h, uint32_t dv) {
         CK(cudaMalloc(&h->d_lsum, (size_t)slots * 2 * sizeof(unsigned long long)));
         h->lsum_slots = slots;
     }
+    return CGB_OK;
+}
+
+// Dense level sums of every plan with sum_dense, children before parents
+// (a position's children sit at higher positions), on the stream.
+cgb_status dense_level_sums(cgb_handle* h) {
+    cgb_status s;
+    if ((s = grow(h, h->d_wsum, h->wsum_cap, (size_t)h->n_wsum * h->dvcap)) != CGB_OK) return s;
+    for (uint32_t e = 0; e < h->q.qe; ++e) {
+        const EdgePlan& P = h->plans[e];
+        if (!P.sum_dense) continue;
+        const uint32_t s0 = P.sum_from, nc = P.n_core;
+        auto arr = [&](uint32_t k) { return h->d_wsum + (size_t)(P.wslot + k - s0) * h->dvcap; };
+        for (uint32_t k = nc; k-- > s0;) {
+            WsumJob J;
+            std::memset(&J, 0, sizeof(J));
+            J.dir = P.bn_dir[P.bn_off[k]];
+            J.dvis = P.bn_dvis[P.bn_off[k]];
+            for (uint32_t t = nc; t < P.n; ++t)
+                if (((P.sum_tails >> t) & 1u) && P.bn_pos[P.bn_off[t]] == k) {
+                    J.tdir[J.nt] = P.bn_dir[P.bn_off[t]];
+                    J.tvis[J.nt] = P.bn_dvis[P.bn_off[t]];
+                    ++J.nt;
+                }
+            for (uint32_t l = k + 1; l < nc; ++l)
+                if (P.bn_pos[P.bn_off[l]] == k) J.child[J.nch++] = arr(l);
+            J.out = arr(k);
+            k_wsum<<<h->num_sms * 8, 256, 0, h->stream>>>(h->rec, h->dvcap, h->pool, h->d_dval, h->dv, J);
+            LAUNCHED();
+        }
+    }
+    CK(cudaGetLastError());
     return CGB_OK;
 }
 
@@ -2482,7 +2612,7 @@ void cgb_destroy(cgb_handle* h) {
                     h->d_seed, h->d_counts, h->d_stats, h->d_tasks, h->d_qctr, h->d_temp, h->d_qe_dirs, h->d_edge_ok,
                     h->d_vb, h->d_rb_slot, h->d_rb_sel, h->d_rb_bits, h->d_rb_ctr, h->d_rb_new, h->d_small_runs,
                     h->d_big_runs, h->d_tiny_runs, h->d_list_ctr, h->d_rev, h->d_touched, h->d_plans,
-                    h->d_vbplans, h->d_dir_edge, h->d_lsum};
+                    h->d_vbplans, h->d_dir_edge, h->d_lsum, h->d_wsum};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (h->h_scal) cudaFreeHost(h->h_scal);
@@ -2553,7 +2683,13 @@ cgb_status cgb_build_index(cgb_handle* h, const uint64_t* keys, uint64_t n, uint
     for (uint32_t d = 0; d < h->nd; ++d) avg[d] = nodes[d] ? (float)card[d] / (float)nodes[d] : 0.f;
     cgb::plan_edges(h->q, avg, h->plans, !(h->cfg.flags & CGB_FLAG_ENUMERATE_TAIL),
                     !(h->cfg.flags & CGB_FLAG_PLAIN_CORE_ORDER), !(h->cfg.flags & CGB_FLAG_NO_SEED_GROUPS),
-                    !(h->cfg.flags & CGB_FLAG_WARP_TAIL), !(h->cfg.flags & CGB_FLAG_NO_LEVEL_SUM));
+                    !(h->cfg.flags & CGB_FLAG_WARP_TAIL), !(h->cfg.flags & CGB_FLAG_NO_LEVEL_SUM), true);
+    h->n_wsum = 0;
+    for (uint32_t e = 0; e < h->q.qe; ++e)
+        if (h->plans[e].sum_dense) {
+            h->plans[e].wslot = (uint8_t)h->n_wsum;
+            h->n_wsum += h->plans[e].n_core - h->plans[e].sum_from;
+        }
     CK(cudaMemcpy(h->d_plans, h->plans, sizeof(EdgePlan) * kMaxQE, cudaMemcpyHostToDevice));
     {
         // valid-bit plans from the reference's starting edge
@@ -2733,7 +2869,12 @@ cgb_status cgb_apply_batch_device(cgb_handle* h, uint32_t dv_count, const uint64
         int bps = h->dfs_occupancy;
         if (h->cfg.dfs_blocks_per_sm) bps = std::min(bps, (int)h->cfg.dfs_blocks_per_sm);
         bool any_sum = false;
-        for (uint32_t e = 0; e < h->q.qe; ++e) any_sum |= h->plans[e].level_sum != 0;
+        for (uint32_t e = 0; e < h->q.qe; ++e) any_sum |= h->plans[e].sum_from != 0 && !h->plans[e].sum_dense;
+        da.wsum = nullptr;
+        if (h->n_wsum && !da.vb && da.tail_cache) {
+            if ((s = dense_level_sums(h)) != CGB_OK) return s;
+            da.wsum = h->d_wsum;
+        }
         lsum_bind(h, any_sum, da);
         if ((s = lsum_clear(h, da)) != CGB_OK) return s;
         if (footprint) k_dfs_count<false, true><<<h->num_sms * bps, kDfsWarps * 32, 0, h->stream>>>(da);
@@ -2835,6 +2976,18 @@ cgb_status cgb_plan_anchor(const cgb_handle* h, uint32_t ei, uint32_t* qvertex) 
     if (!h->have_index) return CGB_ERR_STATE;
     if (ei >= h->q.qe) return CGB_ERR_ARG;
     *qvertex = h->plans[ei].vs[0];
+    return CGB_OK;
+}
+
+cgb_status cgb_plan_info(const cgb_handle* h, uint32_t ei, uint32_t* out4) {
+    if (!h || !out4) return CGB_ERR_ARG;
+    if (!h->have_index) return CGB_ERR_STATE;
+    if (ei >= h->q.qe) return CGB_ERR_ARG;
+    const EdgePlan& P = h->plans[ei];
+    out4[0] = P.n_core;
+    out4[1] = P.sum_from;
+    out4[2] = P.sum_dense;
+    out4[3] = P.tail_lane;
     return CGB_OK;
 }
 

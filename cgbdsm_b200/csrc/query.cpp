@@ -117,7 +117,7 @@ std::string build_query_meta(uint32_t qv, uint32_t qe, const uint32_t* edges, co
 // same-label vertices can collide); groups are limited to 3 members, extra
 // members go back to the core.
 void plan_edges(const QueryMeta& q, const float* avg_deg, EdgePlan* plans, bool analytic_tail, bool pick_last,
-                bool group_pendant, bool lane_tail, bool level_sum) {
+                bool group_pendant, bool lane_tail, bool level_sum, bool dense_sums) {
     for (uint32_t ei = 0; ei < q.qe; ++ei) {
         EdgePlan& p = plans[ei];
         std::memset(&p, 0, sizeof(p));
@@ -320,6 +320,7 @@ void plan_edges(const QueryMeta& q, const float* avg_deg, EdgePlan* plans, bool 
                 if (lab(p.vs[j]) == lab(b)) p.hit_mask |= (uint16_t)(1u << j);
         }
         if (level_sum && analytic_tail && n_core >= 3 && (n_core == q.qv || p.tail_lane || p.tail_const)) {
+            // one position: the last core position j
             const uint32_t j = n_core - 1;
             if (p.bn_off[j + 1] - p.bn_off[j] == 1 && !(p.grouped && ((p.hit_mask >> j) & 1u))) {
                 bool ok = true;
@@ -335,11 +336,51 @@ void plan_edges(const QueryMeta& q, const float* avg_deg, EdgePlan* plans, bool 
                     }
                 }
                 if (ok) {
-                    p.level_sum = 1;
+                    p.sum_from = (uint8_t)j;
                     p.sum_tails = tails;
                     for (uint32_t t = 0; t < j; ++t)
                         if (!known || lab(p.vs[t]) == lab(p.vs[j])) p.sum_same |= (uint16_t)(1u << t);
                 }
+            }
+        }
+        if (level_sum && dense_sums && analytic_tail && known && n_core >= 4) {
+            // several positions [s, n_core) with labels of their own: the
+            // smallest s >= 2 whose positions each have one backward list and
+            // whose pendant tails are single-list groups with labels of their own
+            std::vector<uint32_t> lcount(64, 0);
+            for (uint32_t u = 0; u < q.qv; ++u)
+                if (q.labels[u] < lcount.size()) ++lcount[q.labels[u]];
+            auto unique = [&](uint32_t u) { return q.labels[u] < lcount.size() && lcount[q.labels[u]] == 1; };
+            auto pos_ok = [&](uint32_t k, uint16_t& tails) {
+                if (p.bn_off[k + 1] - p.bn_off[k] != 1 || !unique(p.vs[k])) return false;
+                uint32_t nt = 0, nch = 0;
+                for (uint32_t t = n_core; t < q.qv; ++t) {
+                    bool off = false;
+                    for (uint32_t b2 = p.bn_off[t]; b2 < p.bn_off[t + 1]; ++b2) off |= p.bn_pos[b2] == k;
+                    if (!off) continue;
+                    const bool alone = (t == n_core || p.tail_gid[t - 1] != p.tail_gid[t]) &&
+                                       (t + 1 == q.qv || p.tail_gid[t + 1] != p.tail_gid[t]);
+                    if (p.bn_off[t + 1] - p.bn_off[t] != 1 || !alone || !unique(p.vs[t])) return false;
+                    tails |= (uint16_t)(1u << t);
+                    ++nt;
+                }
+                for (uint32_t l = k + 1; l < n_core; ++l) nch += p.bn_pos[p.bn_off[l]] == k ? 1u : 0u;
+                return nt <= kMaxSumTails && nch <= kMaxSumChildren;
+            };
+            uint32_t best = n_core;
+            uint16_t best_tails = 0;
+            for (uint32_t s0 = n_core - 1; s0 >= 2; --s0) {
+                uint16_t tails = 0;
+                bool ok = true;
+                for (uint32_t k = s0; k < n_core && ok; ++k) ok = pos_ok(k, tails);
+                if (ok) { best = s0; best_tails = tails; }
+                else break;  // a position that fails stays inside every larger range
+            }
+            if (best + 1 < n_core) {
+                p.sum_from = (uint8_t)best;
+                p.sum_dense = 1;
+                p.sum_tails = best_tails;
+                p.sum_same = 0;  // labels of their own: no prefix vertex can lie in a G_k
             }
         }
     }

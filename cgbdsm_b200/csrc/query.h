@@ -69,15 +69,24 @@ struct EdgePlan {
     // unknown); only those are excluded from t's counts.
     uint16_t excl[kMaxQV];
     uint16_t hit_mask;
-    // level_sum: the last core position j has one backward list G (owned by
-    // position p < j), and every tail count is a prefix-only value times the
-    // lengths of the candidate's own lists towards the tail vertices in
-    // sum_tails (single-list groups of their own, no excluded prefix vertex
-    // in their label).  The last level then contributes
-    //   (sum over c in G of those lengths - the same over the matched prefix
-    //    vertices at positions sum_same that lie in G) x the prefix-only value,
-    // and the sum over G depends on the vertex m[p] only: it is computed once
-    // per (plan, vertex) and launch and shared through a table.
+    // Level sums: core positions [sum_from, n_core) are counted, not
+    // enumerated.  Each such position k has one backward list G_k owned by a
+    // position p_k < k, and the tail vertices with a list at k are pendants
+    // of k (one list, a label group of their own), collected in sum_tails.
+    // With W_k(x) = sum over c in G_k(x) of the lengths of c's lists towards
+    // its pendants times W_l(c) for every position l owned by k, a prefix
+    // m[0..sum_from) contributes the product of W_r(m[p_r]) over the
+    // positions r with p_r < sum_from, times the prefix-only tail count.
+    //   sum_from = n_core - 1 (sum_dense 0): one position j; no prefix
+    //     position shares a label with its pendants, no prefix-only tail
+    //     group shares the label of vs[j], and the matched prefix vertices at
+    //     positions sum_same (same label as vs[j]) that lie in G are
+    //     subtracted per prefix; W is computed on demand per (plan, vertex)
+    //     and launch, shared through a table.
+    //   sum_from < n_core - 1 (sum_dense 1): every position in the range and
+    //     every pendant of one has a label no other query vertex has, so no
+    //     two of them can coincide; W_k is precomputed for every vertex
+    //     before the launch (children first) into array wslot + k - sum_from.
     uint16_t sum_tails;
     uint16_t sum_same;  // positions < j whose vertex can lie in G (same label)
     // tail_lane: each lane evaluates its own candidate's tail count at the
@@ -92,11 +101,16 @@ struct EdgePlan {
     // reads (a list's owner or an excluded vertex); a prefix change at a
     // deeper position leaves every prefix-only tail count as it was.
     uint8_t tail_dep;
-    uint8_t level_sum;
+    uint8_t sum_from;   // 0: no level sums
+    uint8_t sum_dense;
+    uint8_t wslot;
     // kPlan* bits: per-plan schedule choices (the multi-query autotuner's)
     uint8_t flags;
+    uint8_t pad_;
 };
 constexpr uint8_t kPlanNoTailCache = 0x1;  // recount every tail subset per core embedding
+constexpr uint32_t kMaxSumTails = 4;     // pendant tails per dense level-sum position
+constexpr uint32_t kMaxSumChildren = 4;  // level-sum positions owned by one dense level-sum position
 
 // Valid-bit plan of one query edge ei (the reference's 1-bit support masks,
 // BuildLocalIndexBitAll, graph_gpu.cu:803-869): its indexing order (BFS from
@@ -133,8 +147,10 @@ std::string parse_query_file(const std::string& path, std::vector<uint32_t>& lab
 // pick_last = true puts the core vertex with the fewest tail neighbours last.
 // group_pendant = true groups the seeds of edges with a pendant endpoint
 // (EdgePlan::grouped; needs labels).  lane_tail = false leaves tail_lane 0;
-// level_sum = false leaves level_sum 0.
+// level_sum = false leaves sum_from 0; dense_sums = false allows only the
+// one-position (table) level sums.  wslot is left 0 (the engine assigns it).
 void plan_edges(const QueryMeta& q, const float* avg_deg, EdgePlan* plans, bool analytic_tail = true,
-                bool pick_last = true, bool group_pendant = true, bool lane_tail = true, bool level_sum = true);
+                bool pick_last = true, bool group_pendant = true, bool lane_tail = true, bool level_sum = true,
+                bool dense_sums = false);
 
 }  // namespace cgb

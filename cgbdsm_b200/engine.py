@@ -25,7 +25,7 @@ EXPORTS = [
     "cgb_default_config", "cgb_create", "cgb_destroy", "cgb_last_error", "cgb_load_query",
     "cgb_load_query_file", "cgb_query_dir", "cgb_build_index", "cgb_apply_batch",
     "cgb_apply_batch_device", "cgb_last_edge_counts", "cgb_read_index", "cgb_last_timings",
-    "cgb_kernel_launches", "cgb_last_stats", "cgb_stream", "cgb_plan_anchor", "cgb_check_symmetry",
+    "cgb_kernel_launches", "cgb_last_stats", "cgb_stream", "cgb_plan_anchor", "cgb_plan_info", "cgb_check_symmetry",
     "cgb_producer_open", "cgb_producer_close", "cgb_producer_last_error",
     "cgb_producer_num_batches", "cgb_producer_initial", "cgb_producer_next", "cgb_producer_vertex_map",
     "cgb_merge_keys_noalloc", "cgb_valid_bits", "cgb_starting_edge",
@@ -136,6 +136,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.cgb_stream.argtypes = [_vp]
     lib.cgb_stream.restype = _vp
     lib.cgb_plan_anchor.argtypes = [_vp, _u32, ctypes.POINTER(_u32)]
+    lib.cgb_plan_info.argtypes = [_vp, _u32, _vp]
     lib.cgb_check_symmetry.argtypes = [_vp, ctypes.POINTER(_u64)]
     lib.cgb_producer_open.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, _u32, _u32,
                                       ctypes.POINTER(_vp)]
@@ -323,6 +324,13 @@ class Engine:
         v = _u32(0)
         self._check(self.lib.cgb_plan_anchor(self.h, ei, ctypes.byref(v)))
         return v.value
+
+    def plan_info(self, ei: int) -> dict:
+        """How query edge ei's plan counts: core positions, first level-sum
+        position (0 = none), dense sums, per-lane tail mode."""
+        out = np.zeros(4, dtype=np.uint32)
+        self._check(self.lib.cgb_plan_info(self.h, ei, out.ctypes.data))
+        return {"n_core": int(out[0]), "sum_from": int(out[1]), "dense": bool(out[2]), "tail_lane": int(out[3])}
 
     def check_symmetry(self) -> int:
         """Index entries whose mirror entry is missing (0 for a symmetric index)."""

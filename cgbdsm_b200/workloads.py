@@ -75,6 +75,12 @@ SPECS = {
     "t_er_tree": WorkloadSpec("t_er_tree", 0, 3_000, 30_000, 3, 0.0, 3_000, 600, 2, 5, 131, 132, 133, 13),
     "t_rmat": WorkloadSpec("t_rmat", 1, 8_192, 60_000, 8, 1.0, 6_000, 1_000, 0, 5, 141, 142, 143, 17),
     "t_tiny": WorkloadSpec("t_tiny", 0, 300, 2_400, 2, 0.0, 400, 50, 0, 4, 151, 152, 153, 3),
+    # trees whose labels reach the level sums: every query label distinct
+    # (dense sums over several positions), or shared with prefix positions
+    # (one position, prefix vertices subtracted); R-MAT tree of C3's shape
+    "t_er_tree_u": WorkloadSpec("t_er_tree_u", 0, 3_000, 30_000, 12, 0.0, 3_000, 600, 2, 6, 161, 162, 163, 161),
+    "t_er_tree_s": WorkloadSpec("t_er_tree_s", 0, 3_000, 30_000, 12, 0.0, 3_000, 600, 2, 6, 161, 162, 163, 160),
+    "t_rmat_tree": WorkloadSpec("t_rmat_tree", 1, 8_192, 60_000, 16, 1.0, 6_000, 1_200, 2, 7, 171, 172, 173, 174),
 }
 
 

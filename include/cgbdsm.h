@@ -180,6 +180,13 @@ void* cgb_stream(const cgb_handle* h);
  * after cgb_build_index. */
 cgb_status cgb_plan_anchor(const cgb_handle* h, uint32_t ei, uint32_t* qvertex);
 
+/* How query edge ei's plan counts (after cgb_build_index), for tests and
+ * tuning: out4[0] = core positions (the others are counted as the tail),
+ * out4[1] = first position counted by level sums (0 = none), out4[2] = 1
+ * when those sums are precomputed for every vertex (several positions),
+ * out4[3] = per-lane tail mode at the last core position (0, 1 or 2). */
+cgb_status cgb_plan_info(const cgb_handle* h, uint32_t ei, uint32_t* out4);
+
 /* Index symmetry check (after any pending delta merge-back): *n_asym = number
  * of index entries y in the list of (a -> b) at x whose mirror entry (x in
  * the list of (b -> a) at y) is missing.  The matcher's per-edge seeding gives

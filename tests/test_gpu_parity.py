@@ -18,7 +18,8 @@ from oracle import bind
 
 pytestmark = pytest.mark.gpu
 
-PIPELINE_CASES = ["t_tiny", "t_er5", "t_er6", "t_er_sparse", "t_er_tree", "t_rmat", "c1", "c1_q25"]
+PIPELINE_CASES = ["t_tiny", "t_er5", "t_er6", "t_er_sparse", "t_er_tree", "t_rmat", "c1", "c1_q25", "t_er_tree_u",
+                  "t_er_tree_s", "t_rmat_tree"]
 
 
 def _key(d, u, v):
@@ -511,3 +512,32 @@ def test_two_live_engines_keep_their_own_plans(workdir):
                 assert c == r["count"], f"{names[k]} batch {b}: engine {c} != reference {r['count']}"
     for e in engs:
         e.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name,dense", [("t_er_tree_u", True), ("t_er_tree_s", False), ("t_rmat_tree", None)])
+def test_level_sum_workloads_reach_their_plans(name, dense, workdir):
+    """The level-sum parity workloads plan the counting they are there to
+    test (their counts are checked against the reference with and without
+    level sums by test_engine_matches_reference_cpu_path): every query label
+    distinct gives sums over several positions, precomputed per vertex; a
+    label shared with prefix positions gives the one-position sums with
+    prefix vertices subtracted."""
+    if not bind.have_ref():
+        pytest.skip("oracle/_ref/libcgbref.so not built")
+    spec = SPECS[name]
+    p = materialize(spec, workdir)
+    qlabels, qedges = read_query(p["query"])
+    ref = bind.RefPipeline(p["query"], p["data"], p["update"], spec.cli_batch_size)
+    eng = Engine()
+    eng.load_query(len(qlabels), qedges, qlabels)
+    eng.build_index(ref.init_keys(), ref.dv_count)
+    ref.close()
+    info = [eng.plan_info(ei) for ei in range(len(qedges))]
+    eng.close()
+    summed = [x for x in info if x["sum_from"]]
+    assert summed, info
+    if dense is True:
+        assert any(x["dense"] and x["sum_from"] + 1 < x["n_core"] for x in summed), info
+    elif dense is False:
+        assert any(not x["dense"] and x["sum_from"] + 1 == x["n_core"] for x in summed), info

@@ -63,7 +63,8 @@ def mq_counts(g, queries, flags=0):
     return out
 
 
-@pytest.mark.parametrize("name", ["t_tiny", "t_er5", "t_er_sparse", "t_er_tree", "t_rmat", "c1_q25"])
+@pytest.mark.parametrize("name", ["t_tiny", "t_er5", "t_er_sparse", "t_er_tree", "t_rmat", "c1_q25", "t_er_tree_s",
+                                  "t_rmat_tree"])
 def test_mq_matches_reference_cpu_path(name, workdir):
     if not bind.have_ref():
         pytest.skip("oracle/_ref/libcgbref.so not built")
