@@ -1046,7 +1046,7 @@ __device__ unsigned long long tail_eval(const EdgePlan& P, const uint32_t* m, ui
 // c's own list: its length minus the excluded prefix vertices it holds (c
 // is not in its own list: no self-loops on this path).  Lanes diverge only
 // in the loads and searches.
-template <class RB>
+template <bool kLane2, class RB>
 __device__ unsigned long long tail_eval_lane(const EdgePlan& P, const uint4* bn, const unsigned long long* cache,
                                              const uint4* __restrict__ rec, uint32_t dvcap, const uint32_t* m,
                                              const uint32_t* __restrict__ pool, const uint32_t* __restrict__ dval,
@@ -1062,7 +1062,7 @@ __device__ unsigned long long tail_eval_lane(const EdgePlan& P, const uint4* bn,
         unsigned long long sc[8];
         for (uint32_t mask = 1; mask < (1u << k); ++mask) {
             unsigned long long cv = cache[t * 8 + mask];
-            if (cv == kDynamic) {
+            if (kLane2 && cv == kDynamic) {
                 const uint32_t q = P.bn_off[t];
                 const size_t at = (size_t)P.bn_dir[q] * dvcap + c;
                 uint4 r = rec[at];
@@ -1316,8 +1316,11 @@ constexpr uint32_t kCandMask = (1u << kCandBits) - 1u;
 // kMulti = true: the plans of every registered query in global memory
 // (a.plans, one per (query, edge); a.qe of them), seed table searched in
 // global memory, each warp's current plan copied to shared memory when its
-// unit changes plan.
-template <bool kMulti, bool kFoot = false>
+// unit changes plan.  kSums = false compiles the level sums and the
+// per-lane pendant tails (tail_lane 2) out: the kernel is bound by
+// instruction fetch, and their code doubled its fetch stalls on patterns
+// whose plans never use them.
+template <bool kMulti, bool kFoot = false, bool kSums = true>
 __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
     __shared__ uint32_t s_cand[kDfsWarps][kMaxQV][32];
     __shared__ uint4 s_bn[kDfsWarps][kMaxBN];
@@ -1529,7 +1532,7 @@ __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
 
         dirty = 0;  // new unit: every cached tail count is stale
         ls_dirty = 0;
-        const bool level_sum = P.sum_from && !a.vb && !self_loops && (tail_cache || !has_tail);
+        const bool level_sum = kSums && P.sum_from && !a.vb && !self_loops && (tail_cache || !has_tail);
         setup(jbase);
         if (kind == 2 && lane == jbase) { st_gen = tgen; st_next = tlo; st_len = thi; }
         if (P.grouped) {
@@ -1772,8 +1775,8 @@ __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
                             }
                             if (lane == 0) { cnt += wsum * tail_const; n_tail += __popc(bal); }
                         }
-                    } else if (has_tail && P.tail_lane && (P.tail_lane == 1 || !self_loops) && tail_cache &&
-                               !hit_last) {
+                    } else if (has_tail && P.tail_lane && (P.tail_lane == 1 || (kSums && !self_loops)) &&
+                               tail_cache && !hit_last) {
                         // the tail depends on the candidate only through prefix-only
                         // lists: every lane counts its own candidate's tail
                         const uint32_t bal = __ballot_sync(kFull, ok);
@@ -1784,7 +1787,8 @@ __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
                             dirty = kClean;
                             if (ok) {
                                 const unsigned long long tc =
-                                    tail_eval_lane(P, bn, s_tc[w], a.rec, a.dvcap, m, a.pool, a.dval, c, n_bytes, rb);
+                                    tail_eval_lane<kSums>(P, bn, s_tc[w], a.rec, a.dvcap, m, a.pool, a.dval, c, n_bytes,
+                                                          rb);
                                 cnt += P.grouped ? tc * (unsigned long long)(X.n - hs) : tc;
                             }
                             if (lane == 0) n_tail += __popc(bal);
@@ -2877,8 +2881,13 @@ cgb_status cgb_apply_batch_device(cgb_handle* h, uint32_t dv_count, const uint64
         }
         lsum_bind(h, any_sum, da);
         if ((s = lsum_clear(h, da)) != CGB_OK) return s;
-        if (footprint) k_dfs_count<false, true><<<h->num_sms * bps, kDfsWarps * 32, 0, h->stream>>>(da);
-        else k_dfs_count<false><<<h->num_sms * bps, kDfsWarps * 32, 0, h->stream>>>(da);
+        bool uses_sums = false;
+        for (uint32_t e = 0; e < h->q.qe; ++e) uses_sums |= h->plans[e].sum_from != 0 || h->plans[e].tail_lane == 2;
+        const dim3 grid(h->num_sms * bps), block(kDfsWarps * 32);
+        if (footprint && uses_sums) k_dfs_count<false, true, true><<<grid, block, 0, h->stream>>>(da);
+        else if (footprint) k_dfs_count<false, true, false><<<grid, block, 0, h->stream>>>(da);
+        else if (uses_sums) k_dfs_count<false, false, true><<<grid, block, 0, h->stream>>>(da);
+        else k_dfs_count<false, false, false><<<grid, block, 0, h->stream>>>(da);
         LAUNCHED();
         CK(cudaGetLastError());
         CK(cudaEventRecord(h->ev[3], h->stream));
