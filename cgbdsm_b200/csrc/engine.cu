@@ -1377,6 +1377,10 @@ __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
     uint32_t ticket = kNoTicket;  // lane 0: ticket of the task ring this warp waits on
     uint32_t dirty = 0;  // shallowest position changed since the tail cache was filled (kClean: none)
     unsigned long long lsum = 0;  // one-position level sum over G of the current m[p]
+    bool mb = false;              // counting a subtree memo (EdgePlan::memo_from) to publish
+    bool mb_split = false;        // part of that subtree went to other warps: count it, publish nothing
+    uint32_t mb_slot = kLsumNone;
+    unsigned long long mb_base = 0;  // lane-local count when the memo's subtree was entered
     uint32_t ls_dirty = 0;        // shallowest position changed since lsum was computed (kClean: none)
     unsigned long long tail_const = 0;  // tail count of the current prefix (plans with tail_const)
     uint32_t idle_spins = 0;
@@ -1488,6 +1492,9 @@ __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
         const uint32_t nc = P.n_core;
         const bool has_tail = nc < P.n;
         SeedGroup X{nullptr, 0u, kNoVertex};
+        // weight of a grouped embedding with hs hits (1 inside a memo's subtree,
+        // whose count is weighted once when it is complete)
+        auto gw = [&](uint32_t hs) -> unsigned long long { return mb ? 1ull : (unsigned long long)(X.n - hs); };
         if (P.grouped) {
             const size_t xat = (size_t)P.seed_dir * a.dvcap + m[0];
             const uint4 xr = a.rec[xat];
@@ -1533,6 +1540,8 @@ __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
         dirty = 0;  // new unit: every cached tail count is stale
         ls_dirty = 0;
         const bool level_sum = kSums && P.sum_from && !a.vb && !self_loops && (tail_cache || !has_tail);
+        const bool memo_on = kSums && P.memo_from && a.lsum_tab && !a.vb && !self_loops;
+        mb = false;
         setup(jbase);
         if (kind == 2 && lane == jbase) { st_gen = tgen; st_next = tlo; st_len = thi; }
         if (P.grouped) {
@@ -1569,6 +1578,34 @@ __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
             }
             const uint32_t gnext = __shfl_sync(kFull, st_next, j);
             uint32_t glen = __shfl_sync(kFull, st_len, j);
+            if (memo_on && !mb && j == P.memo_from && gnext == 0 && glen > 0) {
+                // the whole level below m[memo_pos]: its count from the table,
+                // or counted here (unweighted) and published at the level's end
+                const uint4 gr = bn[P.bn_off[j] + __shfl_sync(kFull, st_gen, j)];
+                if (glen == gr.y + gr.w) {
+                    const unsigned long long K =
+                        ((1ull << 42) | ((unsigned long long)ei << 27) | m[P.memo_pos]) + 1ull;
+                    uint32_t claim = kLsumNone;
+                    bool hit = false;
+                    unsigned long long hv = 0;
+                    if (lane == 0) claim = lsum_find(a.lsum_tab, a.lsum_mask, K, hit, hv);
+                    if (__shfl_sync(kFull, hit ? 1u : 0u, 0)) {
+                        unsigned long long v = __shfl_sync(kFull, hv, 0);
+                        if (P.grouped) v *= gw(__shfl_sync(kFull, st_hs, j));
+                        if (lane == 0) { cnt += v; ++n_tail; }
+                        if (lane == j) st_next = glen;
+                        __syncwarp();
+                        continue;
+                    }
+                    claim = __shfl_sync(kFull, claim, 0);
+                    if (claim != kLsumNone) {
+                        mb = true;
+                        mb_split = false;
+                        mb_slot = claim;
+                        mb_base = cnt;
+                    }
+                }
+            }
             if (level_sum && P.sum_dense && a.wsum && j == P.sum_from && gnext == 0 && glen > 0 &&
                 glen == bn[P.bn_off[j]].y + bn[P.bn_off[j]].w) {
                 // positions [j, n_core) counted at once: the product of the
@@ -1589,7 +1626,7 @@ __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
                     dirty = kClean;
                     v *= tail_static_product(P, s_tc[w]);
                 }
-                if (P.grouped) v *= (unsigned long long)(X.n - __shfl_sync(kFull, st_hs, j));
+                if (P.grouped) v *= gw(__shfl_sync(kFull, st_hs, j));
                 if (lane == 0) { cnt += v; ++n_tail; }
                 if (lane == j) st_next = glen;
                 __syncwarp();
@@ -1647,7 +1684,7 @@ __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
                         dirty = kClean;
                         v *= tail_static_product(P, s_tc[w]);
                     }
-                    if (P.grouped) v *= (unsigned long long)(X.n - __shfl_sync(kFull, st_hs, j));
+                    if (P.grouped) v *= gw(__shfl_sync(kFull, st_hs, j));
                     if (lane == 0) { cnt += v; n_tail += glen - nhit; }
                     if (lane == j) st_next = glen;
                     __syncwarp();
@@ -1684,6 +1721,7 @@ __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
                         slot = __shfl_sync(kFull, slot, 0);
                         if (slot != 0xffffffffu) {
                             const uint32_t d = __ffs(hb) - 1;
+                            if (mb && d >= P.memo_from) mb_split = true;  // the memo's count is no longer all here
                             uint32_t lo = 0, hi = 0;
                             if (lane == d) {
                                 if (d == j) {
@@ -1770,7 +1808,7 @@ __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
                             dirty = kClean;
                             unsigned long long wsum = __popc(bal);
                             if (P.grouped) {
-                                wsum *= (unsigned long long)(X.n - hs);
+                                wsum *= gw(hs);
                                 if (hit_last) wsum -= X.mult_sum(c, ok, lane);
                             }
                             if (lane == 0) { cnt += wsum * tail_const; n_tail += __popc(bal); }
@@ -1789,7 +1827,7 @@ __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
                                 const unsigned long long tc =
                                     tail_eval_lane<kSums>(P, bn, s_tc[w], a.rec, a.dvcap, m, a.pool, a.dval, c, n_bytes,
                                                           rb);
-                                cnt += P.grouped ? tc * (unsigned long long)(X.n - hs) : tc;
+                                cnt += P.grouped ? tc * gw(hs) : tc;
                             }
                             if (lane == 0) n_tail += __popc(bal);
                         }
@@ -1815,13 +1853,13 @@ __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
                                     : tail_count_warp(P, m, bn, a.rec, a.dvcap, a.pool, a.dval, self_loops, lane,
                                                       n_bytes, rb);
                             unsigned long long wt = 1;
-                            if (P.grouped) wt = X.n - hs - (hit_last ? X.mult(cl, lane) : 0u);
+                            if (P.grouped) wt = gw(hs) - (hit_last ? X.mult(cl, lane) : 0u);
                             if (lane == 0) { cnt += tc * wt; ++n_tail; }
                             __syncwarp();
                         }
                     } else if (P.grouped) {
                         const uint32_t nok = __popc(__ballot_sync(kFull, ok));
-                        unsigned long long wsum = (unsigned long long)nok * (X.n - hs);
+                        unsigned long long wsum = (unsigned long long)nok * gw(hs);
                         if (hit_last) wsum -= X.mult_sum(c, ok, lane);
                         if (lane == 0) cnt += wsum;
                     } else {
@@ -1835,6 +1873,20 @@ __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
                 if (lane == j) st_next = gnext + 32;
                 __syncwarp();
                 continue;
+            }
+            if (mb && j == P.memo_from) {
+                // the memo's subtree is complete: publish its count, weight it once
+                const unsigned long long S = warp_sum(cnt - mb_base);
+                if (lane == 0 && !mb_split) {
+                    const unsigned long long K =
+                        ((1ull << 42) | ((unsigned long long)ei << 27) | m[P.memo_pos]) + 1ull;
+                    a.lsum_tab[2 * (size_t)mb_slot + 1] = S;
+                    st_release_u64(a.lsum_tab + 2 * (size_t)mb_slot, (K << 1) | 1ull);
+                }
+                const unsigned long long wv =
+                    P.grouped ? (unsigned long long)(X.n - __shfl_sync(kFull, st_hs, j)) : 1ull;
+                cnt = mb_base + (lane == 0 ? S * wv : 0ull);
+                mb = false;
             }
             --j;
         }
@@ -2873,7 +2925,8 @@ cgb_status cgb_apply_batch_device(cgb_handle* h, uint32_t dv_count, const uint64
         int bps = h->dfs_occupancy;
         if (h->cfg.dfs_blocks_per_sm) bps = std::min(bps, (int)h->cfg.dfs_blocks_per_sm);
         bool any_sum = false;
-        for (uint32_t e = 0; e < h->q.qe; ++e) any_sum |= h->plans[e].sum_from != 0 && !h->plans[e].sum_dense;
+        for (uint32_t e = 0; e < h->q.qe; ++e)
+            any_sum |= (h->plans[e].sum_from != 0 && !h->plans[e].sum_dense) || h->plans[e].memo_from != 0;
         da.wsum = nullptr;
         if (h->n_wsum && !da.vb && da.tail_cache) {
             if ((s = dense_level_sums(h)) != CGB_OK) return s;
@@ -2882,7 +2935,8 @@ cgb_status cgb_apply_batch_device(cgb_handle* h, uint32_t dv_count, const uint64
         lsum_bind(h, any_sum, da);
         if ((s = lsum_clear(h, da)) != CGB_OK) return s;
         bool uses_sums = false;
-        for (uint32_t e = 0; e < h->q.qe; ++e) uses_sums |= h->plans[e].sum_from != 0 || h->plans[e].tail_lane == 2;
+        for (uint32_t e = 0; e < h->q.qe; ++e)
+            uses_sums |= h->plans[e].sum_from != 0 || h->plans[e].tail_lane == 2 || h->plans[e].memo_from != 0;
         const dim3 grid(h->num_sms * bps), block(kDfsWarps * 32);
         if (footprint && uses_sums) k_dfs_count<false, true, true><<<grid, block, 0, h->stream>>>(da);
         else if (footprint) k_dfs_count<false, true, false><<<grid, block, 0, h->stream>>>(da);
@@ -2996,7 +3050,7 @@ cgb_status cgb_plan_info(const cgb_handle* h, uint32_t ei, uint32_t* out4) {
     out4[0] = P.n_core;
     out4[1] = P.sum_from;
     out4[2] = P.sum_dense;
-    out4[3] = P.tail_lane;
+    out4[3] = P.tail_lane | (uint32_t)P.memo_from << 8 | (uint32_t)P.memo_pos << 16;
     return CGB_OK;
 }
 

@@ -383,6 +383,39 @@ void plan_edges(const QueryMeta& q, const float* avg_deg, EdgePlan* plans, bool 
                 p.sum_same = 0;  // labels of their own: no prefix vertex can lie in a G_k
             }
         }
+        if (level_sum && known && analytic_tail && n_core >= 4) {
+            // subtree memo: the first split [s, n_core), with the latest prefix
+            // position p < s that works (not a seed-group position), such that
+            // every backward list of the range and every tail list hangs off p
+            // or the range
+            auto in_range = [&](uint32_t pos, uint32_t s0, uint32_t p0) { return pos == p0 || pos >= s0; };
+            for (uint32_t s0 = 2; s0 + 2 <= n_core && !p.memo_from; ++s0) {
+                for (int pp = (int)s0 - 1; pp >= 0 && !p.memo_from; --pp) {
+                    const uint32_t p0 = (uint32_t)pp;
+                    if (p.grouped && p0 < 2) continue;  // one unit per first vertex: no reuse
+                    bool ok = true;
+                    for (uint32_t k = s0; k < n_core && ok; ++k)
+                        for (uint32_t b2 = p.bn_off[k]; b2 < p.bn_off[k + 1]; ++b2)
+                            ok &= in_range(p.bn_pos[b2], s0, p0);
+                    for (uint32_t t = n_core; t < q.qv && ok; ++t) {
+                        for (uint32_t b2 = p.bn_off[t]; b2 < p.bn_off[t + 1]; ++b2)
+                            ok &= in_range(p.bn_pos[b2], s0, p0);
+                        for (uint32_t c = 0; c < s0; ++c)
+                            if (c != p0) ok &= ((p.excl[t] >> c) & 1u) == 0;
+                    }
+                    for (uint32_t k = s0; k < n_core && ok; ++k)
+                        for (uint32_t c = 0; c < s0; ++c)
+                            if (c != p0) ok &= lab(p.vs[k]) != lab(p.vs[c]);
+                    if (p.grouped) ok &= (p.hit_mask >> s0) == 0;
+                    // dense sums that already cover the range leave nothing to reuse
+                    if (p.sum_dense && p.sum_from <= s0) ok = false;
+                    if (ok) {
+                        p.memo_from = (uint8_t)s0;
+                        p.memo_pos = (uint8_t)p0;
+                    }
+                }
+            }
+        }
     }
 }
 

@@ -106,7 +106,18 @@ struct EdgePlan {
     uint8_t wslot;
     // kPlan* bits: per-plan schedule choices (the multi-query autotuner's)
     uint8_t flags;
-    uint8_t pad_;
+    // Subtree memo: every backward list of positions [memo_from, n_core) and
+    // every list of the tail sits at position memo_pos or inside that range,
+    // the range's core vertices share no label with prefix positions other
+    // than memo_pos, no tail excludes such a position, and (grouped plans) no
+    // position of the range is a hit position.  The count below depth
+    // memo_from is then a function of m[memo_pos] alone: the normal DFS
+    // counts it (unweighted, weighted once when complete) and, when none of
+    // it went to other warps, shares it through the level-sum table, once per
+    // (plan, vertex) and launch.  0: none.
+    uint8_t memo_from;
+    uint8_t memo_pos;
+    uint8_t pad_[3];
 };
 constexpr uint8_t kPlanNoTailCache = 0x1;  // recount every tail subset per core embedding
 constexpr uint32_t kMaxSumTails = 4;     // pendant tails per dense level-sum position

@@ -327,10 +327,12 @@ class Engine:
 
     def plan_info(self, ei: int) -> dict:
         """How query edge ei's plan counts: core positions, first level-sum
-        position (0 = none), dense sums, per-lane tail mode."""
+        position (0 = none), dense sums, per-lane tail mode, memoized subtree
+        (first position, 0 = none; key position)."""
         out = np.zeros(4, dtype=np.uint32)
         self._check(self.lib.cgb_plan_info(self.h, ei, out.ctypes.data))
-        return {"n_core": int(out[0]), "sum_from": int(out[1]), "dense": bool(out[2]), "tail_lane": int(out[3])}
+        return {"n_core": int(out[0]), "sum_from": int(out[1]), "dense": bool(out[2]), "tail_lane": int(out[3] & 0xff),
+                "memo_from": int((out[3] >> 8) & 0xff), "memo_pos": int((out[3] >> 16) & 0xff)}
 
     def check_symmetry(self) -> int:
         """Index entries whose mirror entry is missing (0 for a symmetric index)."""

@@ -81,6 +81,9 @@ SPECS = {
     "t_er_tree_u": WorkloadSpec("t_er_tree_u", 0, 3_000, 30_000, 12, 0.0, 3_000, 600, 2, 6, 161, 162, 163, 161),
     "t_er_tree_s": WorkloadSpec("t_er_tree_s", 0, 3_000, 30_000, 12, 0.0, 3_000, 600, 2, 6, 161, 162, 163, 160),
     "t_rmat_tree": WorkloadSpec("t_rmat_tree", 1, 8_192, 60_000, 16, 1.0, 6_000, 1_200, 2, 7, 171, 172, 173, 174),
+    # the R-MAT 4M/34M stream's label distribution on a small graph (tests
+    # run the headline's patterns on it)
+    "t_rmat32": WorkloadSpec("t_rmat32", 1, 8_192, 60_000, 32, 1.0, 6_000, 1_200, 1, 7, 181, 182, 183, 184),
 }
 
 

@@ -184,7 +184,9 @@ cgb_status cgb_plan_anchor(const cgb_handle* h, uint32_t ei, uint32_t* qvertex);
  * tuning: out4[0] = core positions (the others are counted as the tail),
  * out4[1] = first position counted by level sums (0 = none), out4[2] = 1
  * when those sums are precomputed for every vertex (several positions),
- * out4[3] = per-lane tail mode at the last core position (0, 1 or 2). */
+ * out4[3] = per-lane tail mode at the last core position (0, 1 or 2) in bits
+ * 0-7, the first position of a memoized subtree (0 = none) in bits 8-15 and
+ * the position whose vertex keys it in bits 16-23. */
 cgb_status cgb_plan_info(const cgb_handle* h, uint32_t ei, uint32_t* out4);
 
 /* Index symmetry check (after any pending delta merge-back): *n_asym = number

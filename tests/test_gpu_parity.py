@@ -541,3 +541,54 @@ def test_level_sum_workloads_reach_their_plans(name, dense, workdir):
         assert any(x["dense"] and x["sum_from"] + 1 < x["n_core"] for x in summed), info
     elif dense is False:
         assert any(not x["dense"] and x["sum_from"] + 1 == x["n_core"] for x in summed), info
+
+
+# the 7-vertex sparse pattern of the R-MAT 4M/34M benchmark (labels, edges)
+C3_SPARSE_PATTERN = ([7, 6, 2, 0, 19, 10, 6], [(0, 1), (0, 2), (1, 3), (1, 4), (1, 5), (1, 6), (5, 6)])
+
+
+@pytest.mark.gpu
+def test_memoized_subtrees_match_reference(workdir, tmp_path):
+    """The benchmark's sparse pattern on a small graph with its label
+    distribution: one edge plan counts the subtree below the hub vertex once
+    per (plan, vertex) and launch (EdgePlan.memo_from).  Counts equal the
+    reference's CPU path with memos and level sums on and off, in the
+    single-query and the multi-query engine."""
+    if not bind.have_ref():
+        pytest.skip("oracle/_ref/libcgbref.so not built")
+    from cgbdsm_b200 import MultiQuery
+    from cgbdsm_b200.workloads import GraphData
+
+    spec = SPECS["t_rmat32"]
+    p = materialize(spec, workdir)
+    labels, edges = C3_SPARSE_PATTERN
+    qp = str(tmp_path / "sparse.graph")
+    with open(qp, "w") as f:
+        for i, lb in enumerate(labels):
+            f.write(f"v {i} {lb}\n")
+        for a, b in edges:
+            f.write(f"e {a} {b} 0\n")
+    ref = bind.RefPipeline(qp, p["data"], p["update"], spec.cli_batch_size)
+    init, dv = ref.init_keys(), ref.dv_count
+    batches = []
+    while ref.step() >= 0:
+        batches.append(ref.last())
+    ref.close()
+    want = [r["count"] for r in batches]
+    assert sum(want) > 0
+    for flags in (0, FLAG_NO_LEVEL_SUM):
+        eng = Engine(flags=flags)
+        eng.load_query(len(labels), edges, labels)
+        eng.build_index(init, dv)
+        memo = [eng.plan_info(ei)["memo_from"] for ei in range(len(edges))]
+        assert (any(memo) if flags == 0 else not any(memo)), memo
+        got = [eng.apply_batch(r["dv"], r["ins"], r["del"], r["delta"], r["edge_ok"]) for r in batches]
+        eng.close()
+        assert got == want, f"flags {flags}"
+    g = GraphData(spec)
+    m = MultiQuery(dfs_budget_ms=120000)
+    m.load_graph(g.labels, g.initial)
+    qid = m.register(len(labels), edges, labels)
+    got = [int(m.apply_batch(ins=b)[0][qid]) for b in g.batches()]
+    m.close()
+    assert got == want, "multi-query engine"
