@@ -1925,11 +1925,20 @@ struct WsumJob {
 constexpr uint32_t kWsumLane = 16;  // owners with lists up to this long are summed by one lane
 
 // W(x) = sum over c in G(x) of (product of c's pendant list lengths) x
-// (product of the children's W(c)), for every x < dv.  Lane per owner for
-// short lists (records read coalesced, 32 consecutive owners per warp),
-// the whole warp for each longer one.
+// (product of the children's W(c)), for every x < dv, for the job
+// jobs[job0 + blockIdx.y] (the jobs of one launch are independent: their
+// children are done).  Lane per owner for short lists (records read
+// coalesced, 32 consecutive owners per warp), the whole warp for each longer
+// one.
 __global__ void k_wsum(const uint4* __restrict__ rec, uint32_t dvcap, const uint32_t* __restrict__ pool,
-                       const uint32_t* __restrict__ dval, uint32_t dv, WsumJob J) {
+                       const uint32_t* __restrict__ dval, uint32_t dv, const WsumJob* __restrict__ jobs,
+                       uint32_t job0) {
+    __shared__ WsumJob sJ;
+    static_assert(sizeof(WsumJob) % 4 == 0, "WsumJob is copied as words");
+    for (uint32_t t = threadIdx.x; t < sizeof(WsumJob) / 4; t += blockDim.x)
+        reinterpret_cast<uint32_t*>(&sJ)[t] = reinterpret_cast<const uint32_t*>(jobs + job0 + blockIdx.y)[t];
+    __syncthreads();
+    const WsumJob& J = sJ;
     const uint32_t lane = threadIdx.x & 31;
     const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
     auto term = [&](uint32_t c) -> unsigned long long {
@@ -2193,6 +2202,9 @@ struct cgb_handle {
     uint32_t lsum_slots = 0;
     unsigned long long* d_wsum = nullptr; size_t wsum_cap = 0;  // dense level sums [n_wsum][dvcap]
     uint32_t n_wsum = 0;
+    WsumJob* d_wjobs = nullptr;                 // [n_wsum] jobs, ordered by height (children first)
+    std::vector<uint32_t> wjob_level;           // job offsets of each height (size = heights + 1)
+    const void* wjobs_for = nullptr;            // d_wsum the jobs were built for
 
     // label-keyed mode (the multi-query engine's data-graph index): the
     // "direction" of a key is the label of its target vertex, the delta keys
@@ -2298,31 +2310,58 @@ cgb_status ensure_dvcap(cgb_handle* h, uint32_t dv) {
 
 // Dense level sums of every plan with sum_dense, children before parents
 // (a position's children sit at higher positions), on the stream.
+// The jobs are built (and uploaded) when the arrays move; one launch per
+// height runs every job of that height of every plan.
 cgb_status dense_level_sums(cgb_handle* h) {
     cgb_status s;
     if ((s = grow(h, h->d_wsum, h->wsum_cap, (size_t)h->n_wsum * h->dvcap)) != CGB_OK) return s;
-    for (uint32_t e = 0; e < h->q.qe; ++e) {
-        const EdgePlan& P = h->plans[e];
-        if (!P.sum_dense) continue;
-        const uint32_t s0 = P.sum_from, nc = P.n_core;
-        auto arr = [&](uint32_t k) { return h->d_wsum + (size_t)(P.wslot + k - s0) * h->dvcap; };
-        for (uint32_t k = nc; k-- > s0;) {
-            WsumJob J;
-            std::memset(&J, 0, sizeof(J));
-            J.dir = P.bn_dir[P.bn_off[k]];
-            J.dvis = P.bn_dvis[P.bn_off[k]];
-            for (uint32_t t = nc; t < P.n; ++t)
-                if (((P.sum_tails >> t) & 1u) && P.bn_pos[P.bn_off[t]] == k) {
-                    J.tdir[J.nt] = P.bn_dir[P.bn_off[t]];
-                    J.tvis[J.nt] = P.bn_dvis[P.bn_off[t]];
-                    ++J.nt;
-                }
-            for (uint32_t l = k + 1; l < nc; ++l)
-                if (P.bn_pos[P.bn_off[l]] == k) J.child[J.nch++] = arr(l);
-            J.out = arr(k);
-            k_wsum<<<h->num_sms * 8, 256, 0, h->stream>>>(h->rec, h->dvcap, h->pool, h->d_dval, h->dv, J);
-            LAUNCHED();
+    if (h->wjobs_for != h->d_wsum) {
+        std::vector<std::vector<WsumJob>> by_height;
+        for (uint32_t e = 0; e < h->q.qe; ++e) {
+            const EdgePlan& P = h->plans[e];
+            if (!P.sum_dense) continue;
+            const uint32_t s0 = P.sum_from, nc = P.n_core;
+            auto arr = [&](uint32_t k) { return h->d_wsum + (size_t)(P.wslot + k - s0) * h->dvcap; };
+            uint32_t height[cgb::kMaxQV] = {0};
+            for (uint32_t k = nc; k-- > s0;) {  // children sit at higher positions
+                WsumJob J;
+                std::memset(&J, 0, sizeof(J));
+                J.dir = P.bn_dir[P.bn_off[k]];
+                J.dvis = P.bn_dvis[P.bn_off[k]];
+                for (uint32_t t = nc; t < P.n; ++t)
+                    if (((P.sum_tails >> t) & 1u) && P.bn_pos[P.bn_off[t]] == k) {
+                        J.tdir[J.nt] = P.bn_dir[P.bn_off[t]];
+                        J.tvis[J.nt] = P.bn_dvis[P.bn_off[t]];
+                        ++J.nt;
+                    }
+                for (uint32_t l = k + 1; l < nc; ++l)
+                    if (P.bn_pos[P.bn_off[l]] == k) {
+                        J.child[J.nch++] = arr(l);
+                        height[k] = std::max(height[k], height[l] + 1);
+                    }
+                J.out = arr(k);
+                if (by_height.size() <= height[k]) by_height.resize(height[k] + 1);
+                by_height[height[k]].push_back(J);
+            }
         }
+        std::vector<WsumJob> all;
+        h->wjob_level.assign(1, 0);
+        for (auto& v : by_height) {
+            all.insert(all.end(), v.begin(), v.end());
+            h->wjob_level.push_back((uint32_t)all.size());
+        }
+        if (h->d_wjobs) CK(cudaFree(h->d_wjobs));
+        h->d_wjobs = nullptr;
+        CK(cudaMalloc(&h->d_wjobs, std::max<size_t>(all.size(), 1) * sizeof(WsumJob)));
+        CK(cudaMemcpy(h->d_wjobs, all.data(), all.size() * sizeof(WsumJob), cudaMemcpyHostToDevice));
+        h->wjobs_for = h->d_wsum;
+    }
+    for (size_t lv = 0; lv + 1 < h->wjob_level.size(); ++lv) {
+        const uint32_t j0 = h->wjob_level[lv], nj = h->wjob_level[lv + 1] - j0;
+        if (!nj) continue;
+        const dim3 grid((unsigned)std::max<uint32_t>((uint32_t)h->num_sms * 2, (uint32_t)h->num_sms * 8 / nj), nj);
+        k_wsum<<<grid, 256, 0, h->stream>>>(h->rec, h->dvcap, h->pool, h->d_dval, h->dv, h->d_wjobs, j0);
+        LAUNCHED();
     }
     CK(cudaGetLastError());
     return CGB_OK;
@@ -2668,7 +2707,7 @@ void cgb_destroy(cgb_handle* h) {
                     h->d_seed, h->d_counts, h->d_stats, h->d_tasks, h->d_qctr, h->d_temp, h->d_qe_dirs, h->d_edge_ok,
                     h->d_vb, h->d_rb_slot, h->d_rb_sel, h->d_rb_bits, h->d_rb_ctr, h->d_rb_new, h->d_small_runs,
                     h->d_big_runs, h->d_tiny_runs, h->d_list_ctr, h->d_rev, h->d_touched, h->d_plans,
-                    h->d_vbplans, h->d_dir_edge, h->d_lsum, h->d_wsum};
+                    h->d_vbplans, h->d_dir_edge, h->d_lsum, h->d_wsum, h->d_wjobs};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (h->h_scal) cudaFreeHost(h->h_scal);
@@ -2741,6 +2780,7 @@ cgb_status cgb_build_index(cgb_handle* h, const uint64_t* keys, uint64_t n, uint
                     !(h->cfg.flags & CGB_FLAG_PLAIN_CORE_ORDER), !(h->cfg.flags & CGB_FLAG_NO_SEED_GROUPS),
                     !(h->cfg.flags & CGB_FLAG_WARP_TAIL), !(h->cfg.flags & CGB_FLAG_NO_LEVEL_SUM), true);
     h->n_wsum = 0;
+    h->wjobs_for = nullptr;  // the plans changed: rebuild the level-sum jobs
     for (uint32_t e = 0; e < h->q.qe; ++e)
         if (h->plans[e].sum_dense) {
             h->plans[e].wslot = (uint8_t)h->n_wsum;
