@@ -716,6 +716,7 @@ struct DfsArgs {
     unsigned long long* lsum_tab;  // level-sum table [lsum_mask + 1][2], zeroed before the launch (nullptr: none)
     uint32_t lsum_mask;
     const unsigned long long* wsum;  // dense level sums [array][dvcap] (nullptr: none)
+    uint32_t pair_lane_max;      // pair counting: longest shorter list a lane scans alone
 };
 
 // Footprint of a matching launch: the bytes of every distinct record it
@@ -933,6 +934,7 @@ __device__ unsigned long long tail_count_warp(const EdgePlan& P, const uint32_t*
 // in the set, and intersects the subsets with lists at position j per
 // candidate.
 constexpr unsigned long long kDynamic = ~0ull;
+constexpr uint32_t kPairLaneMax = 64;  // pair counting: longest shorter list a lane scans alone ($CGB_PAIR_LANE_MAX)
 constexpr uint32_t kClean = 0xffu;  // tail cache up to date
 
 // Recounts only the entries that depend on a position >= dirty (the shallowest
@@ -1541,6 +1543,7 @@ __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
         ls_dirty = 0;
         const bool level_sum = kSums && P.sum_from && !a.vb && !self_loops && (tail_cache || !has_tail);
         const bool memo_on = kSums && P.memo_from && a.lsum_tab && !a.vb && !self_loops;
+        const bool pair_on = kSums && P.pair_last && !a.vb && !self_loops && (tail_cache || !has_tail);
         mb = false;
         setup(jbase);
         if (kind == 2 && lane == jbase) { st_gen = tgen; st_next = tlo; st_len = thi; }
@@ -1706,6 +1709,9 @@ __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
                     if (__shfl_sync(kFull, want, 0)) {
                         bool has = false;
                         if (lane >= jbase && lane < j) has = st_next < st_len || st_pos < st_ncand;
+                        // at a pair-counting depth a chunk's passing candidates were
+                        // partly counted already: only its unscanned range is shared
+                        if (pair_on && lane == nc - 2 && lane >= jbase && lane < j) has = st_next < st_len;
                         if (lane == j) has = glen > gnext + 32u;
                         const uint32_t hb = __ballot_sync(kFull, has);
                         uint32_t slot = 0xffffffffu;
@@ -1727,6 +1733,9 @@ __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
                                 if (d == j) {
                                     lo = gnext + 32u;
                                     hi = glen;
+                                } else if (pair_on && d == nc - 2) {
+                                    lo = st_next;  // the buffered survivors stay with this warp
+                                    hi = st_len;
                                 } else {
                                     lo = st_pos < st_ncand ? st_next - 32u + (s_cand[w][d][st_pos] >> kCandBits)
                                                            : st_next;
@@ -1748,6 +1757,7 @@ __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
                             if (lane == 0) *(volatile uint32_t*)(tk + 3) = task_tag(epoch, slot);
                             if (lane == d) {
                                 if (d == j) st_len = gnext + 32u;
+                                else if (pair_on && d == nc - 2) st_len = st_next;
                                 else { st_len = st_next; st_ncand = st_pos; }
                             }
                             if (d == j) glen = gnext + 32u;
@@ -1866,8 +1876,75 @@ __global__ void __launch_bounds__(kDfsWarps * 32, 4) k_dfs_count(DfsArgs a) {
                         cnt += ok ? 1ull : 0ull;
                     }
                 } else {
-                    const uint32_t bal = __ballot_sync(kFull, ok);
-                    if (ok) s_cand[w][j][__popc(bal & ((1u << lane) - 1u))] = c | (lane << kCandBits);
+                    bool desc = ok;  // survivors buffered for the descent
+                    if (pair_on && j == nc - 2) {
+                        // each lane counts its candidate's last level: |A ∩ B|,
+                        // A = the prefix list of the last position, B = the
+                        // candidate's own; candidates whose shorter list is long
+                        // descend as usual
+                        const uint32_t ka = P.pair_a, kb = P.pair_b;
+                        if (lane == 0) {
+                            const size_t at = (size_t)P.bn_dir[ka] * a.dvcap + m[P.bn_pos[ka]];
+                            uint4 r = a.rec[at];
+                            if (!P.bn_dvis[ka]) r.w = 0;
+                            bn[ka] = r;
+                            rb.note(ka, at);
+                        }
+                        __syncwarp();
+                        const uint4 ra = bn[ka];
+                        const uint32_t la = ra.y + ra.w;
+                        unsigned long long pc = 0;
+                        bool counted = false;
+                        if (ok) {
+                            const size_t atb = (size_t)P.bn_dir[kb] * a.dvcap + c;
+                            uint4 rq = a.rec[atb];
+                            if (!P.bn_dvis[kb]) rq.w = 0;
+                            rb.touch(atb);
+                            n_bytes += 16;
+                            const uint32_t lq = rq.y + rq.w;
+                            if (min(la, lq) <= a.pair_lane_max) {
+                                counted = true;
+                                const uint32_t slq = rb.slot_at(atb);
+                                if (lq <= la) {
+                                    for (uint32_t i = 0; i < lq; ++i) {
+                                        const uint32_t x = i < rq.y ? __ldg(a.pool + rq.x + i) : __ldg(a.dval + rq.z + (i - rq.y));
+                                        pc += rb.has(ka, ra, a.pool, a.dval, x) ? 1ull : 0ull;
+                                    }
+                                } else {
+                                    for (uint32_t i = 0; i < la; ++i) {
+                                        const uint32_t x = i < ra.y ? __ldg(a.pool + ra.x + i) : __ldg(a.dval + ra.z + (i - ra.y));
+                                        pc += rb.has_slot(slq, rq, a.pool, a.dval, x) ? 1ull : 0ull;
+                                    }
+                                }
+                                for (uint32_t e = P.pair_excl; e; e &= e - 1) {
+                                    const uint32_t x = m[__ffs(e) - 1];
+                                    if (x != kNoVertex && rb.has(ka, ra, a.pool, a.dval, x) &&
+                                        rb.has_slot(slq, rq, a.pool, a.dval, x))
+                                        --pc;
+                                }
+                            }
+                        }
+                        const uint32_t cb = __ballot_sync(kFull, counted);
+                        if (cb) {
+                            unsigned long long tc = 1;
+                            if (has_tail) {
+                                if (dirty <= P.tail_dep)
+                                    tail_prepare(P, m, bn, s_tc[w], dirty, nc - 2, a.rec, a.dvcap, a.pool, a.dval,
+                                                 self_loops, lane, n_bytes, rb);
+                                dirty = kClean;
+                                tc = tail_static_product(P, s_tc[w]);
+                                // the cache is marked current: so must be the prefix's tail
+                                // count that the descending candidates' last level reads
+                                if (P.tail_const) tail_const = tc;
+                            }
+                            const unsigned long long wgt = P.grouped ? gw(__shfl_sync(kFull, st_hs, j)) : 1ull;
+                            if (counted) cnt += pc * tc * wgt;
+                            if (lane == 0) n_tail += __popc(cb);
+                        }
+                        desc = ok && !counted;
+                    }
+                    const uint32_t bal = __ballot_sync(kFull, desc);
+                    if (desc) s_cand[w][j][__popc(bal & ((1u << lane) - 1u))] = c | (lane << kCandBits);
                     if (lane == j) { st_ncand = __popc(bal); st_pos = 0; }
                 }
                 if (lane == j) st_next = gnext + 32;
@@ -2196,6 +2273,7 @@ struct cgb_handle {
     uint32_t rb_cap = 0;               // bit sets the budget holds
     bool rb_valid = false;             // slot table and bit sets match the index
     uint32_t rb_min_len = kRunBitsMinLen;
+    uint32_t pair_lane_max = kPairLaneMax;
     uint8_t* d_rev = nullptr;          // reverse direction of each direction
     uint32_t* d_touched = nullptr; size_t touched_cap = 0;  // footprint runs: record bit set
     unsigned long long* d_lsum = nullptr;  // level-sum table, sized with the record table
@@ -2657,6 +2735,7 @@ cgb_status cgb_create(const cgb_config* cfg, cgb_handle** out) {
     if (cfg) h->cfg = *cfg; else cgb_default_config(&h->cfg);
     h->device = h->cfg.device;
     if (const char* e = std::getenv("CGB_RUN_BITS_MIN_LEN")) h->rb_min_len = (uint32_t)std::max(1l, std::atol(e));
+    if (const char* e = std::getenv("CGB_PAIR_LANE_MAX")) h->pair_lane_max = (uint32_t)std::max(0l, std::atol(e));
     int ndev = 0;
     cudaError_t e = cudaGetDeviceCount(&ndev);
     if (e != cudaSuccess || ndev == 0) {
@@ -2936,6 +3015,7 @@ cgb_status cgb_apply_batch_device(cgb_handle* h, uint32_t dv_count, const uint64
         da.num_shards = h->cfg.num_shards ? h->cfg.num_shards : 1u;
         da.steal = (h->cfg.flags & CGB_FLAG_NO_STEAL) ? 0u : 1u;
         da.tail_cache = (h->cfg.flags & CGB_FLAG_NO_TAIL_CACHE) ? 0u : 1u;
+        da.pair_lane_max = h->pair_lane_max;
         da.shard = h->cfg.shard_index < da.num_shards ? h->cfg.shard_index : 0u;
         da.self_seen = h->d_self;
         da.vb = (h->cfg.flags & CGB_FLAG_MASK_PRUNE) ? h->d_vb : nullptr;
@@ -2976,7 +3056,8 @@ cgb_status cgb_apply_batch_device(cgb_handle* h, uint32_t dv_count, const uint64
         if ((s = lsum_clear(h, da)) != CGB_OK) return s;
         bool uses_sums = false;
         for (uint32_t e = 0; e < h->q.qe; ++e)
-            uses_sums |= h->plans[e].sum_from != 0 || h->plans[e].tail_lane == 2 || h->plans[e].memo_from != 0;
+            uses_sums |= h->plans[e].sum_from != 0 || h->plans[e].tail_lane == 2 || h->plans[e].memo_from != 0 ||
+                         h->plans[e].pair_last != 0;
         const dim3 grid(h->num_sms * bps), block(kDfsWarps * 32);
         if (footprint && uses_sums) k_dfs_count<false, true, true><<<grid, block, 0, h->stream>>>(da);
         else if (footprint) k_dfs_count<false, true, false><<<grid, block, 0, h->stream>>>(da);

@@ -434,6 +434,7 @@ DfsArgs mq_dfs_args(cgb_mq* m, const EdgePlan* plans, uint32_t G, uint64_t budge
     da.budget_ns = budget_ms * 1000000ull;
     lsum_bind(h, true, da);
     da.wsum = nullptr;  // one-position (table) level sums only
+    da.pair_lane_max = h->pair_lane_max;
     return da;
 }
 

@@ -383,6 +383,28 @@ void plan_edges(const QueryMeta& q, const float* avg_deg, EdgePlan* plans, bool 
                 p.sum_same = 0;  // labels of their own: no prefix vertex can lie in a G_k
             }
         }
+        if (level_sum && analytic_tail && n_core >= 4) {
+            // pair counting at the last core position
+            const uint32_t j = n_core - 1;
+            if (p.bn_off[j + 1] - p.bn_off[j] == 2) {
+                const uint32_t b0 = p.bn_off[j], b1 = b0 + 1;
+                const bool first_prev = p.bn_pos[b0] == j - 1;
+                const uint32_t bb = first_prev ? b0 : b1, ba = first_prev ? b1 : b0;
+                bool ok = p.bn_pos[bb] == j - 1 && p.bn_pos[ba] < j - 1;
+                for (uint32_t t = n_core; t < q.qv && ok; ++t) {
+                    for (uint32_t b2 = p.bn_off[t]; b2 < p.bn_off[t + 1]; ++b2) ok &= p.bn_pos[b2] + 1u < j;
+                    ok &= ((p.excl[t] >> (j - 1)) & 3u) == 0;
+                }
+                if (p.grouped) ok &= ((p.hit_mask >> (j - 1)) & 3u) == 0;
+                if (ok) {
+                    p.pair_last = 1;
+                    p.pair_a = (uint8_t)ba;
+                    p.pair_b = (uint8_t)bb;
+                    for (uint32_t t = 0; t + 1 < j; ++t)
+                        if (!known || lab(p.vs[t]) == lab(p.vs[j])) p.pair_excl |= (uint16_t)(1u << t);
+                }
+            }
+        }
         if (level_sum && known && analytic_tail && n_core >= 4) {
             // subtree memo: the first split [s, n_core), with the latest prefix
             // position p < s that works (not a seed-group position), such that

@@ -117,7 +117,18 @@ struct EdgePlan {
     // (plan, vertex) and launch.  0: none.
     uint8_t memo_from;
     uint8_t memo_pos;
-    uint8_t pad_[3];
+    // Pair counting at the last core position j = n_core - 1: its two lists
+    // are bn[pair_a] (owned by a position < j - 1) and bn[pair_b] (owned by
+    // j - 1), and no tail list or tail exclusion involves j - 1 or j.  Each
+    // lane then counts its own depth-(j - 1) candidate's last level as the
+    // intersection size of the two lists, less the matched prefix vertices
+    // at positions pair_excl (same label as vs[j]) lying in both, times the
+    // prefix-only tail count, instead of the warp descending into it.
+    uint8_t pair_last;
+    uint8_t pair_a, pair_b;
+    uint8_t pad_;
+    uint16_t pair_excl;
+    uint16_t pad2_;
 };
 constexpr uint8_t kPlanNoTailCache = 0x1;  // recount every tail subset per core embedding
 constexpr uint32_t kMaxSumTails = 4;     // pendant tails per dense level-sum position

@@ -26,8 +26,9 @@ int main(int argc, char** argv) {
     cgb::plan_edges(q, avg, plans.data(), true, true, true, true, true, !mq);
     for (uint32_t ei = 0; ei < q.qe; ++ei) {
         const cgb::EdgePlan& p = plans[ei];
-        std::printf("%u %u %u %u %u %u %u %u %u %u %u %u |", ei, p.n, p.n_core, p.sum_from, p.sum_dense, p.sum_tails,
-                    p.sum_same, p.memo_from, p.memo_pos, p.grouped, p.hit_mask, p.tail_lane);
+        std::printf("%u %u %u %u %u %u %u %u %u %u %u %u %u %u %u %u |", ei, p.n, p.n_core, p.sum_from, p.sum_dense,
+                    p.sum_tails, p.sum_same, p.memo_from, p.memo_pos, p.grouped, p.hit_mask, p.tail_lane, p.pair_last,
+                    p.pair_a, p.pair_b, p.pair_excl);
         for (uint32_t j = 0; j < p.n; ++j) std::printf(" %u", p.vs[j]);
         std::printf(" |");
         for (uint32_t j = 0; j <= p.n; ++j) std::printf(" %u", p.bn_off[j]);

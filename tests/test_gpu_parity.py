@@ -592,3 +592,54 @@ def test_memoized_subtrees_match_reference(workdir, tmp_path):
     got = [int(m.apply_batch(ins=b)[0][qid]) for b in g.batches()]
     m.close()
     assert got == want, "multi-query engine"
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("lane_max", [0, 2])
+def test_pair_counting_mixed_with_descent(lane_max, workdir, tmp_path, monkeypatch):
+    """Pair counting at the last core position (EdgePlan.pair_last) counts
+    the candidates whose shorter list is at most $CGB_PAIR_LANE_MAX entries
+    per lane and lets the others descend; shared work from that depth must
+    not count a chunk's candidates twice.  With the bound at 0 or 2 every
+    chunk mixes both kinds, and every chunk is shared (FLAG_FORCE_SPLIT):
+    counts equal the reference's on C1 and on the benchmark's sparse
+    pattern (single-query and multi-query engine)."""
+    if not bind.have_ref():
+        pytest.skip("oracle/_ref/libcgbref.so not built")
+    from cgbdsm_b200 import MultiQuery
+    from cgbdsm_b200.workloads import GraphData
+
+    monkeypatch.setenv("CGB_PAIR_LANE_MAX", str(lane_max))
+    labels, edges = C3_SPARSE_PATTERN
+    qp = str(tmp_path / "sparse.graph")
+    with open(qp, "w") as f:
+        for i, lb in enumerate(labels):
+            f.write(f"v {i} {lb}\n")
+        for a, b in edges:
+            f.write(f"e {a} {b} 0\n")
+    for name, query in [("c1", None), ("t_rmat32", qp)]:
+        spec = SPECS[name]
+        p = materialize(spec, workdir)
+        qfile = query or p["query"]
+        ref = bind.RefPipeline(qfile, p["data"], p["update"], spec.cli_batch_size)
+        init, dv = ref.init_keys(), ref.dv_count
+        batches = []
+        while ref.step() >= 0:
+            batches.append(ref.last())
+        ref.close()
+        ql, qe = read_query(qfile)
+        eng = Engine(flags=FLAG_FORCE_SPLIT)
+        eng.load_query(len(ql), qe, ql)
+        eng.build_index(init, dv)
+        assert any(eng.plan_info(ei)["n_core"] >= 4 for ei in range(len(qe)))
+        got = [eng.apply_batch(r["dv"], r["ins"], r["del"], r["delta"], r["edge_ok"]) for r in batches]
+        eng.close()
+        assert got == [r["count"] for r in batches], name
+        if query:
+            g = GraphData(spec)
+            m = MultiQuery(dfs_budget_ms=120000)
+            m.load_graph(g.labels, g.initial)
+            qid = m.register(len(ql), qe, ql)
+            got = [int(m.apply_batch(ins=b)[0][qid]) for b in g.batches()]
+            m.close()
+            assert got == [r["count"] for r in batches], "multi-query engine"

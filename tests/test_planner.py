@@ -12,6 +12,8 @@ plan which takes a shortcut satisfies the conditions it relies on:
       the range, and the range's labels meet no other prefix position
   per-lane pendant tails: tails off the last core vertex have one list and a
       label group of their own
+  pair counting: the last core position has two lists, one owned by the
+      position before it, and no tail list or exclusion involves either
 """
 from __future__ import annotations
 
@@ -56,7 +58,8 @@ def dump(tmp_path_factory):
             f = [int(x) for x in head.split()]
             plans.append({"ei": f[0], "n": f[1], "nc": f[2], "sum_from": f[3], "dense": f[4], "sum_tails": f[5],
                           "sum_same": f[6], "memo_from": f[7], "memo_pos": f[8], "grouped": f[9], "hit_mask": f[10],
-                          "tail_lane": f[11], "vs": [int(x) for x in vs.split()],
+                          "tail_lane": f[11], "pair_last": f[12], "pair_a": f[13], "pair_b": f[14],
+                          "pair_excl": f[15], "vs": [int(x) for x in vs.split()],
                           "off": [int(x) for x in off.split()], "pos": [int(x) for x in pos.split()],
                           "excl": [int(x) for x in excl.split()], "gid": [int(x) for x in gid.split()]})
         return plans
@@ -116,6 +119,16 @@ def check_plan(p, labels):
         if p["grouped"]:
             assert p["hit_mask"] >> m == 0
         assert not (p["dense"] and s <= m)
+    if p["pair_last"]:
+        j = nc - 1
+        lists = list(range(p["off"][j], p["off"][j + 1]))
+        assert len(lists) == 2 and sorted([p["pair_a"], p["pair_b"]]) == lists
+        assert p["pos"][p["pair_b"]] == j - 1 and p["pos"][p["pair_a"]] < j - 1
+        for t in range(nc, n):
+            assert all(x < j - 1 for x in _lists(p, t)) and ((p["excl"][t] >> (j - 1)) & 3) == 0
+        if p["grouped"]:
+            assert ((p["hit_mask"] >> (j - 1)) & 3) == 0
+        assert p["pair_excl"] == sum(1 << t for t in range(j - 1) if lab[t] == lab[j])
 
 
 def test_headline_patterns_plan_their_shortcuts(dump):
@@ -124,6 +137,7 @@ def test_headline_patterns_plan_their_shortcuts(dump):
     sparse = dump(*C3_SPARSE)
     memo = [(p["ei"], p["memo_from"], p["memo_pos"]) for p in sparse if p["memo_from"]]
     assert memo == [(1, 3, 2)]  # edge (0, 2): the subtree below the hub vertex 1
+    assert sparse[1]["pair_last"]  # and its last level is one intersection per lane
     for labels, edges, plans in [(*C3_TREE, tree), (*C3_SPARSE, sparse)]:
         for p in plans:
             check_plan(p, labels)
@@ -145,6 +159,7 @@ def test_query_set_plans_meet_their_conditions(dump, qset):
                 seen["dense"] += p["dense"]
                 seen["one"] += bool(p["sum_from"]) and not p["dense"]
                 seen["memo"] += bool(p["memo_from"])
+                seen["pair"] += p["pair_last"]
     assert seen["one"] > 0, seen
 
 
