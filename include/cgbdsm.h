@@ -69,8 +69,8 @@ typedef struct {
 #define CGB_FLAG_FOOTPRINT 0x400u         /* measure the matching footprint (cgb_last_stats[4]); slower   */
 #define CGB_FLAG_WARP_TAIL 0x800u         /* count last-level tails one embedding at a time per warp,
                                              never one candidate per lane                                */
-#define CGB_FLAG_NO_LEVEL_SUM 0x1000u     /* scan the last core level per prefix even where its one list
-                                             hangs off an earlier position (no per-owner level sums)     */
+#define CGB_FLAG_NO_LEVEL_SUM 0x1000u     /* enumerate every core level: no level sums (one-position or
+                                             dense), no subtree memos, no per-lane pair counting          */
 
 /* Limits (reference: utils/config.h:5-6; key layout calig_helper_gamma.cu:228-229). */
 #define CGB_MAX_QV 12
